@@ -1,0 +1,253 @@
+/*
+ * s1b -- B200-native (sm_100a) kernels for the s1proc per-burst
+ * interferogram chain: TOPS deramp, FP64 zero-Doppler geocoding with
+ * bilinear resampling and reramp (geo2rdr), crossmul with multilooking and
+ * coherence, and the Goldstein filter.
+ *
+ * C ABI: plain pointers and sizes, no C++ or torch types.  Every function
+ * returns an int status (S1B_OK = 0) and never exits the process.  Device
+ * pointers are caller-owned CUDA device memory; `stream` is a cudaStream_t
+ * passed as void* (NULL = the legacy default stream).  Calls are
+ * asynchronous with respect to the host unless stated otherwise; errors
+ * detected on the device are reported through the status words the
+ * functions document.
+ *
+ * The reference project exposes this path as standalone executables
+ * (geo2rdr, crossmul_daemon, crossmul, goldstein) that exchange binary files.
+ * Each entry point below names the reference code it replaces.
+ */
+#ifndef S1B_H
+#define S1B_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+#define S1B_OK 0
+#define S1B_ERR_INVALID_ARGUMENT 1
+#define S1B_ERR_CUDA 2
+#define S1B_ERR_TOO_LARGE 3
+#define S1B_ERR_EMPTY 4          /* empty DEM window / empty overlap: nothing to do */
+#define S1B_ERR_NO_DEVICE 5
+#define S1B_ERR_UNSUPPORTED 6
+
+/* Human-readable status text (static storage). */
+const char *s1b_status_string(int status);
+/* Library version, major*10000 + minor*100 + patch. */
+int s1b_version(void);
+/* Last CUDA error text recorded by this thread's most recent failing call. */
+const char *s1b_last_error(void);
+/* sizeof(s1b_burst_plan_t) and sizeof(s1b_orbit_poly_t) as compiled into the
+ * library, for bindings that mirror the structs (ctypes, cgo). */
+size_t s1b_sizeof_burst_plan(void);
+size_t s1b_sizeof_orbit_poly(void);
+
+/* ---------------------------------------------------------- input records */
+#define S1B_MAX_STATE_VECTORS 64
+#define S1B_MAX_ORBIT_WINDOWS (S1B_MAX_STATE_VECTORS - 3)
+
+/* Orbit state vectors (host arrays), the content of the reference's orbit
+ * text file: read_orbit_ascii, csrc/src/orbit.cu:147-168.  x, v: [n*3]. */
+typedef struct s1b_orbit_t {
+  int32_t n;
+  const double *t;
+  const double *x;
+  const double *v;
+} s1b_orbit_t;
+
+/* FM-rate or Doppler-centroid polynomial records (host arrays):
+ * read_polynomials, csrc/src/sario.cu:80-103.  Each record holds the
+ * azimuth time, the reference range time t0 and c0 + c1 dt + c2 dt^2. */
+typedef struct s1b_poly_table_t {
+  int32_t n;
+  const double *time;
+  const double *t0;
+  const double *c0;
+  const double *c1;
+  const double *c2;
+} s1b_poly_table_t;
+
+/* Subswath radar parameters: the DB keys geo2rdr reads,
+ * csrc/src/geo2rdr.cu:333-349. */
+typedef struct s1b_radar_t {
+  int32_t samples_per_burst;
+  int32_t lines_per_burst;
+  double prf;
+  double wvl;
+  double hmin;
+  double hmax;
+  double range_sampling_rate;
+  double slant_range_time;
+  double azimuth_steering_rate; /* degrees / s */
+  double azimuth_time_interval;
+  double radar_frequency;
+} s1b_radar_t;
+
+/* One burst: azimuthTimeSeconds<i>, first/lastValidLine<i>,
+ * first/lastValidSample<i> (csrc/src/geo2rdr.cu:365-376). */
+typedef struct s1b_burst_t {
+  double azimuth_time;
+  int32_t first_valid_line;
+  int32_t last_valid_line;
+  int32_t first_valid_sample;
+  int32_t last_valid_sample;
+} s1b_burst_t;
+
+/* Lat/lon grid of the DEM: readrsc, csrc/src/sario.cu:12-60. */
+typedef struct s1b_rsc_t {
+  int32_t nlat;
+  int32_t nlon;
+  double latmax; /* Y_FIRST */
+  double lonmin; /* X_FIRST */
+  double dlat;   /* Y_STEP (negative) */
+  double dlon;   /* X_STEP */
+} s1b_rsc_t;
+
+/* Orbit as piecewise polynomials: one degree-7 polynomial per 4-vector
+ * window (the same interpolant as the reference's 4-point Hermite,
+ * csrc/src/orbit.cu:170-245), expanded around the window centre. */
+typedef struct s1b_orbit_poly_t {
+  int32_t n_state;
+  int32_t n_win; /* n_state - 3; window w (1..n_win) uses vectors w-1..w+2 */
+  double t0;     /* time of state vector 0 */
+  double inv_dt; /* 1 / (t[1] - t[0]), the window selector of orbit.cu:229 */
+  double tc[S1B_MAX_ORBIT_WINDOWS];
+  double c[S1B_MAX_ORBIT_WINDOWS][3][8];
+} s1b_orbit_poly_t;
+
+/* Everything the reference computes on the host for one burst before its
+ * kernels run (csrc/src/geo2rdr.cu:387-400, 469-542, 569-600), plus the
+ * orbit polynomials.  Produced by s1b_burst_plan(); passed to the kernels
+ * by value.  The DEM window is on the RSC grid, [top, bottom) x [left, right). */
+typedef struct s1b_burst_plan_t {
+  s1b_orbit_poly_t orbit;
+  int32_t lines, samples;
+  int32_t first_valid_line, last_valid_line, first_valid_sample, last_valid_sample;
+  int32_t win_left, win_top, win_right, win_bottom;
+  int32_t rsc_nlat, rsc_nlon;
+  double tstart, dtaz, ati;
+  double rngstart, dmrg;
+  double slant_range_time, range_sampling_rate;
+  double wvl, k4pi_wvl; /* 4 pi / wvl */
+  double tmid, xmid[3], vmid[3], amid[3];
+  double ks, etac0;
+  double fm[4]; /* interpolated FM-rate t0, c0, c1, c2 at the burst centre */
+  double dc[4]; /* interpolated Doppler-centroid t0, c0, c1, c2 */
+  double lat0, lon0, dlat, dlon; /* lat of window row 0, lon of window column 0 */
+  double latlon_box[4];          /* latmin, latmax, lonmin, lonmax */
+} s1b_burst_plan_t;
+
+/* Host only.  Fill `plan` for one burst.  Returns S1B_ERR_EMPTY (plan still
+ * filled) when the burst's DEM window is empty, as geo2rdr skips it
+ * (csrc/src/geo2rdr.cu:583-584).  `rsc` may be NULL (no DEM window). */
+int s1b_burst_plan(const s1b_radar_t *radar, const s1b_orbit_t *orbit,
+                   const s1b_poly_table_t *fm, const s1b_poly_table_t *dc,
+                   const s1b_burst_t *burst, const s1b_rsc_t *rsc,
+                   s1b_burst_plan_t *plan);
+
+/* Host only.  Orbit polynomials from state vectors. */
+int s1b_orbit_poly(const s1b_orbit_t *orbit, s1b_orbit_poly_t *poly);
+
+/* Host only.  Burst footprint [latmin, latmax, lonmin, lonmax] at heights
+ * hmin..hmax: replaces bounds(), csrc/src/bounds.cu:288-317. */
+int s1b_bounds(const s1b_orbit_poly_t *orbit, double start_time, double end_time,
+               double start_rng, double end_rng, double hmin, double hmax,
+               double latlons[4]);
+
+/* Host only.  Orbit position/velocity at n times: replaces intp_orbit,
+ * csrc/src/orbit.cu:224-245 (and s1proc.orbit.interp_orbit). */
+int s1b_orbit_eval_host(const s1b_orbit_poly_t *orbit, const double *t, int64_t n,
+                        double *satx, double *satv);
+
+/* ------------------------------------------------------------- geo2rdr */
+
+/* TOPS deramp of one burst: out = in * exp(-i pi kt (eta - etaref)^2).
+ * Replaces deramp_burst, csrc/src/geo2rdr.cu:138-158 (+ the host
+ * coefficients at 469-542).  in/out: complex64 [lines * samples] device
+ * (in == out allowed).  Phase in FP64, reduced mod 2 pi, FP32 rotation. */
+int s1b_deramp(const s1b_burst_plan_t *plan, const void *in, void *out, void *stream);
+
+/* Geocode a deramped burst onto the plan's DEM window: per DEM pixel FP64
+ * llh->ECEF, zero-Doppler Newton, validity window, bilinear interpolation,
+ * reramp and range phase.  Replaces reproject + find_nonzero_rows,
+ * csrc/src/geo2rdr.cu:86-128, 170-248, 273-299.
+ *   dem:       int16 device pointer to the window's first pixel (row `win_top`,
+ *              column `win_left` of the RSC grid); `dem_pitch` elements per row.
+ *   deramped:  complex64 [lines * samples] device.
+ *   out:       complex64 [(win_bottom-win_top) * (win_right-win_left)] device.
+ *   rows:      int32[2] device, or NULL: first and one-past-last window row
+ *              holding a non-zero output pixel (first = nrow, last = -1 when
+ *              none), like the reference's d_first/d_last. */
+int s1b_geo2rdr(const s1b_burst_plan_t *plan, const int16_t *dem, int64_t dem_pitch,
+                const void *deramped, void *out, int32_t *rows, void *stream);
+
+/* Zero-Doppler solve for arbitrary ECEF points (device arrays, n points):
+ * replaces orbitrangetime / orbitrangetime_vec (csrc/src/orbit.cu:247-280,
+ * s1proc/orbit.py:118-188).  Seeds every point with (tline0, orbit(tline0)).
+ * xyz: [n*3] f64; tline: [n] f64; dr: [n*3] f64 (or NULL). */
+int s1b_zero_doppler(const s1b_orbit_poly_t *orbit, const double *xyz, int64_t n,
+                     double tline0, double *tline, double *dr, void *stream);
+
+/* Geodetic -> ECEF (device arrays [n*3], degrees/metres): replaces llh2xyz,
+ * csrc/src/orbit.cu:15-35 and s1proc/geometry.py:150-162, 204-216. */
+int s1b_llh2xyz(const double *llh, double *xyz, int64_t n, void *stream);
+
+/* ------------------------------------------------- crossmul + multilook */
+
+/* One interferogram: conj(ref) * sec over the aligned box, averaged over
+ * rowlook x collook, together with the power looks of both SLCs and the
+ * coherence.  Replaces conj_mul + cpx_col_look + cpx_row_look (+ point_angle)
+ * of crossmul_daemon (csrc/src/sario.cu:199-286, crossmul_daemon.cu:921-975)
+ * and the amplitude/coherence NumPy code (s1proc/coherence.py:14-147).
+ *   ref/sec: complex64 device rasters of ref_height x ref_width (sec_...);
+ *            pixel (r, c) of the global grid is at
+ *            ref[(r - ref_top) * ref_width + (c - ref_left)].
+ *   box:     full-resolution [top, top + nrow_ml*rowlook) x
+ *            [left, left + ncol_ml*collook), inside both rasters.
+ *   outputs  (each may be NULL), [nrow_ml * ncol_ml]:
+ *     ifg   complex64  mean conj(ref)*sec
+ *     amp1  float32    sqrt(mean |ref|^2)
+ *     amp2  float32    sqrt(mean |sec|^2)
+ *     coh   float32    |ifg| / (amp1 + 1e-12) / (amp2 + 1e-12); values > 1
+ *                      replaced by a uniform [0,1) value hashed from
+ *                      (fill_seed, output index)
+ *     phase float32    atan2(ifg)  (--out-float) */
+int s1b_crossmul_looks(const void *ref, int32_t ref_left, int32_t ref_top, int32_t ref_width,
+                       int32_t ref_height, const void *sec, int32_t sec_left, int32_t sec_top,
+                       int32_t sec_width, int32_t sec_height,
+                       int32_t left, int32_t top, int32_t nrow_ml, int32_t ncol_ml,
+                       int32_t rowlook, int32_t collook, void *ifg, float *amp1, float *amp2,
+                       float *coh, float *phase, uint64_t fill_seed, void *stream);
+
+/* Host only.  Intersection box of two cropped rasters aligned to the looks and
+ * the output header, as crossmul_daemon.cu:612-666 (union = 0) or the legacy
+ * crossmul.cu:191-213 (union = 1).  hdr1/hdr2: the 6 leading header words
+ * [nrow0, ncol0, left, top, right, bottom].  box_out: [left, top, right,
+ * bottom]; hdr_out: 6 words.  Returns S1B_ERR_EMPTY for an empty box. */
+int s1b_crossmul_box(const int32_t *hdr1, const int32_t *hdr2, int32_t rowlook,
+                     int32_t collook, int32_t use_union, int32_t *box_out,
+                     int32_t *hdr_out);
+
+/* ------------------------------------------------------------ Goldstein */
+
+/* Scratch bytes s1b_goldstein needs for an nrow x ncol image. */
+size_t s1b_goldstein_scratch_bytes(int32_t nrow, int32_t ncol, int32_t n_win);
+
+/* Goldstein filter of a complex64 image: n_win x n_win patches at step
+ * n_win/4, FFT, 7x7 circular smoothing of |F|, patch-mean normalisation,
+ * ^alpha weighting, inverse FFT, triangular-weight overlap-add.  Replaces
+ * goldstein_filter_cuda_host and its kernels, csrc/src/goldstein.cu:87-408.
+ * n_win must be 32 (the value s1proc uses) and nrow, ncol >= n_win.
+ * in/out: complex64 [nrow * ncol] device (must not alias);
+ * scratch: device buffer of s1b_goldstein_scratch_bytes(). */
+int s1b_goldstein(const void *in, void *out, int32_t nrow, int32_t ncol, int32_t n_win,
+                  float alpha, void *scratch, size_t scratch_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* S1B_H */

@@ -1,0 +1,166 @@
+// Crossmul + multilook + power looks + coherence in one pass on sm_100a.
+//
+// Replaces, for one burst pair, the reference's three kernels conj_mul,
+// cpx_col_look and cpx_row_look (csrc/src/sario.cu:199-286, launched at
+// crossmul_daemon.cu:921-975), point_angle (sario.cu:231-239) and the NumPy
+// amplitude multilook and coherence (s1proc/coherence.py:14-147,
+// s1proc/sario.py:397-420).  Both SLCs are read once; nothing full-size is
+// written.
+//
+// CTA = 256 threads = one multilooked row x M multilooked columns
+// (M * collook <= 512 full-resolution columns, more for very wide looks).
+// Threads read rows with coalesced 8-byte loads, sum the `rowlook` rows in
+// registers, stage per-column sums in shared memory, and M threads finish
+// the `collook` sums and the epilogue.
+#include <cuda_runtime.h>
+
+#include "s1b.h"
+#include "s1b_device.cuh"
+#include "s1b_internal.h"
+
+namespace {
+
+constexpr int XM_THREADS = 256;
+constexpr int XM_MAX_COLLOOK = 4096;
+
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+  // SplitMix64 (Steele, Lea, Flood, OOPSLA 2014)
+  x += 0x9E3779B97F4A7C15ull;
+  uint64_t z = x;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// Uniform [0, 1) fill for coherence values > 1 (the reference draws these
+// from an unseeded np.random.rand, s1proc/coherence.py:143-144).
+__device__ __forceinline__ float fill_uniform(uint64_t seed, uint64_t index) {
+  return (float)(splitmix64((seed << 32) + index) >> 40) * (1.0f / 16777216.0f);
+}
+
+struct XmArgs {
+  const float2 *ref;
+  const float2 *sec;
+  int64_t ref_off;  // element offset of global pixel (top, left) in ref
+  int64_t sec_off;
+  int32_t ref_width, sec_width;
+  int32_t nrow_ml, ncol_ml, rowlook, collook, m_per_cta;
+  float2 *ifg;
+  float *amp1, *amp2, *coh, *phase;
+  uint64_t seed;
+};
+
+__global__ __launch_bounds__(XM_THREADS) void crossmul_looks_kernel(const XmArgs a) {
+  extern __shared__ float4 smem4[];
+  const int W = a.m_per_cta * a.collook;  // full-res columns of this CTA
+  float2 *sI = reinterpret_cast<float2 *>(smem4);
+  float2 *sP = sI + W;  // (|ref|^2, |sec|^2) per column
+  const int i = blockIdx.x;
+  const int j0 = blockIdx.y * a.m_per_cta;
+  const int mcta = min(a.m_per_cta, a.ncol_ml - j0);
+  const int wcta = mcta * a.collook;
+  const int64_t col0 = (int64_t)j0 * a.collook;
+  const int64_t row0 = (int64_t)i * a.rowlook;
+  for (int c = threadIdx.x; c < wcta; c += XM_THREADS) {
+    float ir = 0.f, ii = 0.f, p1 = 0.f, p2 = 0.f;
+    const float2 *pr = a.ref + a.ref_off + row0 * a.ref_width + col0 + c;
+    const float2 *ps = a.sec + a.sec_off + row0 * a.sec_width + col0 + c;
+    for (int k = 0; k < a.rowlook; ++k) {
+      const float2 r = __ldg(pr);
+      const float2 s = __ldg(ps);
+      pr += a.ref_width;
+      ps += a.sec_width;
+      // conj(r) * s  (sario.cu:207-208)
+      ir += r.x * s.x + r.y * s.y;
+      ii += -r.y * s.x + r.x * s.y;
+      p1 += r.x * r.x + r.y * r.y;
+      p2 += s.x * s.x + s.y * s.y;
+    }
+    sI[c] = make_float2(ir, ii);
+    sP[c] = make_float2(p1, p2);
+  }
+  __syncthreads();
+  const float fcl = (float)a.collook, frl = (float)a.rowlook;
+  for (int m = threadIdx.x; m < mcta; m += XM_THREADS) {
+    float ir = 0.f, ii = 0.f, p1 = 0.f, p2 = 0.f;
+    const int base = m * a.collook;
+    for (int u = 0; u < a.collook; ++u) {
+      const float2 v = sI[base + u];
+      const float2 p = sP[base + u];
+      ir += v.x;
+      ii += v.y;
+      p1 += p.x;
+      p2 += p.y;
+    }
+    // mean over collook, then over rowlook, like cpx_col_look / cpx_row_look
+    ir = ir / fcl / frl;
+    ii = ii / fcl / frl;
+    const float am1 = sqrtf(p1 / fcl / frl);
+    const float am2 = sqrtf(p2 / fcl / frl);
+    const int64_t o = (int64_t)i * a.ncol_ml + j0 + m;
+    if (a.ifg) a.ifg[o] = make_float2(ir, ii);
+    if (a.amp1) a.amp1[o] = am1;
+    if (a.amp2) a.amp2[o] = am2;
+    if (a.coh) {
+      // s1proc/coherence.py:142-144
+      float c = hypotf(ir, ii) / (am1 + 1e-12f) / (am2 + 1e-12f);
+      if (c > 1.f) c = fill_uniform(a.seed, (uint64_t)o);
+      a.coh[o] = c;
+    }
+    if (a.phase) a.phase[o] = atan2f(ii, ir);
+  }
+}
+
+}  // namespace
+
+extern "C" int s1b_crossmul_looks(const void *ref, int32_t ref_left, int32_t ref_top,
+                                  int32_t ref_width, int32_t ref_height, const void *sec,
+                                  int32_t sec_left, int32_t sec_top, int32_t sec_width,
+                                  int32_t sec_height, int32_t left, int32_t top,
+                                  int32_t nrow_ml, int32_t ncol_ml, int32_t rowlook,
+                                  int32_t collook, void *ifg, float *amp1, float *amp2,
+                                  float *coh, float *phase, uint64_t fill_seed, void *stream) {
+  if (!ref || !sec) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_crossmul_looks: null input");
+  if (rowlook < 1 || collook < 1 || nrow_ml < 0 || ncol_ml < 0)
+    return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_crossmul_looks: bad looks or size");
+  if (collook > XM_MAX_COLLOOK)
+    return s1b_fail(S1B_ERR_TOO_LARGE, "s1b_crossmul_looks: collook above 4096");
+  if (left < ref_left || left < sec_left || top < ref_top || top < sec_top)
+    return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_crossmul_looks: box outside the rasters");
+  if ((int64_t)left + (int64_t)ncol_ml * collook > (int64_t)ref_left + ref_width ||
+      (int64_t)left + (int64_t)ncol_ml * collook > (int64_t)sec_left + sec_width)
+    return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_crossmul_looks: box wider than the rasters");
+  if ((int64_t)top + (int64_t)nrow_ml * rowlook > (int64_t)ref_top + ref_height ||
+      (int64_t)top + (int64_t)nrow_ml * rowlook > (int64_t)sec_top + sec_height)
+    return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_crossmul_looks: box taller than the rasters");
+  if (nrow_ml == 0 || ncol_ml == 0) return S1B_OK;
+  XmArgs a;
+  a.ref = (const float2 *)ref;
+  a.sec = (const float2 *)sec;
+  a.ref_off = (int64_t)(top - ref_top) * ref_width + (left - ref_left);
+  a.sec_off = (int64_t)(top - sec_top) * sec_width + (left - sec_left);
+  a.ref_width = ref_width;
+  a.sec_width = sec_width;
+  a.nrow_ml = nrow_ml;
+  a.ncol_ml = ncol_ml;
+  a.rowlook = rowlook;
+  a.collook = collook;
+  a.m_per_cta = collook >= 512 ? 1 : 512 / collook;
+  a.ifg = (float2 *)ifg;
+  a.amp1 = amp1;
+  a.amp2 = amp2;
+  a.coh = coh;
+  a.phase = phase;
+  a.seed = fill_seed;
+  const size_t smem = (size_t)a.m_per_cta * collook * 2 * sizeof(float2);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(crossmul_looks_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return s1b_fail(S1B_ERR_CUDA, cudaGetErrorString(e));
+  }
+  const int nchunk = (ncol_ml + a.m_per_cta - 1) / a.m_per_cta;
+  if (nchunk > 65535) return s1b_fail(S1B_ERR_TOO_LARGE, "s1b_crossmul_looks: too many columns");
+  dim3 grid(nrow_ml, nchunk);
+  crossmul_looks_kernel<<<grid, XM_THREADS, smem, (cudaStream_t)stream>>>(a);
+  return s1b_launch_status();
+}

@@ -1,0 +1,266 @@
+// geo2rdr on sm_100a: TOPS deramp, and per-DEM-pixel FP64 zero-Doppler
+// geocoding with bilinear resampling, reramp and range phase.
+//
+// Replaces csrc/src/geo2rdr.cu:86-248 (deramp_burst, reproject,
+// find_first_last_nonzero_rows_kernel) of the reference.  Differences in
+// method (same results within FP64 rounding):
+//   * the orbit is a per-window degree-7 polynomial evaluated by Horner
+//     (s1b_orbit_poly_t) instead of the Lagrange-form Hermite with ~60
+//     divisions per call;
+//   * the zero-Doppler Newton uses the exact derivative (3 steps instead of
+//     7-11);
+//   * llh->ECEF trigonometry is computed once per DEM row / column per CTA;
+//   * FP64 phases are reduced mod 2 pi in FP64, then rotated in FP32;
+//   * the non-zero-row search is folded into the geocoding epilogue.
+#include <cuda_runtime.h>
+
+#include "s1b.h"
+#include "s1b_device.cuh"
+#include "s1b_internal.h"
+
+namespace {
+
+constexpr double kRaD = 6378137.0;
+constexpr double kRe2D = 0.00669437999015;
+
+// ------------------------------------------------------------------ deramp
+// CTA: 256 threads x 2 columns = 512 columns, DERAMP_ROWS rows.  Per-column
+// TOPS coefficients are formed once per thread and reused down the rows.
+constexpr int DERAMP_ROWS = 16;
+
+template <bool kVec>
+__global__ __launch_bounds__(256) void deramp_kernel(const __grid_constant__ s1b_burst_plan_t P,
+                                                     const float2 *__restrict__ in,
+                                                     float2 *__restrict__ out) {
+  const int S = P.samples, L = P.lines;
+  const int c0 = (blockIdx.x * 256 + threadIdx.x) * 2;
+  if (c0 >= S) return;
+  const int r0 = blockIdx.y * DERAMP_ROWS;
+  // geo2rdr.cu:533-541 for the thread's two columns: -pi*kt and etaref
+  double mkt[2], etaref[2];
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const int c = c0 + j < S ? c0 + j : c0;
+    const double tr = P.slant_range_time + c / P.range_sampling_rate;
+    double dt = tr - P.fm[0];
+    const double ka = P.fm[1] + dt * (P.fm[2] + P.fm[3] * dt);
+    dt = tr - P.dc[0];
+    const double fnc = P.dc[1] + dt * (P.dc[2] + P.dc[3] * dt);
+    const double kt = ka * P.ks / (ka - P.ks);
+    mkt[j] = -kPiD * kt;
+    etaref[j] = -fnc / ka - P.etac0;
+  }
+  const bool two = (c0 + 1) < S;
+  const double eta0 = -L * P.ati / 2.;
+#pragma unroll 4
+  for (int rr = 0; rr < DERAMP_ROWS; ++rr) {
+    const int r = r0 + rr;
+    if (r >= L) break;
+    const double eta = eta0 + r * P.ati;  // geo2rdr.cu:530-531
+    const size_t base = (size_t)r * S + c0;
+    float2 a0, a1;
+    if (kVec) {
+      const float4 v = __ldcs(reinterpret_cast<const float4 *>(in + base));
+      a0 = make_float2(v.x, v.y);
+      a1 = make_float2(v.z, v.w);
+    } else {
+      a0 = __ldcs(in + base);
+      a1 = two ? __ldcs(in + base + 1) : make_float2(0.f, 0.f);
+    }
+    const double d0 = eta - etaref[0];
+    const double d1 = eta - etaref[1];
+    const float2 b0 = cmul(a0, phasor(mkt[0] * d0 * d0));
+    const float2 b1 = cmul(a1, phasor(mkt[1] * d1 * d1));
+    if (kVec) {
+      __stcs(reinterpret_cast<float4 *>(out + base), make_float4(b0.x, b0.y, b1.x, b1.y));
+    } else {
+      __stcs(out + base, b0);
+      if (two) __stcs(out + base + 1, b1);
+    }
+  }
+}
+
+// ----------------------------------------------------------------- geo2rdr
+// CTA tile: 32 columns x 8 rows of the DEM window, one pixel per thread.
+constexpr int G_TX = 32, G_TY = 8;
+
+__global__ void rows_init_kernel(int32_t *rows, int nrow) {
+  rows[0] = nrow;
+  rows[1] = -1;
+}
+
+__global__ __launch_bounds__(G_TX *G_TY) void geo2rdr_kernel(
+    const __grid_constant__ s1b_burst_plan_t P, const int16_t *__restrict__ dem, int64_t pitch,
+    const float2 *__restrict__ burst, float2 *__restrict__ out, int32_t *__restrict__ rows,
+    int nrow, int ncol) {
+  __shared__ double s_row[G_TY][3];  // sinlat, coslat, re (per row)
+  __shared__ double s_col[G_TX][2];  // sinlon, coslon (per column)
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int col = blockIdx.x * G_TX + tx;
+  const int row = blockIdx.y * G_TY + ty;
+  const int tid = ty * G_TX + tx;
+  // llh->ECEF trigonometry (orbit.cu:20-27) once per row / column of the tile
+  if (tid < G_TY) {
+    const int r = blockIdx.y * G_TY + tid;
+    const double lat = (P.lat0 + r * P.dlat) * kPiD / 180;
+    double s, c;
+    sincos(lat, &s, &c);
+    s_row[tid][0] = s;
+    s_row[tid][1] = c;
+    s_row[tid][2] = kRaD / sqrt(1. - kRe2D * s * s);
+  } else if (tid >= 32 && tid < 32 + G_TX) {
+    const int c_ = blockIdx.x * G_TX + (tid - 32);
+    const double lon = (P.lon0 + c_ * P.dlon) * kPiD / 180;
+    double s, c;
+    sincos(lon, &s, &c);
+    s_col[tid - 32][0] = s;
+    s_col[tid - 32][1] = c;
+  }
+  __syncthreads();
+  const bool inb = (col < ncol) && (row < nrow);
+  float2 res = make_float2(0.f, 0.f);
+  if (inb) {
+    const double h = (double)__ldg(dem + (int64_t)row * pitch + col);
+    const double sinlat = s_row[ty][0], coslat = s_row[ty][1], re = s_row[ty][2];
+    const double sinlon = s_col[tx][0], coslon = s_col[tx][1];
+    double p[3];
+    p[0] = (re + h) * coslat * coslon;
+    p[1] = (re + h) * coslat * sinlon;
+    p[2] = (re * (1 - kRe2D) + h) * sinlat;
+    // zero-Doppler solve seeded at the burst centre (geo2rdr.cu:588-600)
+    double t = P.tmid;
+    OrbitState st;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      st.x[i] = P.xmid[i];
+      st.v[i] = P.vmid[i];
+      st.a[i] = P.amid[i];
+    }
+    double dr[3];
+    zero_doppler(P.orbit, p, t, st, dr);
+    const double rng = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+    const double rgoff = (rng - P.rngstart) / P.dmrg;
+    const double azoff = (t - P.tstart) / P.dtaz;
+    // validity window, geo2rdr.cu:208-209
+    bool valid = rgoff > P.first_valid_sample && rgoff < P.last_valid_sample - 1 &&
+                 azoff >= P.first_valid_line + 5 && azoff < P.last_valid_line - 5;
+    const int intr = (int)rgoff, inta = (int)azoff;
+    // the 2x2 neighbourhood must lie inside the burst even if the validity
+    // limits passed in exceed the raster
+    valid = valid && intr >= 0 && intr + 1 < P.samples && inta >= 0 && inta + 1 < P.lines;
+    if (valid) {
+      // per-pixel TOPS reramp (geo2rdr.cu:210-219)
+      const double tr = rng * 2 / kSolD;
+      double dt = tr - P.fm[0];
+      const double ka = P.fm[1] + dt * (P.fm[2] + P.fm[3] * dt);
+      dt = tr - P.dc[0];
+      const double fnc = P.dc[1] + dt * (P.dc[2] + P.dc[3] * dt);
+      const double kt = ka * P.ks / (ka - P.ks);
+      const double etaref = -fnc / ka - P.etac0;
+      const double eta = -P.lines * P.dtaz / 2. + t - P.tstart;
+      const double ed = eta - etaref;
+      const double reramp = -kPiD * kt * ed * ed;
+      // bilinear interpolation of the deramped burst (geo2rdr.cu:220-237)
+      const float fr = (float)(rgoff - intr), fa = (float)(azoff - inta);
+      const size_t i1 = (size_t)inta * P.samples + intr;
+      const float2 b1 = __ldg(burst + i1), b2 = __ldg(burst + i1 + 1);
+      const float2 b3 = __ldg(burst + i1 + P.samples), b4 = __ldg(burst + i1 + P.samples + 1);
+      const float2 c1 = make_float2(fmaf(fr, b2.x - b1.x, b1.x), fmaf(fr, b2.y - b1.y, b1.y));
+      const float2 c2 = make_float2(fmaf(fr, b4.x - b3.x, b3.x), fmaf(fr, b4.y - b3.y, b3.y));
+      const float2 v = make_float2(fmaf(fa, c2.x - c1.x, c1.x), fmaf(fa, c2.y - c1.y, c1.y));
+      // range phase and reramp (geo2rdr.cu:238-243)
+      res = cmul(v, phasor(P.k4pi_wvl * rng - reramp));
+    }
+    __stcs(out + (size_t)row * ncol + col, res);
+  }
+  // first / last non-zero output row (geo2rdr.cu:86-128): one vote per warp
+  const unsigned nz = __ballot_sync(0xffffffffu, inb && (res.x != 0.f || res.y != 0.f));
+  if (nz && tx == 0 && rows) {
+    atomicMin(rows, row);
+    atomicMax(rows + 1, row + 1);
+  }
+}
+
+// ------------------------------------------------- generic geometry kernels
+__global__ void zero_doppler_kernel(const __grid_constant__ s1b_orbit_poly_t P, const double *xyz,
+                                    int64_t n, double t0, double *tline, double *drout) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double p[3] = {xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]};
+  double t = t0;
+  OrbitState st;
+  orbit_eval(P, t, st);
+  double dr[3];
+  zero_doppler(P, p, t, st, dr);
+  tline[i] = t;
+  if (drout) {
+    drout[3 * i] = dr[0];
+    drout[3 * i + 1] = dr[1];
+    drout[3 * i + 2] = dr[2];
+  }
+}
+
+__global__ void llh2xyz_kernel(const double *llh, double *xyz, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double lat = llh[3 * i] * kPiD / 180, lon = llh[3 * i + 1] * kPiD / 180, h = llh[3 * i + 2];
+  double sl, cl, so, co;
+  sincos(lat, &sl, &cl);
+  sincos(lon, &so, &co);
+  const double re = kRaD / sqrt(1. - kRe2D * sl * sl);
+  xyz[3 * i] = (re + h) * cl * co;
+  xyz[3 * i + 1] = (re + h) * cl * so;
+  xyz[3 * i + 2] = (re * (1 - kRe2D) + h) * sl;
+}
+
+}  // namespace
+
+extern "C" int s1b_deramp(const s1b_burst_plan_t *plan, const void *in, void *out, void *stream) {
+  if (!plan || !in || !out) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_deramp: null argument");
+  const int S = plan->samples, L = plan->lines;
+  if (S < 1 || L < 1) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_deramp: empty burst");
+  cudaStream_t st = (cudaStream_t)stream;
+  dim3 grid((S + 511) / 512, (L + DERAMP_ROWS - 1) / DERAMP_ROWS);
+  const bool vec = (S % 2 == 0) && ((uintptr_t)in % 16 == 0) && ((uintptr_t)out % 16 == 0);
+  if (vec)
+    deramp_kernel<true><<<grid, 256, 0, st>>>(*plan, (const float2 *)in, (float2 *)out);
+  else
+    deramp_kernel<false><<<grid, 256, 0, st>>>(*plan, (const float2 *)in, (float2 *)out);
+  return s1b_launch_status();
+}
+
+extern "C" int s1b_geo2rdr(const s1b_burst_plan_t *plan, const int16_t *dem, int64_t dem_pitch,
+                           const void *deramped, void *out, int32_t *rows, void *stream) {
+  if (!plan || !dem || !deramped || !out)
+    return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_geo2rdr: null argument");
+  const int nrow = plan->win_bottom - plan->win_top;
+  const int ncol = plan->win_right - plan->win_left;
+  if (nrow <= 0 || ncol <= 0) return s1b_fail(S1B_ERR_EMPTY, "s1b_geo2rdr: empty DEM window");
+  if (dem_pitch < ncol) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_geo2rdr: dem_pitch < window width");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (rows) {
+    rows_init_kernel<<<1, 1, 0, st>>>(rows, nrow);
+    int s = s1b_launch_status();
+    if (s) return s;
+  }
+  dim3 block(G_TX, G_TY);
+  dim3 grid((ncol + G_TX - 1) / G_TX, (nrow + G_TY - 1) / G_TY);
+  geo2rdr_kernel<<<grid, block, 0, st>>>(*plan, dem, dem_pitch, (const float2 *)deramped,
+                                         (float2 *)out, rows, nrow, ncol);
+  return s1b_launch_status();
+}
+
+extern "C" int s1b_zero_doppler(const s1b_orbit_poly_t *orbit, const double *xyz, int64_t n,
+                                double tline0, double *tline, double *dr, void *stream) {
+  if (!orbit || (n > 0 && (!xyz || !tline))) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_zero_doppler: null argument");
+  if (n <= 0) return S1B_OK;
+  zero_doppler_kernel<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(*orbit, xyz, n, tline0, tline, dr);
+  return s1b_launch_status();
+}
+
+extern "C" int s1b_llh2xyz(const double *llh, double *xyz, int64_t n, void *stream) {
+  if (n > 0 && (!llh || !xyz)) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_llh2xyz: null argument");
+  if (n <= 0) return S1B_OK;
+  llh2xyz_kernel<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(llh, xyz, n);
+  return s1b_launch_status();
+}

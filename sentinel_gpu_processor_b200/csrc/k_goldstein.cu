@@ -1,0 +1,266 @@
+// Goldstein phase filter on sm_100a.
+//
+// Replaces goldstein_filter_cuda_host and its kernels (extract_patches,
+// cuFFT forward, gaussian_filter, patchwise_normalize, spectrum_enhancement,
+// cuFFT inverse, batched_overlap_add, normalize_output), reference
+// csrc/src/goldstein.cu:87-408, with two kernels:
+//   1. goldstein_patch_kernel -- one warp per 32x32 patch: coalesced patch
+//      load into shared memory, 2-D FFT as 32-point radix-2 FFTs held in
+//      registers (rows, then columns through a padded shared tile), |F|,
+//      7x7 circular smoothing, patch-mean normalisation, S^alpha weighting,
+//      inverse 2-D FFT, triangular weight and 1/n^2 scale; the weighted patch
+//      is written to scratch.
+//   2. goldstein_gather_kernel -- one thread per output pixel sums the (up to
+//      16) weighted patches covering it in a fixed order and divides by the
+//      summed weights.  No atomics: the result is deterministic.
+#include <cuda_runtime.h>
+
+#include "s1b.h"
+#include "s1b_device.cuh"
+#include "s1b_internal.h"
+
+namespace {
+
+constexpr int GN = 32;        // patch size (s1proc filter.window_size)
+constexpr int GSTEP = GN / 4; // patch step, goldstein.cu:334
+constexpr int GWARPS = 4;     // patches per CTA
+
+// exp(2 pi i k / 32), k = 0..15, from cos/sin of 2 pi k / 32 evaluated in
+// 50-digit decimal arithmetic.
+__constant__ float2 c_tw[16] = {
+    {1.0f, 0.0f},
+    {0.9807852804032304f, 0.19509032201612828f},
+    {0.9238795325112867f, 0.3826834323650898f},
+    {0.8314696123025452f, 0.5555702330196022f},
+    {0.7071067811865476f, 0.7071067811865476f},
+    {0.5555702330196022f, 0.8314696123025452f},
+    {0.3826834323650898f, 0.9238795325112867f},
+    {0.19509032201612828f, 0.9807852804032304f},
+    {0.0f, 1.0f},
+    {-0.19509032201612828f, 0.9807852804032304f},
+    {-0.3826834323650898f, 0.9238795325112867f},
+    {-0.5555702330196022f, 0.8314696123025452f},
+    {-0.7071067811865476f, 0.7071067811865476f},
+    {-0.8314696123025452f, 0.5555702330196022f},
+    {-0.9238795325112867f, 0.3826834323650898f},
+    {-0.9807852804032304f, 0.19509032201612828f},
+};
+
+// The reference project's 7x7 smoothing table, goldstein.cu:43-52 (row
+// ky = -3..3, column kx = -3..3).  Kept as given: the filter output depends
+// on these exact values.
+__constant__ float c_gauss[49] = {
+    0.000004f, 0.000088f, 0.000543f, 0.000948f, 0.000543f, 0.000088f, 0.000004f,
+    0.000088f, 0.001915f, 0.011776f, 0.020584f, 0.011776f, 0.001915f, 0.000088f,
+    0.000543f, 0.011776f, 0.072410f, 0.126584f, 0.072410f, 0.011776f, 0.000543f,
+    0.000948f, 0.020584f, 0.126584f, 0.221141f, 0.126584f, 0.020584f, 0.000948f,
+    0.000543f, 0.011776f, 0.072410f, 0.126584f, 0.072410f, 0.011776f, 0.000543f,
+    0.000088f, 0.001915f, 0.011776f, 0.020584f, 0.011776f, 0.001915f, 0.000088f,
+    0.000004f, 0.000088f, 0.000543f, 0.000948f, 0.000543f, 0.000088f, 0.000004f};
+
+__host__ __device__ constexpr int brev5(int i) {
+  return ((i & 1) << 4) | ((i & 2) << 2) | (i & 4) | ((i & 8) >> 2) | ((i & 16) >> 4);
+}
+
+// In-place 32-point DFT of x (natural order in and out), radix-2
+// decimation in time.  Forward: exp(-2 pi i jk/32); inverse: exp(+...),
+// unnormalised (cuFFT's convention).
+template <bool kInverse>
+__device__ __forceinline__ void fft32(float2 (&x)[GN]) {
+#pragma unroll
+  for (int i = 0; i < GN; ++i) {
+    const int j = brev5(i);
+    if (j > i) {
+      const float2 t = x[i];
+      x[i] = x[j];
+      x[j] = t;
+    }
+  }
+#pragma unroll
+  for (int s = 1; s <= 5; ++s) {
+    const int m = 1 << s, half = m >> 1, stride = GN / m;
+#pragma unroll
+    for (int k = 0; k < GN; k += m) {
+#pragma unroll
+      for (int j = 0; j < half; ++j) {
+        float2 w = c_tw[j * stride];
+        if (!kInverse) w.y = -w.y;
+        const float2 b = x[k + j + half];
+        const float2 t = make_float2(w.x * b.x - w.y * b.y, w.x * b.y + w.y * b.x);
+        const float2 u = x[k + j];
+        x[k + j] = make_float2(u.x + t.x, u.y + t.y);
+        x[k + j + half] = make_float2(u.x - t.x, u.y - t.y);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ float tri_weight(int t) {  // goldstein.cu:257-258
+  return (float)(t < GN / 2 ? t : GN - 1 - t);
+}
+
+__device__ __forceinline__ int patch_origin(int p, int n) {  // goldstein.cu:308-313
+  const int o = p * GSTEP;
+  return o + GN > n ? n - GN : o;
+}
+
+__global__ __launch_bounds__(32 * GWARPS) void goldstein_patch_kernel(
+    const float2 *__restrict__ in, float2 *__restrict__ patches, int nrow, int ncol, int n_win_i,
+    int n_win_j, float alpha) {
+  // one padded 32x33 tile per warp; |F| reuses it once the column FFT
+  // inputs have been read into registers
+  __shared__ float2 sT[GWARPS][GN][GN + 1];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int p = blockIdx.x * GWARPS + warp;
+  if (p >= n_win_i * n_win_j) return;  // warp-uniform; only __syncwarp below
+  const int i1 = patch_origin(p / n_win_j, nrow);
+  const int j1 = patch_origin(p % n_win_j, ncol);
+  float2(*T)[GN + 1] = sT[warp];
+  float(*M)[GN + 1] = reinterpret_cast<float(*)[GN + 1]>(&sT[warp][0][0]);
+#pragma unroll 8
+  for (int r = 0; r < GN; ++r) T[r][lane] = __ldg(in + (size_t)(i1 + r) * ncol + j1 + lane);
+  __syncwarp();
+  float2 x[GN];
+  // forward FFT along rows (lane = row)
+#pragma unroll
+  for (int c = 0; c < GN; ++c) x[c] = T[lane][c];
+  fft32<false>(x);
+  __syncwarp();
+#pragma unroll
+  for (int c = 0; c < GN; ++c) T[lane][c] = x[c];
+  __syncwarp();
+  // forward FFT along columns (lane = column kx); x[ky] = F[ky][kx]
+#pragma unroll
+  for (int r = 0; r < GN; ++r) x[r] = T[r][lane];
+  fft32<false>(x);
+  __syncwarp();
+#pragma unroll
+  for (int r = 0; r < GN; ++r) M[r][lane] = hypotf(x[r].x, x[r].y);
+  __syncwarp();
+  // 7x7 circular smoothing of |F| (goldstein.cu:105-119) and its patch sum
+  float S[GN];
+  float psum = 0.f;
+#pragma unroll
+  for (int y = 0; y < GN; ++y) {
+    float s = 0.f;
+#pragma unroll
+    for (int ky = -3; ky <= 3; ++ky) {
+#pragma unroll
+      for (int kx = -3; kx <= 3; ++kx)
+        s += M[(y + ky + GN) & (GN - 1)][(lane + kx + GN) & (GN - 1)] * c_gauss[(ky + 3) * 7 + kx + 3];
+    }
+    S[y] = s;
+    psum += s;
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) psum += __shfl_xor_sync(0xffffffffu, psum, off);
+  // patch-mean normalisation and S^alpha weighting (goldstein.cu:125-176)
+  const float mean = psum / (float)(GN * GN);
+  const bool ok = mean > 1e-8f;
+  const float inv = 1.0f / mean;
+#pragma unroll
+  for (int y = 0; y < GN; ++y) {
+    const float w = powf(ok ? S[y] * inv : 0.0f, alpha);
+    if (w > 0.0f) {
+      x[y].x *= w;
+      x[y].y *= w;
+    }
+  }
+  // inverse FFT along columns, then rows
+  fft32<true>(x);
+  __syncwarp();
+#pragma unroll
+  for (int y = 0; y < GN; ++y) T[y][lane] = x[y];
+  __syncwarp();
+#pragma unroll
+  for (int c = 0; c < GN; ++c) x[c] = T[lane][c];
+  fft32<true>(x);
+  // triangular weight and 1/n^2 (goldstein.cu:257-269); stage for a
+  // coalesced store
+  const float wy = tri_weight(lane);
+  const float norm = 1.0f / (float)(GN * GN);
+  __syncwarp();
+#pragma unroll
+  for (int c = 0; c < GN; ++c) {
+    const float w = (tri_weight(c) + wy) * norm;
+    T[lane][c] = make_float2(x[c].x * w, x[c].y * w);
+  }
+  __syncwarp();
+  float2 *dst = patches + (size_t)p * (GN * GN);
+#pragma unroll 8
+  for (int r = 0; r < GN; ++r) __stcg(dst + r * GN + lane, T[r][lane]);
+}
+
+__global__ __launch_bounds__(256) void goldstein_gather_kernel(const float2 *__restrict__ patches,
+                                                               float2 *__restrict__ out, int nrow,
+                                                               int ncol, int n_win_i, int n_win_j) {
+  const int y = blockIdx.x;
+  const int x = blockIdx.y * 256 + threadIdx.x;
+  if (x >= ncol) return;
+  float ax = 0.f, ay = 0.f, wsum = 0.f;
+  const int pi0 = y >= GN - 1 ? (y - (GN - 1) + GSTEP - 1) / GSTEP : 0;
+  const int pj0 = x >= GN - 1 ? (x - (GN - 1) + GSTEP - 1) / GSTEP : 0;
+  for (int pi = pi0; pi < n_win_i; ++pi) {
+    const int i1 = patch_origin(pi, nrow);
+    if (i1 > y) break;
+    if (y >= i1 + GN) continue;
+    const int ty = y - i1;
+    const float wy = tri_weight(ty);
+    for (int pj = pj0; pj < n_win_j; ++pj) {
+      const int j1 = patch_origin(pj, ncol);
+      if (j1 > x) break;
+      if (x >= j1 + GN) continue;
+      const int tx = x - j1;
+      const float2 v = __ldcg(patches + ((size_t)pi * n_win_j + pj) * (GN * GN) + ty * GN + tx);
+      ax += v.x;
+      ay += v.y;
+      wsum += tri_weight(tx) + wy;
+    }
+  }
+  if (wsum > 0.f) {  // goldstein.cu:287-291
+    ax /= wsum;
+    ay /= wsum;
+  }
+  out[(size_t)y * ncol + x] = make_float2(ax, ay);
+}
+
+void patch_grid(int nrow, int ncol, int &n_win_i, int &n_win_j) {  // goldstein.cu:335-340
+  n_win_i = (int)ceilf((float)nrow / GSTEP) - 3;
+  n_win_j = (int)ceilf((float)ncol / GSTEP) - 3;
+  if (n_win_i <= 0) n_win_i = 1;
+  if (n_win_j <= 0) n_win_j = 1;
+}
+
+}  // namespace
+
+extern "C" size_t s1b_goldstein_scratch_bytes(int32_t nrow, int32_t ncol, int32_t n_win) {
+  if (n_win != GN || nrow < GN || ncol < GN) return 0;
+  int ni, nj;
+  patch_grid(nrow, ncol, ni, nj);
+  return (size_t)ni * nj * GN * GN * sizeof(float2);
+}
+
+extern "C" int s1b_goldstein(const void *in, void *out, int32_t nrow, int32_t ncol, int32_t n_win,
+                             float alpha, void *scratch, size_t scratch_bytes, void *stream) {
+  if (!in || !out) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_goldstein: null argument");
+  if (n_win != GN) return s1b_fail(S1B_ERR_UNSUPPORTED, "s1b_goldstein: only n_win = 32 is implemented");
+  if (nrow < GN || ncol < GN)
+    return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_goldstein: image smaller than the window");
+  const size_t need = s1b_goldstein_scratch_bytes(nrow, ncol, n_win);
+  if (!scratch || scratch_bytes < need)
+    return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_goldstein: scratch buffer too small");
+  int ni, nj;
+  patch_grid(nrow, ncol, ni, nj);
+  const int64_t npatch = (int64_t)ni * nj;
+  if ((npatch + GWARPS - 1) / GWARPS > 0x7fffffff || (ncol + 255) / 256 > 65535)
+    return s1b_fail(S1B_ERR_TOO_LARGE, "s1b_goldstein: image too large");
+  cudaStream_t st = (cudaStream_t)stream;
+  goldstein_patch_kernel<<<(unsigned)((npatch + GWARPS - 1) / GWARPS), 32 * GWARPS, 0, st>>>(
+      (const float2 *)in, (float2 *)scratch, nrow, ncol, ni, nj, alpha);
+  int s = s1b_launch_status();
+  if (s) return s;
+  dim3 grid(nrow, (ncol + 255) / 256);
+  goldstein_gather_kernel<<<grid, 256, 0, st>>>((const float2 *)scratch, (float2 *)out, nrow, ncol,
+                                                ni, nj);
+  return s1b_launch_status();
+}

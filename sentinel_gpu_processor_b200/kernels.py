@@ -1,0 +1,146 @@
+"""Torch-facing wrappers of the s1b device entry points.
+
+Each function takes CUDA tensors, launches on the current torch stream and
+returns CUDA tensors.  They raise ``S1BError`` on any failure and
+``RuntimeError`` when given CPU tensors: there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _lib
+
+
+def _need_cuda(*ts):
+    for t in ts:
+        if t is not None and not t.is_cuda:
+            raise RuntimeError("s1b kernels take CUDA tensors only (no CPU fallback)")
+
+
+def _c64(t, name):
+    if t.dtype != torch.complex64 or not t.is_contiguous():
+        raise ValueError(f"{name} must be a contiguous complex64 tensor")
+
+
+def deramp(plan: _lib.BurstPlan, slc: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+    """TOPS deramp (reference deramp_burst, geo2rdr.cu:138-158)."""
+    _need_cuda(slc, out)
+    _c64(slc, "slc")
+    if slc.numel() != plan.lines * plan.samples:
+        raise ValueError("slc size does not match the plan")
+    if out is None:
+        out = torch.empty_like(slc)
+    lib = _lib.load()
+    _lib.check(lib.s1b_deramp(ctypes.byref(plan), _lib.dptr(slc), _lib.dptr(out), _lib.stream_ptr()),
+               "s1b_deramp")
+    return out
+
+
+def geo2rdr(plan: _lib.BurstPlan, dem: torch.Tensor, deramped: torch.Tensor, out: torch.Tensor | None = None,
+            rows: torch.Tensor | None = None):
+    """Geocode a deramped burst onto the plan's DEM window.
+
+    ``dem`` is either the full RSC-grid DEM [nlat, nlon] (the window is taken
+    from it without a copy) or the window itself [nrow, ncol] (int16).
+    Returns (out complex64 [nrow, ncol], rows int32 [2] = first, last_excl).
+    """
+    _need_cuda(dem, deramped, out, rows)
+    _c64(deramped, "deramped")
+    if dem.dtype != torch.int16:
+        raise ValueError("dem must be int16")
+    nrow, ncol = plan.nrow, plan.ncol
+    if nrow <= 0 or ncol <= 0:
+        raise _lib.S1BError(_lib.S1B_ERR_EMPTY, "geo2rdr")
+    if dem.shape == (plan.rsc_nlat, plan.rsc_nlon) and (dem.shape != (nrow, ncol) or
+                                                         (plan.win_top, plan.win_left) != (0, 0)):
+        win = dem[plan.win_top:plan.win_bottom, plan.win_left:plan.win_right]
+    else:
+        win = dem
+    if tuple(win.shape) != (nrow, ncol) or win.stride(1) != 1:
+        raise ValueError("dem does not cover the plan's window")
+    if out is None:
+        out = torch.empty((nrow, ncol), dtype=torch.complex64, device=deramped.device)
+    if rows is None:
+        rows = torch.empty(2, dtype=torch.int32, device=deramped.device)
+    lib = _lib.load()
+    _lib.check(lib.s1b_geo2rdr(ctypes.byref(plan), _lib.dptr(win), win.stride(0), _lib.dptr(deramped),
+                               _lib.dptr(out), _lib.dptr(rows), _lib.stream_ptr()), "s1b_geo2rdr")
+    return out, rows
+
+
+def crossmul_looks(ref, ref_box, sec, sec_box, box, rowlook, collook, want=("ifg", "amp1", "amp2", "coh"),
+                   fill_seed=0):
+    """Fused crossmul + looks + power looks + coherence.
+
+    ref/sec: complex64 [h, w] rasters whose (top, left) global coordinates are
+    ``ref_box[:2]`` = (left, top) as (left, top, right, bottom) tuples;
+    ``box`` = aligned (left, top, right, bottom).  Returns a dict of outputs.
+    """
+    _need_cuda(ref, sec)
+    _c64(ref, "ref")
+    _c64(sec, "sec")
+    left, top, right, bottom = box
+    nrow_ml = (bottom - top) // rowlook
+    ncol_ml = (right - left) // collook
+    dev = ref.device
+    outs = {}
+    shape = (nrow_ml, ncol_ml)
+    if "ifg" in want:
+        outs["ifg"] = torch.empty(shape, dtype=torch.complex64, device=dev)
+    for k in ("amp1", "amp2", "coh", "phase"):
+        if k in want:
+            outs[k] = torch.empty(shape, dtype=torch.float32, device=dev)
+    lib = _lib.load()
+    _lib.check(lib.s1b_crossmul_looks(
+        _lib.dptr(ref), ref_box[0], ref_box[1], ref.shape[1], ref.shape[0],
+        _lib.dptr(sec), sec_box[0], sec_box[1], sec.shape[1], sec.shape[0],
+        left, top, nrow_ml, ncol_ml, rowlook, collook,
+        _lib.dptr(outs.get("ifg")), _lib.dptr(outs.get("amp1")), _lib.dptr(outs.get("amp2")),
+        _lib.dptr(outs.get("coh")), _lib.dptr(outs.get("phase")), int(fill_seed), _lib.stream_ptr()),
+        "s1b_crossmul_looks")
+    return outs
+
+
+def goldstein_scratch_bytes(nrow, ncol, n_win=32):
+    return int(_lib.load().s1b_goldstein_scratch_bytes(nrow, ncol, n_win))
+
+
+def goldstein(img: torch.Tensor, alpha: float, n_win: int = 32, out: torch.Tensor | None = None,
+              scratch: torch.Tensor | None = None) -> torch.Tensor:
+    """Goldstein filter (reference goldstein.cu:328-408) of a complex64 image."""
+    _need_cuda(img, out, scratch)
+    _c64(img, "img")
+    nrow, ncol = img.shape
+    need = goldstein_scratch_bytes(nrow, ncol, n_win)
+    if scratch is None:
+        scratch = torch.empty(max(need, 1), dtype=torch.uint8, device=img.device)
+    if out is None:
+        out = torch.empty_like(img)
+    lib = _lib.load()
+    _lib.check(lib.s1b_goldstein(_lib.dptr(img), _lib.dptr(out), nrow, ncol, n_win, float(alpha),
+                                 _lib.dptr(scratch), scratch.numel() * scratch.element_size(),
+                                 _lib.stream_ptr()), "s1b_goldstein")
+    return out
+
+
+def zero_doppler(poly: _lib.OrbitPoly, xyz: torch.Tensor, tline0: float):
+    """Zero-Doppler time and line-of-sight vector for ECEF points [n, 3] (float64)."""
+    _need_cuda(xyz)
+    xyz = xyz.contiguous().to(torch.float64)
+    n = xyz.shape[0]
+    t = torch.empty(n, dtype=torch.float64, device=xyz.device)
+    dr = torch.empty((n, 3), dtype=torch.float64, device=xyz.device)
+    _lib.check(_lib.load().s1b_zero_doppler(ctypes.byref(poly), _lib.dptr(xyz), n, float(tline0), _lib.dptr(t),
+                                            _lib.dptr(dr), _lib.stream_ptr()), "s1b_zero_doppler")
+    return t, dr
+
+
+def llh2xyz(llh: torch.Tensor) -> torch.Tensor:
+    _need_cuda(llh)
+    llh = llh.contiguous().to(torch.float64)
+    out = torch.empty_like(llh)
+    _lib.check(_lib.load().s1b_llh2xyz(_lib.dptr(llh), _lib.dptr(out), llh.shape[0], _lib.stream_ptr()),
+               "s1b_llh2xyz")
+    return out

@@ -1,0 +1,471 @@
+"""Seeded synthetic Sentinel-1 IW scenes.
+
+The reference benchmarks on real Sentinel-1 data that cannot be used here;
+these generators stand in for it with the shapes, geometry and value
+distributions of the workload: a C-band radar (lambda = 0.05546576 m, range
+spacing 2.329562 m, azimuth interval 2.055556e-3 s, near range 8.0e5 m), a
+circular orbit at 693 km and 7.6 km/s sampled by 11 state vectors 10 s
+apart, a secondary orbit offset by a perpendicular baseline, fractal (fBm,
+H = 0.8) terrain on a 1/7200-degree lat/lon grid, circular-Gaussian speckle
+and TOPS azimuth modulation with a chosen Doppler rate.
+
+Everything here is host-side input preparation.  Tensors are made with torch
+(CPU or CUDA) so that large scenes are generated on the device.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import formats
+
+SOL = 299792458.0
+RA = 6378137.0
+RE2 = 0.00669437999015
+
+WAVELENGTH = 0.05546576
+RANGE_SPACING = 2.329562
+AZIMUTH_INTERVAL = 2.055556e-3
+NEAR_RANGE = 8.0e5
+ALTITUDE = 693.0e3
+SPEED = 7600.0
+INCLINATION_DEG = 98.18
+ORBIT_T0 = 50000.0
+ORBIT_DT = 10.0
+ORBIT_N = 11
+GEO_STEP = 1.0 / 7200.0
+
+
+@dataclass
+class Radar:
+    """Per-subswath radar parameters (the keys geo2rdr reads, geo2rdr.cu:333-376)."""
+    samples_per_burst: int
+    lines_per_burst: int
+    prf: float
+    wvl: float
+    hmin: float
+    hmax: float
+    range_sampling_rate: float
+    slant_range_time: float
+    azimuth_steering_rate: float
+    azimuth_time_interval: float
+    radar_frequency: float
+
+
+@dataclass
+class Burst:
+    azimuth_time: float
+    first_valid_line: int
+    last_valid_line: int
+    first_valid_sample: int
+    last_valid_sample: int
+
+
+@dataclass
+class Acquisition:
+    """One SLC (one date) of one subswath: radar, orbit, FM/DC tables, bursts."""
+    radar: Radar
+    orbit: tuple  # (tt [n], xx [n,3], vv [n,3]) float64
+    fm: np.ndarray  # [n, 5] (time, t0, c0, c1, c2)
+    dc: np.ndarray
+    bursts: list
+
+
+@dataclass
+class PairScene:
+    """A reference/secondary pair of bursts over one DEM grid."""
+    name: str
+    seed: int
+    ref: list  # list[Acquisition], one per burst group (per burst for uneven sizes)
+    sec: list
+    rsc: formats.Rsc
+    dem: object  # torch int16 [nlat, nlon]
+    ref_slc: list  # list of torch complex64 [L, S] per burst (TOPS-modulated)
+    sec_slc: list
+    rowlook: int
+    collook: int
+    alpha: float
+    n_win: int = 32
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def burst_pixels(self):
+        return sum(int(s.shape[0]) * int(s.shape[1]) for s in self.ref_slc)
+
+
+# ----------------------------------------------------------------------------
+# Small geodesy helpers (numpy) for scene layout
+# ----------------------------------------------------------------------------
+
+def _llh2xyz(lat, lon, h):
+    lat = np.radians(lat)
+    lon = np.radians(lon)
+    re = RA / np.sqrt(1.0 - RE2 * np.sin(lat) ** 2)
+    return np.stack([(re + h) * np.cos(lat) * np.cos(lon), (re + h) * np.cos(lat) * np.sin(lon),
+                     (re * (1 - RE2) + h) * np.sin(lat)], axis=-1)
+
+
+def _xyz2llh(xyz):
+    x, y, z = xyz[..., 0], xyz[..., 1], xyz[..., 2]
+    lon = np.arctan2(y, x)
+    p = np.hypot(x, y)
+    lat = np.arctan2(z, p * (1 - RE2))
+    for _ in range(6):
+        n = RA / np.sqrt(1 - RE2 * np.sin(lat) ** 2)
+        h = p / np.cos(lat) - n
+        lat = np.arctan2(z, p * (1 - RE2 * n / (n + h)))
+    n = RA / np.sqrt(1 - RE2 * np.sin(lat) ** 2)
+    h = p / np.cos(lat) - n
+    return np.degrees(lat), np.degrees(lon), h
+
+
+def make_orbit(lat_c=35.0, lon_c=10.0, t_c=ORBIT_T0 + 50.0, altitude=ALTITUDE, speed=SPEED,
+               n=ORBIT_N, dt=ORBIT_DT, t0=ORBIT_T0, inclination=INCLINATION_DEG, offset=(0.0, 0.0, 0.0)):
+    """Circular ECEF orbit through the sub-satellite point (lat_c, lon_c) at t_c, ascending."""
+    r = RA + altitude
+    inc = math.radians(inclination)
+    u_c = math.asin(math.sin(math.radians(lat_c)) / math.sin(inc))
+    # longitude of the node such that the sub-satellite longitude at u_c is lon_c
+    dl = math.atan2(math.cos(inc) * math.sin(u_c), math.cos(u_c))
+    om = math.radians(lon_c) - dl
+    e1 = np.array([math.cos(om), math.sin(om), 0.0])
+    e2 = np.array([-math.cos(inc) * math.sin(om), math.cos(inc) * math.cos(om), math.sin(inc)])
+    w = speed / r
+    tt = t0 + dt * np.arange(n, dtype=np.float64)
+    u = u_c + w * (tt - t_c)
+    xx = r * (np.cos(u)[:, None] * e1 + np.sin(u)[:, None] * e2) + np.asarray(offset)[None, :]
+    vv = r * w * (-np.sin(u)[:, None] * e1 + np.cos(u)[:, None] * e2)
+    return tt, xx, vv
+
+
+def _orbit_at(orbit, t):
+    tt, xx, vv = orbit
+    # the orbit is a circle: interpolate the angle exactly from two samples
+    k = int(np.clip(np.searchsorted(tt, t) - 1, 0, len(tt) - 2))
+    a = (t - tt[k]) / (tt[k + 1] - tt[k])
+    p0, p1 = xx[k], xx[k + 1]
+    v0 = vv[k]
+    r = np.linalg.norm(p0)
+    ang = math.acos(np.clip(np.dot(p0, p1) / (r * np.linalg.norm(p1)), -1, 1))
+    e1 = p0 / r
+    e2 = v0 / np.linalg.norm(v0)
+    th = a * ang
+    p = r * (math.cos(th) * e1 + math.sin(th) * e2)
+    v = np.linalg.norm(v0) * (-math.sin(th) * e1 + math.cos(th) * e2)
+    return p, v
+
+
+def rdr2geo(orbit, t, rng, h):
+    """Ground point (lat, lon) at zero Doppler, slant range ``rng``, height ``h``, right-looking."""
+    p, v = _orbit_at(orbit, t)
+    lat, lon, _ = _xyz2llh(p)
+    n_hat = -np.array([math.cos(math.radians(lat)) * math.cos(math.radians(lon)),
+                       math.cos(math.radians(lat)) * math.sin(math.radians(lon)),
+                       math.sin(math.radians(lat))])
+    c_hat = np.cross(n_hat, v)
+    c_hat /= np.linalg.norm(c_hat)
+    n2 = np.cross(v, c_hat)
+    n2 /= np.linalg.norm(n2)  # down direction orthogonal to v
+    lo, hi = 0.0, math.radians(85.0)
+    for _ in range(80):
+        th = 0.5 * (lo + hi)
+        g = p + rng * (math.cos(th) * n2 + math.sin(th) * c_hat)
+        _, _, hg = _xyz2llh(g)
+        if hg > h:  # the look ray rises with the angle: too far out
+            hi = th
+        else:
+            lo = th
+    g = p + rng * (math.cos(th) * n2 + math.sin(th) * c_hat)
+    la, lo_, _ = _xyz2llh(g)
+    return float(la), float(lo_), th
+
+
+# ----------------------------------------------------------------------------
+# Radar, TOPS tables, bursts
+# ----------------------------------------------------------------------------
+
+def make_radar(lines, samples, near_range=NEAR_RANGE, steering_rate=1.590368784, hmin=-100.0, hmax=3100.0):
+    ati = AZIMUTH_INTERVAL
+    return Radar(samples_per_burst=int(samples), lines_per_burst=int(lines), prf=1.0 / ati,
+                 wvl=WAVELENGTH, hmin=float(hmin), hmax=float(hmax),
+                 range_sampling_rate=SOL / (2.0 * RANGE_SPACING),
+                 slant_range_time=2.0 * near_range / SOL, azimuth_steering_rate=float(steering_rate),
+                 azimuth_time_interval=ati, radar_frequency=SOL / WAVELENGTH)
+
+
+def tops_tables(radar: Radar, t_c: float, kt_target: float, vs: float = SPEED):
+    """FM-rate and Doppler-centroid tables whose kt at near range, burst centre, is ``kt_target``.
+
+    ks = 2 vs f0 / c * steering_rate * pi / 180 (geo2rdr.cu:482-483) and the
+    reference forms kt = ka ks / (ka - ks) (geo2rdr.cu:539), so the FM rate
+    is ka = kt ks / (kt - ks).  Three table entries around the burst centre
+    with small coefficient changes exercise the time interpolation.
+    """
+    ks = 2.0 * vs * radar.radar_frequency / SOL * radar.azimuth_steering_rate * math.pi / 180.0
+    ka = kt_target * ks / (kt_target - ks)
+    swath_t = radar.samples_per_burst / radar.range_sampling_rate
+    t0 = radar.slant_range_time
+    fm, dc = [], []
+    for k, dtk in enumerate((-2.75, 0.25, 3.25)):
+        s = 1.0 + 0.002 * (k - 1)
+        fm.append([t_c + dtk, t0, ka * s, 0.02 * ka / swath_t, 0.0])
+        dc.append([t_c + dtk, t0, 30.0 * s, -4.0e4, 1.0e6])
+    return np.asarray(fm), np.asarray(dc)
+
+
+def burst_meta(t_start, lines, samples, margin_l=24, margin_s=40):
+    return Burst(azimuth_time=float(t_start), first_valid_line=margin_l, last_valid_line=lines - margin_l,
+                 first_valid_sample=margin_s, last_valid_sample=samples - margin_s)
+
+
+def tops_coefficients(acq: Acquisition, burst: Burst):
+    """kt[S], etaref[S], eta[L] of a burst (the host formulas of geo2rdr.cu:469-542)."""
+    r = acq.radar
+    L, S = r.lines_per_burst, r.samples_per_burst
+    tc = burst.azimuth_time + L * r.azimuth_time_interval / 2
+    vs = SPEED
+    ks = 2.0 * vs * r.radar_frequency / SOL * r.azimuth_steering_rate * math.pi / 180.0
+
+    def interp(tab):
+        i = int(np.argmin(np.abs(tab[:, 0] - tc)))
+        if tab[i, 0] < tc and i < len(tab) - 1:
+            f = (tc - tab[i, 0]) / (tab[i + 1, 0] - tab[i, 0])
+            return tab[i, 1:] + f * (tab[i + 1, 1:] - tab[i, 1:])
+        if tab[i, 0] > tc and i > 0:
+            f = (tc - tab[i - 1, 0]) / (tab[i, 0] - tab[i - 1, 0])
+            return tab[i - 1, 1:] + f * (tab[i, 1:] - tab[i - 1, 1:])
+        return tab[i, 1:].copy()
+
+    fm = interp(acq.fm)
+    dc = interp(acq.dc)
+    tr = r.slant_range_time + np.arange(S) / r.range_sampling_rate
+    ka = fm[1] + (tr - fm[0]) * (fm[2] + fm[3] * (tr - fm[0]))
+    fnc = dc[1] + (tr - dc[0]) * (dc[2] + dc[3] * (tr - dc[0]))
+    kt = ka * ks / (ka - ks)
+    etac = -fnc / ka
+    etaref = etac - etac[0]
+    eta = -L * r.azimuth_time_interval / 2.0 + np.arange(L) * r.azimuth_time_interval
+    return kt, etaref, eta
+
+
+# ----------------------------------------------------------------------------
+# Terrain and speckle (torch)
+# ----------------------------------------------------------------------------
+
+def _hash01(ix, iy, octave, seed, torch):
+    """Uniform [0,1) lattice values from a 32-bit integer hash (Wang/Jenkins style mixing)."""
+    h = (ix * 374761393 + iy * 668265263 + octave * 2147483647 + seed * 1274126177) & 0xFFFFFFFF
+    h = ((h ^ (h >> 13)) * 1274126177) & 0xFFFFFFFF
+    h = (h ^ (h >> 16)) & 0xFFFFFFFF
+    return h.to(torch.float32) * (1.0 / 4294967296.0)
+
+
+def fbm_height(lat, lon, seed, hmax, H=0.8, base_deg=0.2, octaves=9):
+    """Fractal terrain in [0, hmax] m evaluated at (lat, lon) degrees (torch float64 tensors).
+
+    Sum of value-noise octaves with amplitude 2^(-k H) (fBm with Hurst
+    exponent H); lattice values come from a hash of the global lattice index,
+    so any window of the globe is generated consistently.
+    """
+    import torch
+    acc = torch.zeros_like(lat, dtype=torch.float32)
+    norm = 0.0
+    for k in range(octaves):
+        cell = base_deg / (2 ** k)
+        u = lat / cell
+        v = lon / cell
+        iu = torch.floor(u)
+        iv = torch.floor(v)
+        fu = (u - iu).to(torch.float32)
+        fv = (v - iv).to(torch.float32)
+        fu = fu * fu * (3 - 2 * fu)
+        fv = fv * fv * (3 - 2 * fv)
+        iu = iu.to(torch.int64)
+        iv = iv.to(torch.int64)
+        v00 = _hash01(iu, iv, k, seed, torch)
+        v10 = _hash01(iu + 1, iv, k, seed, torch)
+        v01 = _hash01(iu, iv + 1, k, seed, torch)
+        v11 = _hash01(iu + 1, iv + 1, k, seed, torch)
+        n = (v00 * (1 - fu) * (1 - fv) + v10 * fu * (1 - fv) + v01 * (1 - fu) * fv + v11 * fu * fv)
+        a = 2.0 ** (-k * H)
+        acc += a * (n - 0.5)
+        norm += a
+    z = acc / norm
+    z = (z - z.min()) / max(float(z.max() - z.min()), 1e-6)
+    return z * hmax
+
+
+def make_dem(rsc: formats.Rsc, seed, hmax, device="cpu"):
+    import torch
+    lat = rsc.latmax + rsc.dlat * torch.arange(rsc.nlat, dtype=torch.float64, device=device)[:, None]
+    lon = rsc.lonmin + rsc.dlon * torch.arange(rsc.nlon, dtype=torch.float64, device=device)[None, :]
+    lat, lon = torch.broadcast_tensors(lat, lon)
+    h = fbm_height(lat, lon, seed, hmax)
+    return torch.round(h).to(torch.int16).contiguous()
+
+
+def speckle(lines, samples, gen, device):
+    import torch
+    z = torch.randn((lines, samples, 2), generator=gen, device=device, dtype=torch.float32)
+    z *= math.sqrt(0.5)
+    return torch.view_as_complex(z)
+
+
+def tops_modulate(slc, acq: Acquisition, burst: Burst, sign=+1.0):
+    """Multiply by exp(sign * i pi kt (eta - etaref)^2) (inverse of the deramp)."""
+    import torch
+    kt, etaref, eta = tops_coefficients(acq, burst)
+    dev = slc.device
+    kt = torch.as_tensor(kt, dtype=torch.float64, device=dev)
+    etaref = torch.as_tensor(etaref, dtype=torch.float64, device=dev)
+    eta = torch.as_tensor(eta, dtype=torch.float64, device=dev)
+    d = eta[:, None] - etaref[None, :]
+    ph = sign * math.pi * kt[None, :] * d * d
+    ph = torch.remainder(ph, 2 * math.pi).to(torch.float32)
+    return slc * torch.polar(torch.ones_like(ph), ph)
+
+
+# ----------------------------------------------------------------------------
+# Scenes
+# ----------------------------------------------------------------------------
+
+CONFIGS = {
+    # name: (lines, samples, rowlook, collook, alpha, hmax, kt)
+    "tiny": (96, 320, 2, 4, 0.5, 800.0, -1500.0),
+    "small": (160, 640, 2, 8, 0.5, 1500.0, -1500.0),
+    "c0": (512, 2048, 2, 8, 0.5, 1500.0, -1500.0),
+    "c1": (1500, 21000, 4, 20, 0.6, 3000.0, -1500.0),
+}
+
+
+def _look_angle(r_sat, rng):
+    re = RA
+    return math.acos((r_sat ** 2 + rng ** 2 - re ** 2) / (2 * r_sat * rng))
+
+
+def secondary_offset(orbit, t_c, near_range, baseline):
+    """ECEF offset of ``baseline`` metres perpendicular to the velocity and to the mid-swath look vector."""
+    p, v = _orbit_at(orbit, t_c)
+    n_hat = -p / np.linalg.norm(p)
+    c_hat = np.cross(n_hat, v)
+    c_hat /= np.linalg.norm(c_hat)
+    th = _look_angle(np.linalg.norm(p), near_range)
+    b_hat = -math.sin(th) * n_hat + math.cos(th) * c_hat
+    return baseline * b_hat
+
+
+def footprint_rsc(acqs, hmin, hmax, margin=0.08, step=GEO_STEP):
+    """RSC grid (1/7200 degree) covering every burst footprint, with a margin."""
+    lats, lons = [], []
+    for acq in acqs:
+        r = acq.radar
+        for b in acq.bursts:
+            t0 = b.azimuth_time
+            t1 = t0 + (r.lines_per_burst - 1) * r.azimuth_time_interval
+            r0 = r.slant_range_time * SOL / 2
+            r1 = r0 + (r.samples_per_burst - 1) * SOL / 2 / r.range_sampling_rate
+            for t in (t0, t1):
+                for rg in (r0, r1):
+                    for h in (hmin, hmax):
+                        la, lo, _ = rdr2geo(acq.orbit, t, rg, h)
+                        lats.append(la)
+                        lons.append(lo)
+    la0, la1 = min(lats), max(lats)
+    lo0, lo1 = min(lons), max(lons)
+    dla = (la1 - la0) * margin
+    dlo = (lo1 - lo0) * margin
+    latmax = la1 + dla
+    lonmin = lo0 - dlo
+    nlat = int(math.ceil((la1 - la0 + 2 * dla) / step)) + 1
+    nlon = int(math.ceil((lo1 - lo0 + 2 * dlo) / step)) + 1
+    return formats.rsc_roundtrip(formats.Rsc(nlat=nlat, nlon=nlon, latmax=latmax, lonmin=lonmin,
+                                             dlat=-step, dlon=step))
+
+
+def make_pair(config="c0", seed=20261203, device="cpu", baseline=150.0, coherence=0.7,
+              lines=None, samples=None, rowlook=None, collook=None, alpha=None):
+    """A one-burst reference/secondary pair (configs 'tiny', 'small', 'c0', 'c1')."""
+    import torch
+    L, S, rl, cl, al, hmax, kt = CONFIGS[config]
+    L = int(lines or L)
+    S = int(samples or S)
+    rl = int(rowlook or rl)
+    cl = int(collook or cl)
+    al = float(alpha if alpha is not None else al)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    t_c = ORBIT_T0 + 50.0 + float(rng.uniform(-1.0, 1.0))
+    orbit_ref = make_orbit(t_c=ORBIT_T0 + 50.0)
+    off = secondary_offset(orbit_ref, t_c, NEAR_RANGE + S * RANGE_SPACING / 2, baseline)
+    orbit_sec = make_orbit(t_c=ORBIT_T0 + 50.0, offset=off)
+    hmin_db, hmax_db = -100.0, hmax + 100.0
+    radar = make_radar(L, S, hmin=hmin_db, hmax=hmax_db)
+    t_start = t_c - L * AZIMUTH_INTERVAL / 2
+    fm, dc = tops_tables(radar, t_c, kt)
+    burst = burst_meta(t_start, L, S)
+    ref = Acquisition(radar=radar, orbit=orbit_ref, fm=fm, dc=dc, bursts=[burst])
+    sec = Acquisition(radar=radar, orbit=orbit_sec, fm=fm.copy(), dc=dc.copy(), bursts=[burst])
+    rsc = footprint_rsc([ref, sec], 0.0, hmax)
+    dem = make_dem(rsc, seed, hmax, device=device)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    s_ref = speckle(L, S, gen, device)
+    noise = speckle(L, S, gen, device)
+    s_sec = coherence * s_ref + math.sqrt(1 - coherence ** 2) * noise
+    ref_slc = tops_modulate(s_ref, ref, burst).contiguous()
+    sec_slc = tops_modulate(s_sec, sec, burst).contiguous()
+    return PairScene(name=config, seed=seed, ref=[ref], sec=[sec], rsc=rsc, dem=dem,
+                     ref_slc=[ref_slc], sec_slc=[sec_slc], rowlook=rl, collook=cl, alpha=al)
+
+
+def make_frame(seed=20261203, device="cpu", n_swaths=3, n_bursts=9, baseline=150.0,
+               line_range=(1480, 1530), sample_range=(20000, 25500), overlap=100,
+               kt_range=(-1700.0, -1400.0), coh_range=(0.3, 0.9), rowlook=4, collook=20,
+               alpha=0.5, hmax=3000.0, scale=1.0):
+    """A full IW frame: ``n_swaths`` x ``n_bursts`` bursts of uneven size.
+
+    Each burst is its own Acquisition (the reference handles one burst size
+    per subswath run).  ``scale`` shrinks line/sample counts for tests.
+    """
+    import torch
+    rng = np.random.Generator(np.random.PCG64(seed))
+    orbit_ref = make_orbit(t_c=ORBIT_T0 + 50.0)
+    near = [NEAR_RANGE, NEAR_RANGE + 4.6e4, NEAR_RANGE + 9.2e4]
+    steer = [1.590368784, 0.979863325, 1.397440818]
+    refs, secs, ref_slc, sec_slc, cohs = [], [], [], [], []
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    acq_dur = 0.0
+    for sw in range(n_swaths):
+        kt = float(rng.uniform(*kt_range))
+        off = secondary_offset(orbit_ref, ORBIT_T0 + 50.0, near[sw] + 2.6e4, baseline)
+        orbit_sec = make_orbit(t_c=ORBIT_T0 + 50.0, offset=off)
+        t = ORBIT_T0 + 50.0 - 0.5 * n_bursts * 2.75
+        for b in range(n_bursts):
+            L = int(round(rng.integers(line_range[0], line_range[1] + 1) * scale))
+            S = int(round(rng.integers(sample_range[0], sample_range[1] + 1) * scale))
+            L = max(L, 64)
+            S = max(S, 128)
+            radar = make_radar(L, S, near_range=near[sw], steering_rate=steer[sw], hmin=-100.0, hmax=hmax + 100.0)
+            t_c = t + L * AZIMUTH_INTERVAL / 2
+            fm, dc = tops_tables(radar, t_c, kt)
+            burst = burst_meta(t, L, S)
+            ref = Acquisition(radar=radar, orbit=orbit_ref, fm=fm, dc=dc, bursts=[burst])
+            sec = Acquisition(radar=radar, orbit=orbit_sec, fm=fm.copy(), dc=dc.copy(), bursts=[burst])
+            g = float(rng.uniform(*coh_range))
+            s_ref = speckle(L, S, gen, device)
+            noise = speckle(L, S, gen, device)
+            s_sec = g * s_ref + math.sqrt(1 - g * g) * noise
+            refs.append(ref)
+            secs.append(sec)
+            ref_slc.append(tops_modulate(s_ref, ref, burst).contiguous())
+            sec_slc.append(tops_modulate(s_sec, sec, burst).contiguous())
+            cohs.append(g)
+            t += (L - int(overlap * scale)) * AZIMUTH_INTERVAL
+            acq_dur = max(acq_dur, t)
+    rsc = footprint_rsc(refs + secs, 0.0, hmax, margin=0.02)
+    dem = make_dem(rsc, seed, hmax, device=device)
+    return PairScene(name="frame", seed=seed, ref=refs, sec=secs, rsc=rsc, dem=dem, ref_slc=ref_slc,
+                     sec_slc=sec_slc, rowlook=rowlook, collook=collook, alpha=alpha,
+                     extra={"coherence": cohs})

@@ -1,0 +1,161 @@
+"""geo2rdr parity on the GPU: deramp, zero-Doppler geocoding, crop rows,
+against the float64 oracle (oracle/geo2rdr.py) on seeded synthetic bursts.
+
+Tolerances (north star): RMS wrapped-phase difference <= 1e-3 rad,
+geo2rdr offsets <= 1e-4 px.  Measured errors are far below them; the
+assertions use the stated bounds and a tighter amplitude bound.
+"""
+import numpy as np
+import pytest
+import torch
+
+from helpers import oracle_burst, oracle_radar, oracle_rsc, phase_rms, rel_err
+from oracle import geo2rdr as og2
+from oracle import geometry as og
+from sentinel_gpu_processor_b200 import _lib, geo2rdr, kernels, plan as P, synth
+
+pytestmark = pytest.mark.gpu
+
+PHASE_TOL = 1e-3  # rad, RMS
+OFFSET_TOL = 1e-4  # px
+
+
+def _scene(cfg, seed, **kw):
+    return synth.make_pair(cfg, seed=seed, **kw)
+
+
+@pytest.mark.parametrize("cfg,seed", [("tiny", 3), ("small", 4)])
+def test_deramp_matches_oracle(cuda, cfg, seed):
+    sc = _scene(cfg, seed)
+    acq = sc.ref[0]
+    pl = P.burst_plan(acq.radar, acq.orbit, acq.fm, acq.dc, acq.bursts[0], sc.rsc)
+    slc = sc.ref_slc[0]
+    got = kernels.deramp(pl, slc.to(cuda)).cpu().numpy()
+    co = og2.burst_coefficients(oracle_radar(acq.radar), acq.orbit, acq.fm, acq.dc, oracle_burst(acq.bursts[0]))
+    want = og2.deramp(slc.numpy(), co)
+    assert phase_rms(got, want) < 2e-6
+    assert rel_err(np.abs(got), np.abs(want)) < 1e-6
+
+
+def test_deramp_inplace_and_odd_width(cuda):
+    sc = _scene("tiny", 5, samples=321)  # odd width: scalar path
+    acq = sc.ref[0]
+    pl = P.burst_plan(acq.radar, acq.orbit, acq.fm, acq.dc, acq.bursts[0], sc.rsc)
+    slc = sc.ref_slc[0].to(cuda)
+    ref = kernels.deramp(pl, slc.clone()).cpu().numpy()
+    x = slc.clone()
+    kernels.deramp(pl, x, out=x)
+    np.testing.assert_array_equal(x.cpu().numpy(), ref)
+    co = og2.burst_coefficients(oracle_radar(acq.radar), acq.orbit, acq.fm, acq.dc, oracle_burst(acq.bursts[0]))
+    assert phase_rms(ref, og2.deramp(sc.ref_slc[0].numpy(), co)) < 2e-6
+
+
+def _oracle_geocode(sc, acq, slc):
+    r = oracle_radar(acq.radar)
+    b = oracle_burst(acq.bursts[0])
+    rsc = oracle_rsc(sc.rsc)
+    return og2.geo2rdr_burst(slc, sc.dem.numpy(), rsc, r, acq.orbit, acq.fm, acq.dc, b)
+
+
+@pytest.mark.parametrize("cfg,seed,which", [("tiny", 11, "ref"), ("tiny", 12, "sec"), ("small", 13, "ref")])
+def test_geocode_burst_matches_oracle(cuda, cfg, seed, which):
+    sc = _scene(cfg, seed)
+    acq = getattr(sc, which)[0]
+    slc = (sc.ref_slc if which == "ref" else sc.sec_slc)[0]
+    pl = P.burst_plan(acq.radar, acq.orbit, acq.fm, acq.dc, acq.bursts[0], sc.rsc)
+    got = geo2rdr.geocode_burst(pl, slc.to(cuda), sc.dem.to(cuda))
+    want = _oracle_geocode(sc, acq, slc.numpy())
+    assert got is not None and want is not None
+    gh, gd = got
+    wh, wd = want
+    # crop rows may differ only if a boundary pixel flips validity
+    assert abs(int(gh[3]) - int(wh[3])) <= 1 and abs(int(gh[5]) - int(wh[5])) <= 1
+    np.testing.assert_array_equal(gh[[0, 1, 2, 4]], wh[[0, 1, 2, 4]])
+    top = max(int(gh[3]), int(wh[3]))
+    bot = min(int(gh[5]), int(wh[5]))
+    g = gd.cpu().numpy()[top - int(gh[3]):bot - int(gh[3])]
+    w = wd[top - int(wh[3]):bot - int(wh[3])]
+    gm = np.abs(g) > 0
+    wm = np.abs(w) > 0
+    assert (gm != wm).mean() < 1e-3  # validity masks agree except boundary pixels
+    both = gm & wm
+    assert both.sum() > 0.3 * both.size
+    assert phase_rms(g, w, both) < PHASE_TOL
+    assert rel_err(np.abs(g), np.abs(w), both) < 1e-4
+
+
+def test_zero_doppler_offsets_match_oracle(cuda):
+    sc = _scene("small", 21)
+    acq = sc.ref[0]
+    pl = P.burst_plan(acq.radar, acq.orbit, acq.fm, acq.dc, acq.bursts[0], sc.rsc)
+    rng = np.random.default_rng(0)
+    n = 4000
+    lat = pl.latlon_box[0] + rng.uniform(0, 1, n) * (pl.latlon_box[1] - pl.latlon_box[0])
+    lon = pl.latlon_box[2] + rng.uniform(0, 1, n) * (pl.latlon_box[3] - pl.latlon_box[2])
+    h = rng.uniform(-100, 3000, n)
+    llh = np.stack([lat, lon, h], -1)
+    xyz_g = kernels.llh2xyz(torch.from_numpy(llh).to(cuda)).cpu().numpy()
+    xyz_o = og.llh2xyz(llh)
+    assert np.abs(xyz_g - xyz_o).max() < 1e-6  # metres
+    t_g, dr_g = kernels.zero_doppler(pl.orbit, torch.from_numpy(xyz_o).to(cuda), pl.tmid)
+    tt, xx, vv = acq.orbit
+    xm, vm = og.intp_orbit(tt, xx, vv, np.float64(pl.tmid))
+    t_o, dr_o, _ = og.orbitrangetime(tt, xx, vv, xyz_o, pl.tmid, xm, vm)
+    az_err = np.abs(t_g.cpu().numpy() - t_o) / pl.dtaz
+    rg_err = np.abs(np.linalg.norm(dr_g.cpu().numpy(), axis=1) - np.linalg.norm(dr_o, axis=1)) / pl.dmrg
+    assert az_err.max() < OFFSET_TOL
+    assert rg_err.max() < OFFSET_TOL
+
+
+def test_geocode_deterministic(cuda):
+    sc = _scene("tiny", 31)
+    acq = sc.ref[0]
+    pl = P.burst_plan(acq.radar, acq.orbit, acq.fm, acq.dc, acq.bursts[0], sc.rsc)
+    a = geo2rdr.geocode_burst(pl, sc.ref_slc[0].to(cuda), sc.dem.to(cuda))
+    b = geo2rdr.geocode_burst(pl, sc.ref_slc[0].to(cuda), sc.dem.to(cuda))
+    np.testing.assert_array_equal(a[0], b[0])
+    assert torch.equal(a[1], b[1])
+
+
+def test_geocode_window_clipped_by_grid(cuda):
+    """A DEM grid that covers only part of the footprint: the window is
+    clamped (geo2rdr.cu:579-582) and results still match the oracle."""
+    sc = _scene("tiny", 41)
+    full = sc.rsc
+    # keep the northern half of the grid only
+    from sentinel_gpu_processor_b200 import formats
+    half = formats.Rsc(nlat=full.nlat // 2, nlon=full.nlon, latmax=full.latmax, lonmin=full.lonmin,
+                       dlat=full.dlat, dlon=full.dlon)
+    dem = sc.dem[:half.nlat].contiguous()
+    acq = sc.ref[0]
+    pl = P.burst_plan(acq.radar, acq.orbit, acq.fm, acq.dc, acq.bursts[0], half)
+    assert pl.win_bottom == half.nlat
+    got = geo2rdr.geocode_burst(pl, sc.ref_slc[0].to(cuda), dem.to(cuda))
+    want = og2.geo2rdr_burst(sc.ref_slc[0].numpy(), dem.numpy(), oracle_rsc(half), oracle_radar(acq.radar),
+                             acq.orbit, acq.fm, acq.dc, oracle_burst(acq.bursts[0]))
+    assert (got is None) == (want is None)
+    if got is not None:
+        assert abs(int(got[0][3]) - int(want[0][3])) <= 1
+
+
+def test_geocode_empty_window_raises(cuda):
+    sc = _scene("tiny", 51)
+    from sentinel_gpu_processor_b200 import formats
+    far = formats.Rsc(nlat=50, nlon=50, latmax=sc.rsc.latmax + 5.0, lonmin=sc.rsc.lonmin, dlat=sc.rsc.dlat,
+                      dlon=sc.rsc.dlon)
+    acq = sc.ref[0]
+    pl = P.burst_plan(acq.radar, acq.orbit, acq.fm, acq.dc, acq.bursts[0], far)
+    assert pl.nrow <= 0 or pl.ncol <= 0
+    assert geo2rdr.geocode_burst(pl, sc.ref_slc[0].to(cuda), torch.zeros((50, 50), dtype=torch.int16,
+                                                                          device=cuda)) is None
+    with pytest.raises(_lib.S1BError):
+        kernels.geo2rdr(pl, torch.zeros((50, 50), dtype=torch.int16, device=cuda),
+                        torch.zeros(pl.lines * pl.samples, dtype=torch.complex64, device=cuda))
+
+
+def test_cpu_tensors_rejected(cuda):
+    sc = _scene("tiny", 61)
+    acq = sc.ref[0]
+    pl = P.burst_plan(acq.radar, acq.orbit, acq.fm, acq.dc, acq.bursts[0], sc.rsc)
+    with pytest.raises(RuntimeError):
+        kernels.deramp(pl, sc.ref_slc[0].reshape(-1))
