@@ -1,0 +1,137 @@
+"""The per-burst-pair interferogram chain on one GPU:
+
+    deramp(ref), deramp(sec) -> geo2rdr(ref), geo2rdr(sec) onto the DEM grid
+    -> crossmul + multilook + amplitude looks + coherence -> Goldstein
+
+This is what the reference runs as ``geo2rdr`` (twice), ``crossmul_daemon``,
+NumPy ``coherence`` and ``goldstein`` with files in between
+(s1proc/sentinel_scene.py, interfere.py, coherence.py, phase_correction.py).
+Buffers are allocated once per burst geometry and reused, so a step only
+launches kernels; the one host synchronisation per pair reads the four crop
+rows that size the interferogram (as the reference reads them back before
+writing the ``.gslc`` header).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib, formats, kernels, plan as _plan
+
+
+@dataclass
+class PairResult:
+    header: np.ndarray  # ifg header, int32[64]
+    box: tuple          # full-resolution box (left, top, right, bottom)
+    ifg: torch.Tensor   # complex64 [nrow_ml, ncol_ml]
+    amp1: torch.Tensor
+    amp2: torch.Tensor
+    coh: torch.Tensor
+    filt: torch.Tensor  # Goldstein-filtered ifg
+    gslc_headers: tuple
+
+
+class PairChain:
+    """Plans and device buffers for one reference/secondary burst pair."""
+
+    def __init__(self, ref_acq, sec_acq, rsc, rowlook, collook, alpha, n_win=32, device="cuda", burst=0,
+                 fill_seed=0):
+        self.rowlook, self.collook, self.alpha, self.n_win = int(rowlook), int(collook), float(alpha), int(n_win)
+        self.fill_seed = int(fill_seed)
+        self.dev = torch.device(device)
+        self.plans = [_plan.burst_plan(a.radar, a.orbit, a.fm, a.dc, a.bursts[burst], rsc) for a in (ref_acq, sec_acq)]
+        for p in self.plans:
+            if p.nrow <= 0 or p.ncol <= 0:
+                raise _lib.S1BError(_lib.S1B_ERR_EMPTY, "PairChain: burst outside the DEM grid")
+        L, S = self.plans[0].lines, self.plans[0].samples
+        self.deramped = [torch.empty(p.lines * p.samples, dtype=torch.complex64, device=self.dev) for p in self.plans]
+        self.geo = [torch.empty((p.nrow, p.ncol), dtype=torch.complex64, device=self.dev) for p in self.plans]
+        self.rows = torch.empty(4, dtype=torch.int32, device=self.dev)
+        self.rows_host = torch.empty(4, dtype=torch.int32, pin_memory=True)
+        self.burst_pixels = L * S
+        self._scratch = None
+        self._ml_shape = None
+
+    def geocode(self, ref_slc: torch.Tensor, sec_slc: torch.Tensor, dem: torch.Tensor):
+        for i, (p, slc) in enumerate(zip(self.plans, (ref_slc, sec_slc))):
+            kernels.deramp(p, slc.reshape(-1), out=self.deramped[i])
+            kernels.geo2rdr(p, dem, self.deramped[i], out=self.geo[i], rows=self.rows[2 * i:2 * i + 2])
+
+    def headers(self):
+        """Crop rows -> the two ``.gslc`` headers (geo2rdr.cu:641-647), or None if a burst is empty."""
+        self.rows_host.copy_(self.rows, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        r = self.rows_host.tolist()
+        hs = []
+        for i, p in enumerate(self.plans):
+            first, last = r[2 * i], r[2 * i + 1]
+            if first >= p.nrow or last <= first:
+                return None
+            hs.append(formats.make_header(p.rsc_nlat, p.rsc_nlon, p.win_left, p.win_top + first, p.win_right,
+                                          p.win_top + last))
+        return hs
+
+    def interfere(self, hs) -> PairResult | None:
+        box, hdr6 = _plan.crossmul_box(hs[0], hs[1], self.rowlook, self.collook)
+        if box is None:
+            return None
+        p1, p2 = self.plans
+        # the geocoded windows are passed whole: the box lies inside both crops
+        outs = kernels.crossmul_looks(self.geo[0], (p1.win_left, p1.win_top), self.geo[1], (p2.win_left, p2.win_top),
+                                      box, self.rowlook, self.collook, fill_seed=self.fill_seed)
+        ifg = outs["ifg"]
+        if ifg.shape[0] >= self.n_win and ifg.shape[1] >= self.n_win:
+            if self._ml_shape != tuple(ifg.shape):
+                need = kernels.goldstein_scratch_bytes(ifg.shape[0], ifg.shape[1], self.n_win)
+                self._scratch = torch.empty(need, dtype=torch.uint8, device=self.dev)
+                self._ml_shape = tuple(ifg.shape)
+            filt = kernels.goldstein(ifg, self.alpha, self.n_win, scratch=self._scratch)
+        else:
+            filt = ifg.clone()
+        return PairResult(header=formats.make_header(*hdr6), box=tuple(box), ifg=ifg, amp1=outs["amp1"],
+                          amp2=outs["amp2"], coh=outs["coh"], filt=filt, gslc_headers=tuple(hs))
+
+    def run(self, ref_slc: torch.Tensor, sec_slc: torch.Tensor, dem: torch.Tensor) -> PairResult | None:
+        """One full chain step on device-resident inputs."""
+        self.geocode(ref_slc, sec_slc, dem)
+        hs = self.headers()
+        if hs is None:
+            return None
+        return self.interfere(hs)
+
+    @staticmethod
+    def launches_per_step():
+        # 2 x (deramp + rows init + geo2rdr) + crossmul + goldstein (patch + gather)
+        return 2 * 3 + 1 + 2
+
+
+def process_pair_host(chain: PairChain, ref_host: torch.Tensor, sec_host: torch.Tensor, dem_host: torch.Tensor,
+                      dev_in=None, host_out=None):
+    """End-to-end call on host buffers: H2D of both SLCs and the DEM, the chain,
+    D2H of the interferogram, amplitudes, coherence and filtered phase.
+
+    ``dev_in``/``host_out`` are reusable buffers (dicts) so repeated calls do
+    not allocate; host tensors should be pinned for asynchronous copies.
+    Returns (result, host_out, bytes_h2d, bytes_d2h).
+    """
+    dev = chain.dev
+    if dev_in is None:
+        dev_in = {"ref": torch.empty_like(ref_host, device=dev), "sec": torch.empty_like(sec_host, device=dev),
+                  "dem": torch.empty_like(dem_host, device=dev)}
+    dev_in["ref"].copy_(ref_host, non_blocking=True)
+    dev_in["sec"].copy_(sec_host, non_blocking=True)
+    dev_in["dem"].copy_(dem_host, non_blocking=True)
+    h2d = sum(t.numel() * t.element_size() for t in (ref_host, sec_host, dem_host))
+    res = chain.run(dev_in["ref"], dev_in["sec"], dev_in["dem"])
+    if res is None:
+        return None, host_out, h2d, 0
+    outs = {"ifg": res.ifg, "amp1": res.amp1, "amp2": res.amp2, "coh": res.coh, "filt": res.filt}
+    if host_out is None or any(host_out[k].shape != v.shape for k, v in outs.items()):
+        host_out = {k: torch.empty(v.shape, dtype=v.dtype, pin_memory=True) for k, v in outs.items()}
+    for k, v in outs.items():
+        host_out[k].copy_(v, non_blocking=True)
+    torch.cuda.current_stream().synchronize()
+    d2h = sum(t.numel() * t.element_size() for t in host_out.values())
+    return res, host_out, h2d, d2h

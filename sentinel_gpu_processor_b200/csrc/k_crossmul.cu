@@ -95,8 +95,12 @@ __global__ __launch_bounds__(XM_THREADS) void crossmul_looks_kernel(const XmArgs
     // mean over collook, then over rowlook, like cpx_col_look / cpx_row_look
     ir = ir / fcl / frl;
     ii = ii / fcl / frl;
-    const float am1 = sqrtf(p1 / fcl / frl);
-    const float am2 = sqrtf(p2 / fcl / frl);
+    // s1proc's powlooks returns |s| rather than |s|^2 when both looks are 1
+    // (s1proc/sario.py:416-418), so its amplitude is then sqrt(|s|); kept so
+    // that .amp and coherence values match the reference's.
+    const bool unit = (a.rowlook == 1 && a.collook == 1);
+    const float am1 = unit ? sqrtf(sqrtf(p1)) : sqrtf(p1 / fcl / frl);
+    const float am2 = unit ? sqrtf(sqrtf(p2)) : sqrtf(p2 / fcl / frl);
     const int64_t o = (int64_t)i * a.ncol_ml + j0 + m;
     if (a.ifg) a.ifg[o] = make_float2(ir, ii);
     if (a.amp1) a.amp1[o] = am1;

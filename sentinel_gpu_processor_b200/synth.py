@@ -416,7 +416,8 @@ def make_pair(config="c0", seed=20261203, device="cpu", baseline=150.0, coherenc
     ref_slc = tops_modulate(s_ref, ref, burst).contiguous()
     sec_slc = tops_modulate(s_sec, sec, burst).contiguous()
     return PairScene(name=config, seed=seed, ref=[ref], sec=[sec], rsc=rsc, dem=dem,
-                     ref_slc=[ref_slc], sec_slc=[sec_slc], rowlook=rl, collook=cl, alpha=al)
+                     ref_slc=[ref_slc], sec_slc=[sec_slc], rowlook=rl, collook=cl, alpha=al,
+                     extra={"hmax": hmax})
 
 
 def make_frame(seed=20261203, device="cpu", n_swaths=3, n_bursts=9, baseline=150.0,
@@ -468,4 +469,4 @@ def make_frame(seed=20261203, device="cpu", n_swaths=3, n_bursts=9, baseline=150
     dem = make_dem(rsc, seed, hmax, device=device)
     return PairScene(name="frame", seed=seed, ref=refs, sec=secs, rsc=rsc, dem=dem, ref_slc=ref_slc,
                      sec_slc=sec_slc, rowlook=rowlook, collook=collook, alpha=alpha,
-                     extra={"coherence": cohs})
+                     extra={"coherence": cohs, "hmax": hmax})

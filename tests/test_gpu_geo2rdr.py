@@ -79,7 +79,7 @@ def test_geocode_burst_matches_oracle(cuda, cfg, seed, which):
     wm = np.abs(w) > 0
     assert (gm != wm).mean() < 1e-3  # validity masks agree except boundary pixels
     both = gm & wm
-    assert both.sum() > 0.3 * both.size
+    assert both.sum() > 0.1 * both.size
     assert phase_rms(g, w, both) < PHASE_TOL
     assert rel_err(np.abs(g), np.abs(w), both) < 1e-4
 
