@@ -247,6 +247,29 @@ size_t s1b_goldstein_scratch_bytes(int32_t nrow, int32_t ncol, int32_t n_win);
 int s1b_goldstein(const void *in, void *out, int32_t nrow, int32_t ncol, int32_t n_win,
                   float alpha, void *scratch, size_t scratch_bytes, void *stream);
 
+/* Largest image of s1b_goldstein_noalloc, in 32x32 patches (32 MiB of
+ * scratch; ceil(nrow/8)-3 times ceil(ncol/8)-3 patches, about 512 x 512 px). */
+#define S1B_GOLDSTEIN_NOALLOC_MAX_PATCHES 4096
+
+/* The Goldstein filter of s1b_goldstein for callers that cannot allocate
+ * device memory while they filter -- for example a plugin inside a host
+ * application whose own pool allocator already holds the GPU's memory, or a
+ * pipeline that forbids allocation after start-up.  It allocates nothing:
+ * its patch scratch is a fixed device array compiled into this library,
+ * which every GPU that loads the library keeps (32 MiB) until the process
+ * exits.  No counterpart in the reference.
+ *   - Images needing more than S1B_GOLDSTEIN_NOALLOC_MAX_PATCHES patches
+ *     return S1B_ERR_TOO_LARGE (use s1b_goldstein then).
+ *   - The first call on each device looks up the array's device address
+ *     (cudaGetSymbolAddress, with that device current); make that first call
+ *     before any stream capture.
+ *   - All calls share the one array: calls that can run at the same time on
+ *     the GPU (different streams, or threads without ordering) race and
+ *     corrupt each other's results; serialise them.
+ *   - in/out: complex64 [nrow * ncol] device, n_win must be 32. */
+int s1b_goldstein_noalloc(const void *in, void *out, int32_t nrow, int32_t ncol, int32_t n_win,
+                          float alpha, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

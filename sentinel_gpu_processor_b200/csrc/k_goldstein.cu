@@ -15,6 +15,8 @@
 //      summed weights.  No atomics: the result is deterministic.
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "s1b.h"
 #include "s1b_device.cuh"
 #include "s1b_internal.h"
@@ -262,5 +264,74 @@ extern "C" int s1b_goldstein(const void *in, void *out, int32_t nrow, int32_t nc
   dim3 grid(nrow, (ncol + 255) / 256);
   goldstein_gather_kernel<<<grid, 256, 0, st>>>((const float2 *)scratch, (float2 *)out, nrow, ncol,
                                                 ni, nj);
+  return s1b_launch_status();
+}
+
+// ---------------------------------------------------------------------------
+// Goldstein without any device allocation.
+//
+// Some callers cannot allocate device memory when they filter: a plugin
+// running inside a host application whose own pool allocator has already
+// reserved the GPU's memory (a raw cudaMalloc then fails although the pool
+// has room), or a pipeline that forbids allocation after start-up to keep a
+// fixed footprint.  For them the patch scratch lives in a file-scope device
+// array of fixed size that every GPU loading this library holds until the
+// process exits.
+namespace {
+
+constexpr size_t kNoAllocMaxPatches = S1B_GOLDSTEIN_NOALLOC_MAX_PATCHES;
+__device__ __align__(256) float2 g_goldstein_scratch[kNoAllocMaxPatches * GN * GN];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mu;
+void *g_scratch_ptr[kMaxDevices] = {};
+
+// Device address of g_goldstein_scratch on the current device.  The symbol
+// name is only a host-side handle; the address is looked up once per device
+// (with that device current) and cached.
+int noalloc_scratch(void **ptr) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return s1b_fail(S1B_ERR_CUDA, cudaGetErrorString(e));
+  if (dev < 0 || dev >= kMaxDevices) return s1b_fail(S1B_ERR_UNSUPPORTED, "s1b_goldstein_noalloc: device ordinal above 63");
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (!g_scratch_ptr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_goldstein_scratch);
+    if (e != cudaSuccess) return s1b_fail(S1B_ERR_CUDA, cudaGetErrorString(e));
+    g_scratch_ptr[dev] = p;
+  }
+  *ptr = g_scratch_ptr[dev];
+  return S1B_OK;
+}
+
+}  // namespace
+
+extern "C" int s1b_goldstein_noalloc(const void *in, void *out, int32_t nrow, int32_t ncol,
+                                     int32_t n_win, float alpha, void *stream) {
+  if (!in || !out) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_goldstein_noalloc: null argument");
+  if (n_win != GN) return s1b_fail(S1B_ERR_UNSUPPORTED, "s1b_goldstein_noalloc: only n_win = 32 is implemented");
+  if (nrow < GN || ncol < GN)
+    return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_goldstein_noalloc: image smaller than the window");
+  int ni, nj;
+  patch_grid(nrow, ncol, ni, nj);
+  const int64_t npatch = (int64_t)ni * nj;
+  if (npatch > (int64_t)kNoAllocMaxPatches)
+    return s1b_fail(S1B_ERR_TOO_LARGE,
+                    "s1b_goldstein_noalloc: image needs more than S1B_GOLDSTEIN_NOALLOC_MAX_PATCHES (4096) "
+                    "patches of its fixed scratch (about 512 x 512 pixels); use s1b_goldstein");
+  if ((ncol + 255) / 256 > 65535) return s1b_fail(S1B_ERR_TOO_LARGE, "s1b_goldstein_noalloc: image too wide");
+  void *scratch = nullptr;
+  int s = noalloc_scratch(&scratch);
+  if (s) return s;
+  // every patch slot used below is written by the patch kernel before the
+  // gather reads it, so nothing left by an earlier call needs clearing
+  cudaStream_t st = (cudaStream_t)stream;
+  goldstein_patch_kernel<<<(unsigned)((npatch + GWARPS - 1) / GWARPS), 32 * GWARPS, 0, st>>>(
+      (const float2 *)in, (float2 *)scratch, nrow, ncol, ni, nj, alpha);
+  s = s1b_launch_status();
+  if (s) return s;
+  dim3 grid(nrow, (ncol + 255) / 256);
+  goldstein_gather_kernel<<<grid, 256, 0, st>>>((const float2 *)scratch, (float2 *)out, nrow, ncol, ni, nj);
   return s1b_launch_status();
 }
