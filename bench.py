@@ -1,16 +1,17 @@
 """Benchmark: IW-burst pixels/s of the chain geo2rdr -> resample -> ifg -> coherence -> Goldstein.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl s1b|reference] [--config c1]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl s1b|reference] [--config frame|c1]
 
-A step is one pass of the chain over one reference/secondary burst pair of
-one full IW burst (1500 lines x 21000 samples, complex64, looks 4 x 20,
-Goldstein alpha 0.6, 32 x 32 patches): TOPS deramp and FP64 geocoding of
-both SLCs onto the DEM grid, crossmul + multilook + amplitude looks +
-coherence, Goldstein filter.  ``value`` = burst pixels (lines x samples of
-the reference burst, counted once per pair) per second with inputs resident
-in HBM; ``e2e`` = the same through the host-buffer call
-(``chain.process_pair_host``) with H2D of both SLCs and the DEM and D2H of
-the products inside the timed region.
+A step is one pass of the chain over a full synthetic IW frame (default,
+3 subswaths x 9 bursts of uneven size, lines 1480-1530, samples
+20000-25500, complex64, looks 4 x 20, Goldstein alpha 0.5, 32 x 32 patches)
+or over one IW burst pair (--config c1, configs[1]: 1500 x 21000, alpha 0.6):
+for every burst pair, TOPS deramp and FP64 geocoding of both SLCs onto the
+DEM grid, crossmul + multilook + amplitude looks + coherence, Goldstein.
+``value`` = burst pixels (lines x samples of each reference burst, counted
+once per pair) per second with inputs resident in HBM; ``e2e`` = the same
+with pinned H2D of every SLC and the DEM and D2H of the products inside the
+timed region.
 
 With N > 1 (torchrun) every rank processes its own seeded burst pair (weak
 scaling, no data-path collective); timings are the max over ranks.
@@ -52,7 +53,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="s1b", choices=["s1b", "reference"])
-    ap.add_argument("--config", default="c1", choices=["c1", "c0", "small"])
+    ap.add_argument("--config", default="frame", choices=["frame", "c1", "c0", "small"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -88,54 +89,93 @@ def barrier(world):
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """SM clock and throttle-reason samples during the timed region.
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    A background thread polls NVML every 5 ms (the timed region can be far
+    shorter than nvidia-smi's 200 ms minimum period); without NVML it falls
+    back to ``nvidia-smi -lms 200``.
+    """
+
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4}
 
     def __init__(self, index):
         self.index = index
-        self.proc = None
-        self.path = None
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = None
+        self._thread = None
+        self._smi = None
 
     def start(self):
+        import threading
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+        except Exception:  # noqa: BLE001 -- any NVML failure: fall back
+            self._start_smi()
+            return
+        self._stop = threading.Event()
+
+        def loop():
+            while not self._stop.is_set():
+                try:
+                    self.samples.append(float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)))
+                    r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    for nm, bit in self.REASONS.items():
+                        if r & bit:
+                            self.reasons.add(nm)
+                except Exception:  # noqa: BLE001
+                    pass
+                self._stop.wait(0.005)
+
+        self._thread = threading.Thread(target=loop, daemon=True)
+        self._thread.start()
+
+    def _start_smi(self):
         if not shutil.which("nvidia-smi"):
             return
-        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        fd, path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
-        self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                      "-i", str(self.index), "-lms", "200"], stdout=open(self.path, "w"),
-                                     stderr=subprocess.DEVNULL)
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        self._smi = (subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-i",
+                                       str(self.index), "-lms", "200"], stdout=open(path, "w"),
+                                      stderr=subprocess.DEVNULL), path)
 
     def stop(self):
-        if self.proc is None:
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=2)
+        elif self._smi is not None:
+            proc, path = self._smi
+            proc.terminate()
+            try:
+                proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                proc.kill()
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            with open(path) as f:
+                for line in f:
+                    q = [x.strip() for x in line.split(",")]
+                    if len(q) < 6:
+                        continue
+                    try:
+                        self.samples.append(float(q[0]))
+                        self.max_mhz = float(q[1])
+                    except ValueError:
+                        continue
+                    for nm, v in zip(names, q[2:6]):
+                        if v.lower() == "active":
+                            self.reasons.add(nm)
+            os.unlink(path)
+        if not self.samples:
             return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        with open(self.path) as f:
-            for line in f:
-                p = [x.strip() for x in line.split(",")]
-                if len(p) < 9:
-                    continue
-                try:
-                    sm.append(float(p[1]))
-                    mx = float(p[2])
-                except ValueError:
-                    continue
-                for nm, v in zip(names, p[5:9]):
-                    if v.lower() == "active":
-                        reasons.add(nm)
-        os.unlink(self.path)
-        if not sm:
-            return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
 
 
 def peaks():
@@ -194,27 +234,91 @@ def cpu_baseline():
 # s1b arm
 # ----------------------------------------------------------------------------
 
+def _workload(args, rank, dev):
+    """(scene, chain, run(), host-buffer run maker, description) for the config."""
+    from sentinel_gpu_processor_b200 import synth
+    from sentinel_gpu_processor_b200.chain import FrameChain, PairChain
+    if args.config == "frame":
+        sc = synth.make_frame(seed=20261203 + 2000 + rank, device=dev)
+        chain = FrameChain(sc.ref, sc.sec, sc.rsc, sc.rowlook, sc.collook, sc.alpha, device=dev)
+        ins = (sc.ref_slc, sc.sec_slc, sc.dem)
+        desc = (f"full IW frame: {len(sc.ref)} bursts (3 subswaths x 9) of uneven size, lines 1480-1530, samples "
+                f"20000-25500, 100-line overlap (configs[2])")
+        return sc, chain, lambda: chain.run(*ins), desc
+    sc = make_scene(args.config, 20261203 + 1000 + rank, dev)
+    chain = PairChain(sc.ref[0], sc.sec[0], sc.rsc, sc.rowlook, sc.collook, sc.alpha, device=dev)
+    ins = (sc.ref_slc[0], sc.sec_slc[0], sc.dem)
+    p0 = chain.plans[0]
+    desc = f"one IW burst pair {p0.lines} x {p0.samples} complex64 (configs[1])" if args.config == "c1" else \
+        f"burst pair {p0.lines} x {p0.samples} ({args.config})"
+    return sc, chain, lambda: chain.run(*ins), desc
+
+
+def _e2e(chain, sc, args, world):
+    """End-to-end rate through host buffers: pinned H2D of every SLC and the DEM,
+    the chain, D2H of ifg/amplitudes/coherence/filtered ifg, per step."""
+    import torch
+    frame = args.config == "frame"
+    refs = sc.ref_slc if frame else sc.ref_slc[:1]
+    secs = sc.sec_slc if frame else sc.sec_slc[:1]
+    ref_h = [t.cpu().pin_memory() for t in refs]
+    sec_h = [t.cpu().pin_memory() for t in secs]
+    dem_h = sc.dem.cpu().pin_memory()
+    ref_d = [torch.empty_like(t, device=chain.dev) for t in ref_h]
+    sec_d = [torch.empty_like(t, device=chain.dev) for t in sec_h]
+    dem_d = torch.empty_like(dem_h, device=chain.dev)
+    host_out = {}
+    h2d = sum(t.numel() * t.element_size() for t in ref_h + sec_h) + dem_h.numel() * dem_h.element_size()
+
+    def step():
+        dem_d.copy_(dem_h, non_blocking=True)
+        d2h = 0
+        for k in range(len(ref_h)):
+            ref_d[k].copy_(ref_h[k], non_blocking=True)
+            sec_d[k].copy_(sec_h[k], non_blocking=True)
+            res = chain.run_pair(k, ref_d[k], sec_d[k], dem_d) if frame else chain.run(ref_d[k], sec_d[k], dem_d)
+            if res is None:
+                continue
+            for name in ("ifg", "amp1", "amp2", "coh", "filt"):
+                v = getattr(res, name)
+                key = (k, name)
+                if key not in host_out or host_out[key].shape != v.shape:
+                    host_out[key] = torch.empty(v.shape, dtype=v.dtype, pin_memory=True)
+                host_out[key].copy_(v, non_blocking=True)
+                d2h += v.numel() * v.element_size()
+        torch.cuda.current_stream().synchronize()
+        return d2h
+
+    step()
+    k_e2e = max(3, args.steps // 4) if frame else max(3, args.steps // 2)
+    barrier(world)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    s2, t2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s2.record(stream)
+    d2h = 0
+    for _ in range(k_e2e):
+        d2h = step()
+    t2.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(s2.elapsed_time(t2), world)
+    return world * k_e2e * chain.burst_pixels / (e2e_ms / 1e3), h2d, d2h
+
+
 def run_s1b(args):
     import torch
-
-    from sentinel_gpu_processor_b200.chain import PairChain, process_pair_host
     rank, world, local = dist_setup(args.gpus)
     dev = torch.device("cuda", local)
-    seed = 20261203 + 1000 * 1 + rank
-    sc = make_scene(args.config, seed, dev)
-    chain = PairChain(sc.ref[0], sc.sec[0], sc.rsc, sc.rowlook, sc.collook, sc.alpha, device=dev)
-    ref, sec, dem = sc.ref_slc[0], sc.sec_slc[0], sc.dem
-    p0 = chain.plans[0]
-    geo_px = [p.nrow * p.ncol for p in chain.plans]
+    sc, chain, run, desc = _workload(args, rank, dev)
+    warm = max(args.warmup, 3)
     res = None
-    for _ in range(max(args.warmup, 3)):
-        res = chain.run(ref, sec, dem)
+    for _ in range(warm):
+        res = run()
     torch.cuda.synchronize()
-    if res is None:
-        raise SystemExit("empty interferogram for the synthetic pair")
+    if res is None or (isinstance(res, list) and any(r is None for r in res)):
+        raise SystemExit("empty interferogram for the synthetic input")
     stream = torch.cuda.current_stream()
-    # kernel events around the two geocoding launches of every timed step
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(2 * args.steps)]
+    chain.geo_events = []
     clocks = Clocks(local)
     barrier(world)
     torch.cuda.synchronize()
@@ -222,68 +326,56 @@ def run_s1b(args):
     start = torch.cuda.Event(enable_timing=True)
     stop = torch.cuda.Event(enable_timing=True)
     start.record(stream)
-    from sentinel_gpu_processor_b200 import kernels
-    for k in range(args.steps):
-        for i, (pl, slc) in enumerate(zip(chain.plans, (ref, sec))):
-            kernels.deramp(pl, slc.reshape(-1), out=chain.deramped[i])
-            e0, e1 = ev[2 * k + i]
-            e0.record(stream)
-            kernels.geo2rdr(pl, dem, chain.deramped[i], out=chain.geo[i], rows=chain.rows[2 * i:2 * i + 2])
-            e1.record(stream)
-        hs = chain.headers()
-        res = chain.interfere(hs)
+    for _ in range(args.steps):
+        res = run()
     stop.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
+    ev = chain.geo_events
+    chain.geo_events = None
     barrier(world)
-    elapsed_ms = start.elapsed_time(stop)
-    elapsed_ms = max_over_ranks(elapsed_ms, world)
+    elapsed_ms = max_over_ranks(start.elapsed_time(stop), world)
     geo_ms = [a.elapsed_time(b) for a, b in ev]
     geo_avg_ms = sum(geo_ms) / len(geo_ms)
     value = world * args.steps * chain.burst_pixels / (elapsed_ms / 1e3)
+    e2e, h2d, d2h = _e2e(chain, sc, args, world)
 
-    # end to end through the host-buffer call
-    ref_h = ref.cpu().pin_memory()
-    sec_h = sec.cpu().pin_memory()
-    dem_h = dem.cpu().pin_memory()
-    dev_in, host_out = None, None
-    dev_in = {"ref": torch.empty_like(ref), "sec": torch.empty_like(sec), "dem": torch.empty_like(dem)}
-    _, host_out, _, _ = process_pair_host(chain, ref_h, sec_h, dem_h, dev_in, host_out)
-    k_e2e = max(3, args.steps // 2)
-    barrier(world)
-    torch.cuda.synchronize()
-    s2, t2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s2.record(stream)
-    for _ in range(k_e2e):
-        _, host_out, h2d, d2h = process_pair_host(chain, ref_h, sec_h, dem_h, dev_in, host_out)
-    t2.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(s2.elapsed_time(t2), world)
-    e2e = world * k_e2e * chain.burst_pixels / (e2e_ms / 1e3)
-
+    if args.config == "frame":
+        geo_px = chain.geo_pixels()
+        burst_px = chain.burst_pixels_all()
+        launches = chain.launches_per_step()
+        ml = [list(r.ifg.shape) for r in res]
+        extra = {"bursts": len(chain.pairs), "burst_px_per_step": chain.burst_pixels,
+                 "ifg_ml_shapes_first3": ml[:3]}
+    else:
+        geo_px = [p.nrow * p.ncol for p in chain.plans]
+        burst_px = [p.lines * p.samples for p in chain.plans]
+        launches = chain.launches_per_step()
+        extra = {"lines": chain.plans[0].lines, "samples": chain.plans[0].samples, "ifg_ml": list(res.ifg.shape)}
     peak, peak_kind = peaks()
-    geo_bytes = GEO_BYTES_PER_GEO_PX * (geo_px[0] + geo_px[1]) / 2 + GEO_BYTES_PER_BURST_PX * chain.burst_pixels
+    geo_bytes = (GEO_BYTES_PER_GEO_PX * sum(geo_px) + GEO_BYTES_PER_BURST_PX * sum(burst_px)) / len(geo_px)
     achieved = geo_bytes / (geo_avg_ms / 1e3) / 1e9
     traffic = None
     if GEO_DRAM_BYTES_PER_GEO_PX is not None:
-        traffic = GEO_DRAM_BYTES_PER_GEO_PX * (geo_px[0] + geo_px[1]) / 2
+        traffic = GEO_DRAM_BYTES_PER_GEO_PX * sum(geo_px) / len(geo_px)
+    cfg = {"workload": desc, "looks": [sc.rowlook, sc.collook],
+           "goldstein": {"alpha": sc.alpha, "n_win": 32, "step": 8}, "geo_px_total": sum(geo_px),
+           "l2": "inputs larger than L2 (>= 252 MB per SLC, read once per step)", "parallelism": f"replicas{world}"}
+    cfg.update(extra)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": max(args.warmup, 3), "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+        "warmup": warm, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64 geometry + c64", "data": "synthetic",
-        "config": {"workload": f"one IW burst pair {p0.lines} x {p0.samples} complex64 (configs[1])",
-                   "lines": p0.lines, "samples": p0.samples, "looks": [sc.rowlook, sc.collook],
-                   "goldstein": {"alpha": sc.alpha, "n_win": 32, "step": 8},
-                   "geo_px": geo_px, "ifg_ml": list(res.ifg.shape),
-                   "l2": "inputs larger than L2 (two 252 MB SLCs + DEM per step)", "parallelism": f"replicas{world}"},
+        "config": cfg,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": PairChain.launches_per_step() * args.steps,
+        "gpu_launches": launches * args.steps,
         "roofline": {"bound": "hbm", "kernel": "geo2rdr_kernel", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_kind": peak_kind, "bytes_per_launch": geo_bytes, "launch_ms": geo_avg_ms,
                      "note": "geocoding is FP64-compute bound (zero-Doppler Newton); its HBM fraction is low "
                              "by design"},
-        "kernels_ms": {"geo2rdr_avg": geo_avg_ms, "step": elapsed_ms / args.steps},
+        "kernels_ms": {"geo2rdr_avg": geo_avg_ms, "geo2rdr_share": sum(geo_ms) / (elapsed_ms * world / world),
+                       "step": elapsed_ms / args.steps},
     }
     if clk is not None:
         line["clocks"] = clk
@@ -310,14 +402,27 @@ def run_reference(args):
     from oracle import coherence as oc
     from oracle import crossmul as ox
     from oracle import refrun
-    from sentinel_gpu_processor_b200 import formats
+    from sentinel_gpu_processor_b200 import formats, synth
     if not refrun.available():
         print(json.dumps({"impl": "reference", "unavailable": "reference executables not built in oracle/_ref "
                                                               "(python oracle/build_ref.py)"}))
         return
+    if args.config == "frame":
+        # a bounded sample of the frame: its first burst pair (the reference
+        # runs geo2rdr once per burst for uneven burst sizes)
+        frame = synth.make_frame(seed=20261203 + 2000, device="cuda")
+        base_sc = synth.frame_pair(frame, 0)
+        del frame
+        base_sc.dem = base_sc.dem.cpu()
+        base_sc.ref_slc = [t.cpu() for t in base_sc.ref_slc]
+        base_sc.sec_slc = [t.cpu() for t in base_sc.sec_slc]
+        sample = "first burst pair of the frame (configs[2]) per step"
+    else:
+        base_sc = make_scene(args.config, 20261203 + 1000, "cpu")
+        sample = "one burst pair per step"
     # the reference geo2rdr overruns its DEM/output buffers on some grids
     # (oracle/refrun.geo2rdr_buffers_safe); run it only on a checked-safe grid
-    sc = refrun.make_reference_safe(make_scene(args.config, 20261203 + 1000, "cpu"))
+    sc = refrun.make_reference_safe(base_sc)
     base = "/dev/shm" if os.path.isdir("/dev/shm") else None
     wd = tempfile.mkdtemp(prefix="s1b_refbench_", dir=base)
     try:
@@ -362,12 +467,12 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64 geometry + c64", "data": "synthetic",
-        "config": {"workload": f"one IW burst pair {L} x {S} complex64 (configs[1])", "lines": L, "samples": S,
+        "config": {"workload": f"{args.config}: {sample}, burst {L} x {S} complex64", "lines": L, "samples": S,
                    "looks": [sc.rowlook, sc.collook], "goldstein": {"alpha": sc.alpha, "n_win": 32, "step": 8},
                    "files": "reference formats on /dev/shm"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                         "sample": "the reference executables geo2rdr x2, crossmul_daemon, goldstein (sm_100a "
-                                   "builds of the reference sources) + its NumPy coherence, per burst pair"},
+                         "sample": f"{sample}: the reference executables geo2rdr x2, crossmul_daemon, goldstein "
+                                   "(sm_100a builds of the reference sources) + its NumPy coherence, wall clock"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "world_size_requested": world,
     }

@@ -21,6 +21,22 @@ import torch
 from . import _lib, formats, kernels, plan as _plan
 
 
+def _start_event(sink):
+    if sink is None:
+        return None
+    e = torch.cuda.Event(enable_timing=True)
+    e.record()
+    return e
+
+
+def _end_event(sink, start):
+    if sink is None:
+        return
+    e = torch.cuda.Event(enable_timing=True)
+    e.record()
+    sink.append((start, e))
+
+
 @dataclass
 class PairResult:
     header: np.ndarray  # ifg header, int32[64]
@@ -49,15 +65,18 @@ class PairChain:
         self.deramped = [torch.empty(p.lines * p.samples, dtype=torch.complex64, device=self.dev) for p in self.plans]
         self.geo = [torch.empty((p.nrow, p.ncol), dtype=torch.complex64, device=self.dev) for p in self.plans]
         self.rows = torch.empty(4, dtype=torch.int32, device=self.dev)
-        self.rows_host = torch.empty(4, dtype=torch.int32, pin_memory=True)
+        self.rows_host = torch.empty(4, dtype=torch.int32, pin_memory=torch.cuda.is_available())
         self.burst_pixels = L * S
         self._scratch = None
         self._ml_shape = None
+        self.geo_events = None  # list to collect (start, end) CUDA events around geocoding launches
 
     def geocode(self, ref_slc: torch.Tensor, sec_slc: torch.Tensor, dem: torch.Tensor):
         for i, (p, slc) in enumerate(zip(self.plans, (ref_slc, sec_slc))):
             kernels.deramp(p, slc.reshape(-1), out=self.deramped[i])
+            ev = _start_event(self.geo_events)
             kernels.geo2rdr(p, dem, self.deramped[i], out=self.geo[i], rows=self.rows[2 * i:2 * i + 2])
+            _end_event(self.geo_events, ev)
 
     def headers(self):
         """Crop rows -> the two ``.gslc`` headers (geo2rdr.cu:641-647), or None if a burst is empty."""
@@ -135,3 +154,80 @@ def process_pair_host(chain: PairChain, ref_host: torch.Tensor, sec_host: torch.
     torch.cuda.current_stream().synchronize()
     d2h = sum(t.numel() * t.element_size() for t in host_out.values())
     return res, host_out, h2d, d2h
+
+
+class FrameChain:
+    """All burst pairs of a frame (configs[2]: subswaths x bursts of uneven
+    size) processed pair by pair with shared device buffers sized for the
+    largest burst and DEM window."""
+
+    def __init__(self, refs, secs, rsc, rowlook, collook, alpha, n_win=32, device="cuda", fill_seed=0):
+        self.dev = torch.device(device)
+        self.rowlook, self.collook, self.alpha, self.n_win = int(rowlook), int(collook), float(alpha), int(n_win)
+        self.pairs = []
+        for ra, sa in zip(refs, secs):
+            pls = [_plan.burst_plan(a.radar, a.orbit, a.fm, a.dc, a.bursts[0], rsc) for a in (ra, sa)]
+            if any(p.nrow <= 0 or p.ncol <= 0 for p in pls):
+                raise _lib.S1BError(_lib.S1B_ERR_EMPTY, "FrameChain: burst outside the DEM grid")
+            self.pairs.append(pls)
+        max_burst = max(p.lines * p.samples for pls in self.pairs for p in pls)
+        max_geo = max(p.nrow * p.ncol for pls in self.pairs for p in pls)
+        self.deramped = [torch.empty(max_burst, dtype=torch.complex64, device=self.dev) for _ in range(2)]
+        self.geo = [torch.empty(max_geo, dtype=torch.complex64, device=self.dev) for _ in range(2)]
+        self.rows = torch.empty(4 * len(self.pairs), dtype=torch.int32, device=self.dev)
+        self.rows_host = torch.empty(4 * len(self.pairs), dtype=torch.int32,
+                                     pin_memory=torch.cuda.is_available())
+        self.burst_pixels = sum(pls[0].lines * pls[0].samples for pls in self.pairs)
+        self.fill_seed = int(fill_seed)
+        self._scratch = torch.empty(0, dtype=torch.uint8, device=self.dev)
+        self.geo_events = None
+
+    def _geo_view(self, i, p):
+        return self.geo[i][:p.nrow * p.ncol].view(p.nrow, p.ncol)
+
+    def run_pair(self, k, ref_slc, sec_slc, dem):
+        pls = self.pairs[k]
+        for i, (p, slc) in enumerate(zip(pls, (ref_slc, sec_slc))):
+            kernels.deramp(p, slc.reshape(-1), out=self.deramped[i][:p.lines * p.samples])
+            ev = _start_event(self.geo_events)
+            kernels.geo2rdr(p, dem, self.deramped[i][:p.lines * p.samples], out=self._geo_view(i, p),
+                            rows=self.rows[4 * k + 2 * i:4 * k + 2 * i + 2])
+            _end_event(self.geo_events, ev)
+        self.rows_host[4 * k:4 * k + 4].copy_(self.rows[4 * k:4 * k + 4], non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        r = self.rows_host[4 * k:4 * k + 4].tolist()
+        hs = []
+        for i, p in enumerate(pls):
+            first, last = r[2 * i], r[2 * i + 1]
+            if first >= p.nrow or last <= first:
+                return None
+            hs.append(formats.make_header(p.rsc_nlat, p.rsc_nlon, p.win_left, p.win_top + first, p.win_right,
+                                          p.win_top + last))
+        box, hdr6 = _plan.crossmul_box(hs[0], hs[1], self.rowlook, self.collook)
+        if box is None:
+            return None
+        p1, p2 = pls
+        outs = kernels.crossmul_looks(self._geo_view(0, p1), (p1.win_left, p1.win_top), self._geo_view(1, p2),
+                                      (p2.win_left, p2.win_top), box, self.rowlook, self.collook,
+                                      fill_seed=self.fill_seed)
+        ifg = outs["ifg"]
+        filt = ifg
+        if ifg.shape[0] >= self.n_win and ifg.shape[1] >= self.n_win:
+            need = kernels.goldstein_scratch_bytes(ifg.shape[0], ifg.shape[1], self.n_win)
+            if self._scratch.numel() < need:
+                self._scratch = torch.empty(need, dtype=torch.uint8, device=self.dev)
+            filt = kernels.goldstein(ifg, self.alpha, self.n_win, scratch=self._scratch)
+        return PairResult(header=formats.make_header(*hdr6), box=tuple(box), ifg=ifg, amp1=outs["amp1"],
+                          amp2=outs["amp2"], coh=outs["coh"], filt=filt, gslc_headers=tuple(hs))
+
+    def run(self, ref_slcs, sec_slcs, dem):
+        return [self.run_pair(k, r, s, dem) for k, (r, s) in enumerate(zip(ref_slcs, sec_slcs))]
+
+    def launches_per_step(self):
+        return len(self.pairs) * PairChain.launches_per_step()
+
+    def geo_pixels(self):
+        return [p.nrow * p.ncol for pls in self.pairs for p in pls]
+
+    def burst_pixels_all(self):
+        return [p.lines * p.samples for pls in self.pairs for p in pls]

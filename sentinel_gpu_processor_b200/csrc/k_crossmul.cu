@@ -61,23 +61,55 @@ __global__ __launch_bounds__(XM_THREADS) void crossmul_looks_kernel(const XmArgs
   const int wcta = mcta * a.collook;
   const int64_t col0 = (int64_t)j0 * a.collook;
   const int64_t row0 = (int64_t)i * a.rowlook;
-  for (int c = threadIdx.x; c < wcta; c += XM_THREADS) {
-    float ir = 0.f, ii = 0.f, p1 = 0.f, p2 = 0.f;
-    const float2 *pr = a.ref + a.ref_off + row0 * a.ref_width + col0 + c;
-    const float2 *ps = a.sec + a.sec_off + row0 * a.sec_width + col0 + c;
-    for (int k = 0; k < a.rowlook; ++k) {
-      const float2 r = __ldg(pr);
-      const float2 s = __ldg(ps);
-      pr += a.ref_width;
-      ps += a.sec_width;
-      // conj(r) * s  (sario.cu:207-208)
-      ir += r.x * s.x + r.y * s.y;
-      ii += -r.y * s.x + r.x * s.y;
-      p1 += r.x * r.x + r.y * r.y;
-      p2 += s.x * s.x + s.y * s.y;
+  // Each thread owns columns c and c + 256 of the chunk (when present) and
+  // issues the loads of four rows of both SLCs for both columns before it
+  // accumulates, so 16 independent 8-byte loads are in flight per thread.
+  for (int c = threadIdx.x; c < wcta; c += 2 * XM_THREADS) {
+    const bool two = c + XM_THREADS < wcta;
+    const int cc = two ? c + XM_THREADS : c;
+    float ir[2] = {0.f, 0.f}, ii[2] = {0.f, 0.f}, p1[2] = {0.f, 0.f}, p2[2] = {0.f, 0.f};
+    const float2 *pr = a.ref + a.ref_off + row0 * a.ref_width + col0;
+    const float2 *ps = a.sec + a.sec_off + row0 * a.sec_width + col0;
+    int k = 0;
+    for (; k + 4 <= a.rowlook; k += 4) {
+      float2 r[4][2], s[4][2];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        r[u][0] = __ldg(pr + (int64_t)(k + u) * a.ref_width + c);
+        r[u][1] = __ldg(pr + (int64_t)(k + u) * a.ref_width + cc);
+        s[u][0] = __ldg(ps + (int64_t)(k + u) * a.sec_width + c);
+        s[u][1] = __ldg(ps + (int64_t)(k + u) * a.sec_width + cc);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          // conj(r) * s  (sario.cu:207-208)
+          ir[q] += r[u][q].x * s[u][q].x + r[u][q].y * s[u][q].y;
+          ii[q] += -r[u][q].y * s[u][q].x + r[u][q].x * s[u][q].y;
+          p1[q] += r[u][q].x * r[u][q].x + r[u][q].y * r[u][q].y;
+          p2[q] += s[u][q].x * s[u][q].x + s[u][q].y * s[u][q].y;
+        }
+      }
     }
-    sI[c] = make_float2(ir, ii);
-    sP[c] = make_float2(p1, p2);
+    for (; k < a.rowlook; ++k) {
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int col = q ? cc : c;
+        const float2 r = __ldg(pr + (int64_t)k * a.ref_width + col);
+        const float2 s = __ldg(ps + (int64_t)k * a.sec_width + col);
+        ir[q] += r.x * s.x + r.y * s.y;
+        ii[q] += -r.y * s.x + r.x * s.y;
+        p1[q] += r.x * r.x + r.y * r.y;
+        p2[q] += s.x * s.x + s.y * s.y;
+      }
+    }
+    sI[c] = make_float2(ir[0], ii[0]);
+    sP[c] = make_float2(p1[0], p2[0]);
+    if (two) {
+      sI[cc] = make_float2(ir[1], ii[1]);
+      sP[cc] = make_float2(p1[1], p2[1]);
+    }
   }
   __syncthreads();
   const float fcl = (float)a.collook, frl = (float)a.rowlook;

@@ -81,103 +81,115 @@ __global__ __launch_bounds__(256) void deramp_kernel(const __grid_constant__ s1b
 }
 
 // ----------------------------------------------------------------- geo2rdr
-// CTA tile: 32 columns x 8 rows of the DEM window, one pixel per thread.
-constexpr int G_TX = 32, G_TY = 8;
+// CTA tile: G_TX columns x G_RY rows of the DEM window.  Each thread owns one
+// column and walks down the tile's rows: the zero-Doppler solution of the
+// pixel above seeds the Newton of the next one (adjacent rows are ~2 ms apart
+// in azimuth time, so one exact-Newton step lands below the 5e-9 s
+// tolerance and each pixel needs a single orbit evaluation).  Warps cover
+// 32 consecutive columns of a row, so DEM reads and output writes coalesce.
+constexpr int G_TX = 128, G_RY = 16;
 
 __global__ void rows_init_kernel(int32_t *rows, int nrow) {
   rows[0] = nrow;
   rows[1] = -1;
 }
 
-__global__ __launch_bounds__(G_TX *G_TY) void geo2rdr_kernel(
+__global__ __launch_bounds__(G_TX) void geo2rdr_kernel(
     const __grid_constant__ s1b_burst_plan_t P, const int16_t *__restrict__ dem, int64_t pitch,
     const float2 *__restrict__ burst, float2 *__restrict__ out, int32_t *__restrict__ rows,
     int nrow, int ncol) {
-  __shared__ double s_row[G_TY][3];  // sinlat, coslat, re (per row)
+  __shared__ double s_row[G_RY][3];  // sinlat, coslat, re (per row)
   __shared__ double s_col[G_TX][2];  // sinlon, coslon (per column)
-  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tx = threadIdx.x;
   const int col = blockIdx.x * G_TX + tx;
-  const int row = blockIdx.y * G_TY + ty;
-  const int tid = ty * G_TX + tx;
+  const int row0 = blockIdx.y * G_RY;
   // llh->ECEF trigonometry (orbit.cu:20-27) once per row / column of the tile
-  if (tid < G_TY) {
-    const int r = blockIdx.y * G_TY + tid;
-    const double lat = (P.lat0 + r * P.dlat) * kPiD / 180;
+  if (tx < G_RY) {
+    const double lat = (P.lat0 + (row0 + tx) * P.dlat) * kPiD / 180;
     double s, c;
     sincos(lat, &s, &c);
-    s_row[tid][0] = s;
-    s_row[tid][1] = c;
-    s_row[tid][2] = kRaD / sqrt(1. - kRe2D * s * s);
-  } else if (tid >= 32 && tid < 32 + G_TX) {
-    const int c_ = blockIdx.x * G_TX + (tid - 32);
-    const double lon = (P.lon0 + c_ * P.dlon) * kPiD / 180;
+    s_row[tx][0] = s;
+    s_row[tx][1] = c;
+    s_row[tx][2] = kRaD / sqrt(1. - kRe2D * s * s);
+  }
+  {
+    const double lon = (P.lon0 + col * P.dlon) * kPiD / 180;
     double s, c;
     sincos(lon, &s, &c);
-    s_col[tid - 32][0] = s;
-    s_col[tid - 32][1] = c;
+    s_col[tx][0] = s;
+    s_col[tx][1] = c;
   }
   __syncthreads();
-  const bool inb = (col < ncol) && (row < nrow);
-  float2 res = make_float2(0.f, 0.f);
-  if (inb) {
-    const double h = (double)__ldg(dem + (int64_t)row * pitch + col);
-    const double sinlat = s_row[ty][0], coslat = s_row[ty][1], re = s_row[ty][2];
-    const double sinlon = s_col[tx][0], coslon = s_col[tx][1];
-    double p[3];
-    p[0] = (re + h) * coslat * coslon;
-    p[1] = (re + h) * coslat * sinlon;
-    p[2] = (re * (1 - kRe2D) + h) * sinlat;
-    // zero-Doppler solve seeded at the burst centre (geo2rdr.cu:588-600)
-    double t = P.tmid;
-    OrbitState st;
+  const bool colok = col < ncol;
+  const double sinlon = s_col[tx][0], coslon = s_col[tx][1];
+  const double inv_dmrg = 1.0 / P.dmrg, prf = 1.0 / P.dtaz, two_over_c = 2.0 / kSolD;
+  // Newton state carried down the column; the first pixel starts at the
+  // burst centre like the reference (geo2rdr.cu:588-600)
+  double t = P.tmid;
+  OrbitState st;
 #pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      st.x[i] = P.xmid[i];
-      st.v[i] = P.vmid[i];
-      st.a[i] = P.amid[i];
-    }
-    double dr[3];
-    zero_doppler(P.orbit, p, t, st, dr);
-    const double rng = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
-    const double rgoff = (rng - P.rngstart) / P.dmrg;
-    const double azoff = (t - P.tstart) / P.dtaz;
-    // validity window, geo2rdr.cu:208-209
-    bool valid = rgoff > P.first_valid_sample && rgoff < P.last_valid_sample - 1 &&
-                 azoff >= P.first_valid_line + 5 && azoff < P.last_valid_line - 5;
-    const int intr = (int)rgoff, inta = (int)azoff;
-    // the 2x2 neighbourhood must lie inside the burst even if the validity
-    // limits passed in exceed the raster
-    valid = valid && intr >= 0 && intr + 1 < P.samples && inta >= 0 && inta + 1 < P.lines;
-    if (valid) {
-      // per-pixel TOPS reramp (geo2rdr.cu:210-219)
-      const double tr = rng * 2 / kSolD;
-      double dt = tr - P.fm[0];
-      const double ka = P.fm[1] + dt * (P.fm[2] + P.fm[3] * dt);
-      dt = tr - P.dc[0];
-      const double fnc = P.dc[1] + dt * (P.dc[2] + P.dc[3] * dt);
-      const double kt = ka * P.ks / (ka - P.ks);
-      const double etaref = -fnc / ka - P.etac0;
-      const double eta = -P.lines * P.dtaz / 2. + t - P.tstart;
-      const double ed = eta - etaref;
-      const double reramp = -kPiD * kt * ed * ed;
-      // bilinear interpolation of the deramped burst (geo2rdr.cu:220-237)
-      const float fr = (float)(rgoff - intr), fa = (float)(azoff - inta);
-      const size_t i1 = (size_t)inta * P.samples + intr;
-      const float2 b1 = __ldg(burst + i1), b2 = __ldg(burst + i1 + 1);
-      const float2 b3 = __ldg(burst + i1 + P.samples), b4 = __ldg(burst + i1 + P.samples + 1);
-      const float2 c1 = make_float2(fmaf(fr, b2.x - b1.x, b1.x), fmaf(fr, b2.y - b1.y, b1.y));
-      const float2 c2 = make_float2(fmaf(fr, b4.x - b3.x, b3.x), fmaf(fr, b4.y - b3.y, b3.y));
-      const float2 v = make_float2(fmaf(fa, c2.x - c1.x, c1.x), fmaf(fa, c2.y - c1.y, c1.y));
-      // range phase and reramp (geo2rdr.cu:238-243)
-      res = cmul(v, phasor(P.k4pi_wvl * rng - reramp));
-    }
-    __stcs(out + (size_t)row * ncol + col, res);
+  for (int i = 0; i < 3; ++i) {
+    st.x[i] = P.xmid[i];
+    st.v[i] = P.vmid[i];
+    st.a[i] = P.amid[i];
   }
-  // first / last non-zero output row (geo2rdr.cu:86-128): one vote per warp
-  const unsigned nz = __ballot_sync(0xffffffffu, inb && (res.x != 0.f || res.y != 0.f));
-  if (nz && tx == 0 && rows) {
-    atomicMin(rows, row);
-    atomicMax(rows + 1, row + 1);
+  const int rmax = min(G_RY, nrow - row0);
+  for (int r = 0; r < rmax; ++r) {
+    const int row = row0 + r;
+    float2 res = make_float2(0.f, 0.f);
+    if (colok) {
+      const double h = (double)__ldg(dem + (int64_t)row * pitch + col);
+      const double sinlat = s_row[r][0], coslat = s_row[r][1], re = s_row[r][2];
+      double p[3];
+      p[0] = (re + h) * coslat * coslon;
+      p[1] = (re + h) * coslat * sinlon;
+      p[2] = (re * (1 - kRe2D) + h) * sinlat;
+      double dr[3];
+      zero_doppler(P.orbit, p, t, st, dr);
+      const double rng = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+      const double rgoff = (rng - P.rngstart) * inv_dmrg;
+      const double azoff = (t - P.tstart) * prf;
+      // validity window, geo2rdr.cu:208-209
+      bool valid = rgoff > P.first_valid_sample && rgoff < P.last_valid_sample - 1 &&
+                   azoff >= P.first_valid_line + 5 && azoff < P.last_valid_line - 5;
+      const int intr = (int)rgoff, inta = (int)azoff;
+      // the 2x2 neighbourhood must lie inside the burst even if the validity
+      // limits passed in exceed the raster
+      valid = valid && intr >= 0 && intr + 1 < P.samples && inta >= 0 && inta + 1 < P.lines;
+      if (valid) {
+        // per-pixel TOPS reramp (geo2rdr.cu:210-219); kt = ka ks / (ka - ks)
+        // and etac = -fnc / ka share one reciprocal of ka (ka - ks)
+        const double tr = rng * two_over_c;
+        double dt = tr - P.fm[0];
+        const double ka = P.fm[1] + dt * (P.fm[2] + P.fm[3] * dt);
+        dt = tr - P.dc[0];
+        const double fnc = P.dc[1] + dt * (P.dc[2] + P.dc[3] * dt);
+        const double kmk = ka - P.ks;
+        const double inv = 1.0 / (ka * kmk);
+        const double kt = ka * P.ks * (ka * inv);
+        const double etaref = -fnc * (kmk * inv) - P.etac0;
+        const double eta = -P.lines * P.dtaz / 2. + t - P.tstart;
+        const double ed = eta - etaref;
+        const double reramp = -kPiD * kt * ed * ed;
+        // bilinear interpolation of the deramped burst (geo2rdr.cu:220-237)
+        const float fr = (float)(rgoff - intr), fa = (float)(azoff - inta);
+        const size_t i1 = (size_t)inta * P.samples + intr;
+        const float2 b1 = __ldg(burst + i1), b2 = __ldg(burst + i1 + 1);
+        const float2 b3 = __ldg(burst + i1 + P.samples), b4 = __ldg(burst + i1 + P.samples + 1);
+        const float2 c1 = make_float2(fmaf(fr, b2.x - b1.x, b1.x), fmaf(fr, b2.y - b1.y, b1.y));
+        const float2 c2 = make_float2(fmaf(fr, b4.x - b3.x, b3.x), fmaf(fr, b4.y - b3.y, b3.y));
+        const float2 v = make_float2(fmaf(fa, c2.x - c1.x, c1.x), fmaf(fa, c2.y - c1.y, c1.y));
+        // range phase and reramp (geo2rdr.cu:238-243)
+        res = cmul(v, phasor(P.k4pi_wvl * rng - reramp));
+      }
+      __stcs(out + (size_t)row * ncol + col, res);
+    }
+    // first / last non-zero output row (geo2rdr.cu:86-128): one vote per warp
+    const unsigned nz = __ballot_sync(0xffffffffu, colok && (res.x != 0.f || res.y != 0.f));
+    if (nz && (tx & 31) == 0 && rows) {
+      atomicMin(rows, row);
+      atomicMax(rows + 1, row + 1);
+    }
   }
 }
 
@@ -243,9 +255,9 @@ extern "C" int s1b_geo2rdr(const s1b_burst_plan_t *plan, const int16_t *dem, int
     int s = s1b_launch_status();
     if (s) return s;
   }
-  dim3 block(G_TX, G_TY);
-  dim3 grid((ncol + G_TX - 1) / G_TX, (nrow + G_TY - 1) / G_TY);
-  geo2rdr_kernel<<<grid, block, 0, st>>>(*plan, dem, dem_pitch, (const float2 *)deramped,
+  dim3 grid((ncol + G_TX - 1) / G_TX, (nrow + G_RY - 1) / G_RY);
+  if (grid.y > 65535) return s1b_fail(S1B_ERR_TOO_LARGE, "s1b_geo2rdr: DEM window too tall");
+  geo2rdr_kernel<<<grid, G_TX, 0, st>>>(*plan, dem, dem_pitch, (const float2 *)deramped,
                                          (float2 *)out, rows, nrow, ncol);
   return s1b_launch_status();
 }

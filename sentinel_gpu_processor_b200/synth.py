@@ -470,3 +470,25 @@ def make_frame(seed=20261203, device="cpu", n_swaths=3, n_bursts=9, baseline=150
     return PairScene(name="frame", seed=seed, ref=refs, sec=secs, rsc=rsc, dem=dem, ref_slc=ref_slc,
                      sec_slc=sec_slc, rowlook=rowlook, collook=collook, alpha=alpha,
                      extra={"coherence": cohs, "hmax": hmax})
+
+
+def frame_pair(frame: PairScene, k: int, margin: int = 64) -> PairScene:
+    """Burst pair ``k`` of a frame as its own PairScene, on the part of the
+    frame's DEM grid that covers both bursts' footprints (plus a margin)."""
+    from . import plan as _plan
+    ref, sec = frame.ref[k], frame.sec[k]
+    wins = []
+    for a in (ref, sec):
+        p = _plan.burst_plan(a.radar, a.orbit, a.fm, a.dc, a.bursts[0], frame.rsc)
+        wins.append(p.window)
+    r = frame.rsc
+    left = max(0, min(w[0] for w in wins) - margin)
+    top = max(0, min(w[1] for w in wins) - margin)
+    right = min(r.nlon, max(w[2] for w in wins) + margin)
+    bottom = min(r.nlat, max(w[3] for w in wins) + margin)
+    sub = formats.rsc_roundtrip(formats.Rsc(nlat=bottom - top, nlon=right - left, latmax=r.latmax + r.dlat * top,
+                                            lonmin=r.lonmin + r.dlon * left, dlat=r.dlat, dlon=r.dlon))
+    dem = make_dem(sub, frame.seed, frame.extra["hmax"], device=frame.dem.device)
+    return PairScene(name=f"frame[{k}]", seed=frame.seed, ref=[ref], sec=[sec], rsc=sub, dem=dem,
+                     ref_slc=[frame.ref_slc[k]], sec_slc=[frame.sec_slc[k]], rowlook=frame.rowlook,
+                     collook=frame.collook, alpha=frame.alpha, extra={"hmax": frame.extra["hmax"]})
