@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="s1b", choices=["s1b", "reference"])
-    ap.add_argument("--config", default="frame", choices=["frame", "c1", "c0", "small"])
+    ap.add_argument("--config", default="frame", choices=["frame", "c1", "c1geo", "c0", "small"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -245,12 +245,23 @@ def _workload(args, rank, dev):
         desc = (f"full IW frame: {len(sc.ref)} bursts (3 subswaths x 9) of uneven size, lines 1480-1530, samples "
                 f"20000-25500, 100-line overlap (configs[2])")
         return sc, chain, lambda: chain.run(*ins), desc
-    sc = make_scene(args.config, 20261203 + 1000 + rank, dev)
+    if args.config == "c1":
+        from sentinel_gpu_processor_b200.chain import RadarChain
+        sc = synth.make_radar_pair("c1", seed=20261203 + 1000 + rank, device=dev)
+        chain = RadarChain(sc.ref, sc.sec, sc.ref_slc.shape[0], sc.ref_slc.shape[1], sc.rowlook, sc.collook,
+                           sc.alpha, device=dev)
+        ins = (sc.ref_slc, sc.sec_slc, sc.lat, sc.lon, sc.hgt)
+        chain.capture(*ins)
+        desc = (f"one IW burst pair {sc.ref_slc.shape[0]} x {sc.ref_slc.shape[1]} complex64 with float64 lat/lon/hgt "
+                "rasters of the reference grid; 8-tap sinc resampling, 5 x 5 coherence; one CUDA graph per step "
+                "(configs[1])")
+        return sc, chain, chain.replay, desc
+    sc = make_scene("c1" if args.config == "c1geo" else args.config, 20261203 + 1000 + rank, dev)
     chain = PairChain(sc.ref[0], sc.sec[0], sc.rsc, sc.rowlook, sc.collook, sc.alpha, device=dev)
     ins = (sc.ref_slc[0], sc.sec_slc[0], sc.dem)
     p0 = chain.plans[0]
-    desc = f"one IW burst pair {p0.lines} x {p0.samples} complex64 (configs[1])" if args.config == "c1" else \
-        f"burst pair {p0.lines} x {p0.samples} ({args.config})"
+    desc = (f"one IW burst pair {p0.lines} x {p0.samples} complex64, geocoded on the DEM grid as the reference "
+            f"does (configs[1] sizes)") if args.config == "c1geo" else f"burst pair {p0.lines} x {p0.samples} ({args.config})"
     return sc, chain, lambda: chain.run(*ins), desc
 
 
@@ -258,6 +269,8 @@ def _e2e(chain, sc, args, world):
     """End-to-end rate through host buffers: pinned H2D of every SLC and the DEM,
     the chain, D2H of ifg/amplitudes/coherence/filtered ifg, per step."""
     import torch
+    if args.config == "c1":
+        return _e2e_radar(chain, sc, args, world)
     frame = args.config == "frame"
     refs = sc.ref_slc if frame else sc.ref_slc[:1]
     secs = sc.sec_slc if frame else sc.sec_slc[:1]
@@ -305,6 +318,113 @@ def _e2e(chain, sc, args, world):
     return world * k_e2e * chain.burst_pixels / (e2e_ms / 1e3), h2d, d2h
 
 
+def _e2e_radar(chain, sc, args, world):
+    """End to end for the radar-grid chain: pinned H2D of both SLCs and the
+    float64 lat/lon/height rasters into the graph's input tensors, graph
+    replay, D2H of ifg, amplitudes, looked and full-resolution coherence and
+    the filtered ifg."""
+    import torch
+    dev_ins = (sc.ref_slc, sc.sec_slc, sc.lat, sc.lon, sc.hgt)
+    host_ins = [t.cpu().pin_memory() for t in dev_ins]
+    h2d = sum(t.numel() * t.element_size() for t in host_ins)
+    outs = chain.outs
+    names = ("ifg", "amp1", "amp2", "coh", "filt", "coh_full")
+    host_out = {n: torch.empty(outs[n].shape, dtype=outs[n].dtype, pin_memory=True) for n in names}
+    d2h = sum(t.numel() * t.element_size() for t in host_out.values())
+
+    def step():
+        for d, h in zip(dev_ins, host_ins):
+            d.copy_(h, non_blocking=True)
+        chain.replay()
+        for n in names:
+            host_out[n].copy_(outs[n], non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+
+    step()
+    k_e2e = max(3, args.steps // 2)
+    barrier(world)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    s2, t2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s2.record(stream)
+    for _ in range(k_e2e):
+        step()
+    t2.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(s2.elapsed_time(t2), world)
+    return world * k_e2e * chain.burst_pixels / (e2e_ms / 1e3), h2d, d2h
+
+
+KERNELS = ("deramp", "geo2rdr", "crossmul_looks", "goldstein", "geo2rdr_offsets", "resample", "box_coherence")
+
+
+def _instrumented(run, steps):
+    """Per-entry-point device times over ``steps`` eager steps: the library call
+    of every s1b entry point is bracketed by CUDA events on the current stream
+    (kernels.timer hook).  Returns {name: [ms, ...]}."""
+    import contextlib
+
+    import torch
+
+    from sentinel_gpu_processor_b200 import kernels as K
+    rec = {}
+
+    @contextlib.contextmanager
+    def timer(name):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        yield
+        e1.record()
+        rec.setdefault(name, []).append((e0, e1))
+
+    K.timer = timer
+    try:
+        for _ in range(steps):
+            run()
+        torch.cuda.synchronize()
+    finally:
+        K.timer = None
+    return {n: [a.elapsed_time(b) for a, b in v] for n, v in rec.items() if n in KERNELS}
+
+
+def _radar_inputs(sc):
+    return (sc.ref_slc, sc.sec_slc, sc.lat, sc.lon, sc.hgt)
+
+
+def _kernel_table(chain, sc, args, times, peak):
+    """Algorithmic bytes per launch and achieved GB/s for each entry point."""
+    rows = {}
+    if args.config == "c1":
+        px = chain.burst_pixels
+        ml = (chain.box[3] // chain.rowlook) * (chain.box[2] // chain.collook)
+        box_px = chain.box[2] * chain.box[3]
+        bytes_per = {"geo2rdr_offsets": 32 * px, "resample": 24 * px, "crossmul_looks": 16 * box_px + 20 * ml,
+                     "box_coherence": 20 * px, "goldstein": 16 * ml}
+    else:
+        pls = [p for pl in chain.pairs for p in pl] if args.config == "frame" else chain.plans
+        n = len(pls)
+        burst = sum(p.lines * p.samples for p in pls) / n
+        geo = sum(p.nrow * p.ncol for p in pls) / n
+        bytes_per = {"deramp": 16 * burst, "geo2rdr": GEO_BYTES_PER_GEO_PX * geo + GEO_BYTES_PER_BURST_PX * burst}
+        if args.config == "frame":
+            res = chain.last
+            box_px = sum((r.box[2] - r.box[0]) * (r.box[3] - r.box[1]) for r in res) / len(res)
+            ml = sum(r.ifg.numel() for r in res) / len(res)
+        else:
+            r = chain.last
+            box_px = (r.box[2] - r.box[0]) * (r.box[3] - r.box[1])
+            ml = r.ifg.numel()
+        bytes_per.update({"crossmul_looks": 16 * box_px + 20 * ml, "goldstein": 16 * ml})
+    for name, ts in times.items():
+        if name not in bytes_per:
+            continue
+        ms = sum(ts) / len(ts)
+        gbs = bytes_per[name] / (ms / 1e3) / 1e9
+        rows[name] = {"launches": len(ts), "avg_ms": ms, "total_ms": sum(ts), "bytes_per_launch": bytes_per[name],
+                      "achieved_gbs": gbs, "frac": gbs / peak}
+    return rows
+
+
 def run_s1b(args):
     import torch
     rank, world, local = dist_setup(args.gpus)
@@ -318,7 +438,6 @@ def run_s1b(args):
     if res is None or (isinstance(res, list) and any(r is None for r in res)):
         raise SystemExit("empty interferogram for the synthetic input")
     stream = torch.cuda.current_stream()
-    chain.geo_events = []
     clocks = Clocks(local)
     barrier(world)
     torch.cuda.synchronize()
@@ -331,37 +450,43 @@ def run_s1b(args):
     stop.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    ev = chain.geo_events
     chain.geo_events = None
     barrier(world)
     elapsed_ms = max_over_ranks(start.elapsed_time(stop), world)
-    geo_ms = [a.elapsed_time(b) for a, b in ev]
-    geo_avg_ms = sum(geo_ms) / len(geo_ms)
     value = world * args.steps * chain.burst_pixels / (elapsed_ms / 1e3)
     e2e, h2d, d2h = _e2e(chain, sc, args, world)
 
-    if args.config == "frame":
-        geo_px = chain.geo_pixels()
-        burst_px = chain.burst_pixels_all()
-        launches = chain.launches_per_step()
-        ml = [list(r.ifg.shape) for r in res]
-        extra = {"bursts": len(chain.pairs), "burst_px_per_step": chain.burst_pixels,
-                 "ifg_ml_shapes_first3": ml[:3]}
+    if isinstance(res, list):
+        chain.last = res
     else:
-        geo_px = [p.nrow * p.ncol for p in chain.plans]
-        burst_px = [p.lines * p.samples for p in chain.plans]
-        launches = chain.launches_per_step()
-        extra = {"lines": chain.plans[0].lines, "samples": chain.plans[0].samples, "ifg_ml": list(res.ifg.shape)}
+        chain.last = res
     peak, peak_kind = peaks()
-    geo_bytes = (GEO_BYTES_PER_GEO_PX * sum(geo_px) + GEO_BYTES_PER_BURST_PX * sum(burst_px)) / len(geo_px)
-    achieved = geo_bytes / (geo_avg_ms / 1e3) / 1e9
+    times = _instrumented(run if args.config != "c1" else (lambda: chain.run(*_radar_inputs(sc))),
+                          max(2, min(args.steps, 10)))
+    table = _kernel_table(chain, sc, args, times, peak)
+    top = max(table, key=lambda n: table[n]["total_ms"])
+    if args.config == "frame":
+        extra = {"bursts": len(chain.pairs), "burst_px_per_step": chain.burst_pixels,
+                 "geo_px_total": sum(chain.geo_pixels()),
+                 "ifg_ml_shapes_first3": [list(r.ifg.shape) for r in res[:3]]}
+        launches = chain.launches_per_step()
+    elif args.config == "c1":
+        extra = {"lines": chain.L, "samples": chain.S, "ifg_ml": list(res["ifg"].shape), "interp": chain.interp,
+                 "coherence_window": chain.win, "cuda_graph": True}
+        launches = chain.launches_per_step()
+    else:
+        extra = {"lines": chain.plans[0].lines, "samples": chain.plans[0].samples,
+                 "geo_px_total": sum(p.nrow * p.ncol for p in chain.plans), "ifg_ml": list(res.ifg.shape)}
+        launches = chain.launches_per_step()
     traffic = None
-    if GEO_DRAM_BYTES_PER_GEO_PX is not None:
-        traffic = GEO_DRAM_BYTES_PER_GEO_PX * sum(geo_px) / len(geo_px)
+    if top == "geo2rdr" and GEO_DRAM_BYTES_PER_GEO_PX is not None:
+        pls = [p for pl in chain.pairs for p in pl] if args.config == "frame" else chain.plans
+        traffic = GEO_DRAM_BYTES_PER_GEO_PX * sum(p.nrow * p.ncol for p in pls) / len(pls)
     cfg = {"workload": desc, "looks": [sc.rowlook, sc.collook],
-           "goldstein": {"alpha": sc.alpha, "n_win": 32, "step": 8}, "geo_px_total": sum(geo_px),
+           "goldstein": {"alpha": sc.alpha, "n_win": 32, "step": 8},
            "l2": "inputs larger than L2 (>= 252 MB per SLC, read once per step)", "parallelism": f"replicas{world}"}
     cfg.update(extra)
+    t = table[top]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": warm, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
@@ -369,13 +494,13 @@ def run_s1b(args):
         "config": cfg,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches * args.steps,
-        "roofline": {"bound": "hbm", "kernel": "geo2rdr_kernel", "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                     "peak_kind": peak_kind, "bytes_per_launch": geo_bytes, "launch_ms": geo_avg_ms,
-                     "note": "geocoding is FP64-compute bound (zero-Doppler Newton); its HBM fraction is low "
-                             "by design"},
-        "kernels_ms": {"geo2rdr_avg": geo_avg_ms, "geo2rdr_share": sum(geo_ms) / (elapsed_ms * world / world),
-                       "step": elapsed_ms / args.steps},
+        "roofline": {"bound": "hbm", "kernel": top, "achieved": t["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                     "frac": t["frac"], "traffic": traffic, "peak_kind": peak_kind,
+                     "bytes_per_launch": t["bytes_per_launch"], "launch_ms": t["avg_ms"],
+                     "timed": "CUDA events around every launch of the entry point over instrumented eager steps",
+                     "note": ("FP64-compute bound (zero-Doppler Newton): low HBM fraction by design"
+                              if top in ("geo2rdr", "geo2rdr_offsets") else "HBM-bound")},
+        "kernels": table,
     }
     if clk is not None:
         line["clocks"] = clk

@@ -232,6 +232,42 @@ int s1b_crossmul_box(const int32_t *hdr1, const int32_t *hdr2, int32_t rowlook,
                      int32_t collook, int32_t use_union, int32_t *box_out,
                      int32_t *hdr_out);
 
+/* ------------------------------------------------- radar-grid coregistration
+ * (no reference counterpart: the reference geocodes every SLC onto a lat/lon
+ * grid instead; these resample the secondary onto the reference radar grid
+ * with the reference's geometry and TOPS formulas). */
+
+#define S1B_INTERP_BILINEAR 0
+#define S1B_INTERP_SINC8 1
+
+/* Secondary sample coordinates of every pixel of the reference radar grid:
+ * for float64 lat/lon/height rasters [lines * samples] of the reference
+ * grid, the zero-Doppler time and range on the secondary orbit of `plan`
+ * (the formulas of csrc/src/geo2rdr.cu:197-207), stored as float32 offsets
+ * relative to the pixel index: az_off = az - row, rg_off = rg - column. */
+int s1b_geo2rdr_offsets(const s1b_burst_plan_t *plan, const double *lat, const double *lon,
+                        const double *hgt, int32_t lines, int32_t samples, float *az_off,
+                        float *rg_off, void *stream);
+
+/* Resample the secondary burst of `plan` (complex64 [plan->lines *
+ * plan->samples], as acquired, TOPS-modulated) onto the reference grid:
+ * deramp (geo2rdr.cu:138-158), interpolate at (row + az_off, col + rg_off)
+ * with an 8-tap windowed sinc (S1B_INTERP_SINC8: weights sinc(k-f) *
+ * (0.5 + 0.5 cos(pi (k-f)/4)), k = -3..4, normalised) or bilinear, reramp with
+ * the secondary's TOPS phase at the fractional position.  Pixels whose kernel
+ * support leaves the burst are 0.  out: complex64 [lines * samples]. */
+int s1b_resample(const s1b_burst_plan_t *plan, const void *sec, const float *az_off,
+                 const float *rg_off, int32_t lines, int32_t samples, int32_t interp, void *out,
+                 void *stream);
+
+/* Coherence |sum conj(ref) sec| / sqrt(sum |ref|^2 sum |sec|^2) over win x win
+ * boxes at full resolution (win odd, <= 9; windows clipped at the raster
+ * border), sums compensated in float32.  ref/sec: complex64 [lines *
+ * samples]; coh: float32 [lines * samples]; status: int32 device word, set
+ * to 1 if a tile's shared-memory staging did not complete (not expected). */
+int s1b_box_coherence(const void *ref, const void *sec, int32_t lines, int32_t samples, int32_t win,
+                      float *coh, int32_t *status, void *stream);
+
 /* ------------------------------------------------------------ Goldstein */
 
 /* Scratch bytes s1b_goldstein needs for an nrow x ncol image. */

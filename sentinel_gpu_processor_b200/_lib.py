@@ -21,6 +21,8 @@ S1B_ERR_EMPTY = 4
 S1B_ERR_NO_DEVICE = 5
 S1B_ERR_UNSUPPORTED = 6
 MAX_STATE_VECTORS = 64
+S1B_INTERP_BILINEAR = 0
+S1B_INTERP_SINC8 = 1
 MAX_WIN = MAX_STATE_VECTORS - 3
 
 
@@ -114,6 +116,11 @@ _SIGNATURES = {
                                    c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_uint64, c_void_p]),
     "s1b_crossmul_box": (c_int, [POINTER(c_int32), POINTER(c_int32), c_int32, c_int32, c_int32,
                                  POINTER(c_int32), POINTER(c_int32)]),
+    "s1b_geo2rdr_offsets": (c_int, [POINTER(BurstPlan), c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p,
+                                    c_void_p, c_void_p]),
+    "s1b_resample": (c_int, [POINTER(BurstPlan), c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p,
+                             c_void_p]),
+    "s1b_box_coherence": (c_int, [c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p, c_void_p, c_void_p]),
     "s1b_goldstein_scratch_bytes": (c_size_t, [c_int32, c_int32, c_int32]),
     "s1b_goldstein": (c_int, [c_void_p, c_void_p, c_int32, c_int32, c_int32, c_float, c_void_p, c_size_t,
                               c_void_p]),

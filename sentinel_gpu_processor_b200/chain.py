@@ -231,3 +231,76 @@ class FrameChain:
 
     def burst_pixels_all(self):
         return [p.lines * p.samples for pls in self.pairs for p in pls]
+
+
+class RadarChain:
+    """Radar-grid chain for one burst pair (configs[0]/[1] processing):
+    secondary offsets from the reference grid's float64 lat/lon/height,
+    TOPS-aware 8-tap sinc resampling of the secondary onto the reference grid,
+    crossmul + multilook + amplitude looks, 5 x 5 full-resolution coherence,
+    Goldstein.  No host synchronisation: a step can be captured in a CUDA
+    graph (``capture``) and replayed."""
+
+    def __init__(self, ref_acq, sec_acq, lines, samples, rowlook, collook, alpha, win=5, n_win=32,
+                 interp="sinc8", device="cuda", fill_seed=0):
+        self.dev = torch.device(device)
+        self.sec_plan = _plan.burst_plan(sec_acq.radar, sec_acq.orbit, sec_acq.fm, sec_acq.dc, sec_acq.bursts[0],
+                                         None)
+        self.L, self.S = int(lines), int(samples)
+        self.rowlook, self.collook, self.alpha, self.win, self.n_win = (int(rowlook), int(collook), float(alpha),
+                                                                        int(win), int(n_win))
+        self.interp = interp
+        self.fill_seed = int(fill_seed)
+        L, S = self.L, self.S
+        self.az = torch.empty((L, S), dtype=torch.float32, device=self.dev)
+        self.rg = torch.empty((L, S), dtype=torch.float32, device=self.dev)
+        self.sec_rs = torch.empty((L, S), dtype=torch.complex64, device=self.dev)
+        self.coh_full = torch.empty((L, S), dtype=torch.float32, device=self.dev)
+        self.status = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        self.box = (0, 0, (S // self.collook) * self.collook, (L // self.rowlook) * self.rowlook)
+        nml = (L // self.rowlook, S // self.collook)
+        need = kernels.goldstein_scratch_bytes(nml[0], nml[1], self.n_win) if min(nml) >= self.n_win else 0
+        self.scratch = torch.empty(max(need, 1), dtype=torch.uint8, device=self.dev)
+        self.filt = torch.empty(nml, dtype=torch.complex64, device=self.dev)
+        self.burst_pixels = L * S
+        self.outs = None
+        self.graph = None
+        self.geo_events = None
+
+    def run(self, ref_slc, sec_slc, lat, lon, hgt):
+        ev = _start_event(self.geo_events)
+        kernels.geo2rdr_offsets(self.sec_plan, lat, lon, hgt, self.az, self.rg)
+        _end_event(self.geo_events, ev)
+        kernels.resample(self.sec_plan, sec_slc, self.az, self.rg, self.interp, out=self.sec_rs)
+        outs = kernels.crossmul_looks(ref_slc, (0, 0), self.sec_rs, (0, 0), self.box, self.rowlook, self.collook,
+                                      fill_seed=self.fill_seed)
+        kernels.box_coherence(ref_slc, self.sec_rs, self.win, out=self.coh_full, status=self.status)
+        if self.filt.shape[0] >= self.n_win and self.filt.shape[1] >= self.n_win:
+            kernels.goldstein(outs["ifg"], self.alpha, self.n_win, out=self.filt, scratch=self.scratch)
+        outs["filt"] = self.filt
+        outs["coh_full"] = self.coh_full
+        self.outs = outs
+        return outs
+
+    def capture(self, ref_slc, sec_slc, lat, lon, hgt):
+        """Record one step into a CUDA graph on static inputs; ``replay()`` reruns it."""
+        self.run(ref_slc, sec_slc, lat, lon, hgt)  # warm-up outside the capture (attributes, scratch)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(g, stream=s):
+                self.run(ref_slc, sec_slc, lat, lon, hgt)
+        torch.cuda.current_stream().wait_stream(s)
+        self.graph = g
+        return self.outs
+
+    def replay(self):
+        self.graph.replay()
+        return self.outs
+
+    @staticmethod
+    def launches_per_step():
+        # offsets, resample, crossmul, box coherence (+ status memset), goldstein patch + gather
+        return 6

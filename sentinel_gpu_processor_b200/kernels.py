@@ -12,6 +12,17 @@ import torch
 
 from . import _lib
 
+# Optional timing hook: a callable name -> context manager wrapped around the
+# library call of each entry point (bench.py brackets them with CUDA events).
+timer = None
+
+
+def _call(name, fn, *args):
+    if timer is None:
+        return fn(*args)
+    with timer(name):
+        return fn(*args)
+
 
 def _need_cuda(*ts):
     for t in ts:
@@ -33,7 +44,7 @@ def deramp(plan: _lib.BurstPlan, slc: torch.Tensor, out: torch.Tensor | None = N
     if out is None:
         out = torch.empty_like(slc)
     lib = _lib.load()
-    _lib.check(lib.s1b_deramp(ctypes.byref(plan), _lib.dptr(slc), _lib.dptr(out), _lib.stream_ptr()),
+    _lib.check(_call("deramp", lib.s1b_deramp, ctypes.byref(plan), _lib.dptr(slc), _lib.dptr(out), _lib.stream_ptr()),
                "s1b_deramp")
     return out
 
@@ -65,7 +76,7 @@ def geo2rdr(plan: _lib.BurstPlan, dem: torch.Tensor, deramped: torch.Tensor, out
     if rows is None:
         rows = torch.empty(2, dtype=torch.int32, device=deramped.device)
     lib = _lib.load()
-    _lib.check(lib.s1b_geo2rdr(ctypes.byref(plan), _lib.dptr(win), win.stride(0), _lib.dptr(deramped),
+    _lib.check(_call("geo2rdr", lib.s1b_geo2rdr, ctypes.byref(plan), _lib.dptr(win), win.stride(0), _lib.dptr(deramped),
                                _lib.dptr(out), _lib.dptr(rows), _lib.stream_ptr()), "s1b_geo2rdr")
     return out, rows
 
@@ -93,7 +104,7 @@ def crossmul_looks(ref, ref_box, sec, sec_box, box, rowlook, collook, want=("ifg
         if k in want:
             outs[k] = torch.empty(shape, dtype=torch.float32, device=dev)
     lib = _lib.load()
-    _lib.check(lib.s1b_crossmul_looks(
+    _lib.check(_call("crossmul_looks", lib.s1b_crossmul_looks, 
         _lib.dptr(ref), ref_box[0], ref_box[1], ref.shape[1], ref.shape[0],
         _lib.dptr(sec), sec_box[0], sec_box[1], sec.shape[1], sec.shape[0],
         left, top, nrow_ml, ncol_ml, rowlook, collook,
@@ -119,7 +130,7 @@ def goldstein(img: torch.Tensor, alpha: float, n_win: int = 32, out: torch.Tenso
     if out is None:
         out = torch.empty_like(img)
     lib = _lib.load()
-    _lib.check(lib.s1b_goldstein(_lib.dptr(img), _lib.dptr(out), nrow, ncol, n_win, float(alpha),
+    _lib.check(_call("goldstein", lib.s1b_goldstein, _lib.dptr(img), _lib.dptr(out), nrow, ncol, n_win, float(alpha),
                                  _lib.dptr(scratch), scratch.numel() * scratch.element_size(),
                                  _lib.stream_ptr()), "s1b_goldstein")
     return out
@@ -132,7 +143,7 @@ def zero_doppler(poly: _lib.OrbitPoly, xyz: torch.Tensor, tline0: float):
     n = xyz.shape[0]
     t = torch.empty(n, dtype=torch.float64, device=xyz.device)
     dr = torch.empty((n, 3), dtype=torch.float64, device=xyz.device)
-    _lib.check(_lib.load().s1b_zero_doppler(ctypes.byref(poly), _lib.dptr(xyz), n, float(tline0), _lib.dptr(t),
+    _lib.check(_call("zero_doppler", _lib.load().s1b_zero_doppler, ctypes.byref(poly), _lib.dptr(xyz), n, float(tline0), _lib.dptr(t),
                                             _lib.dptr(dr), _lib.stream_ptr()), "s1b_zero_doppler")
     return t, dr
 
@@ -141,6 +152,62 @@ def llh2xyz(llh: torch.Tensor) -> torch.Tensor:
     _need_cuda(llh)
     llh = llh.contiguous().to(torch.float64)
     out = torch.empty_like(llh)
-    _lib.check(_lib.load().s1b_llh2xyz(_lib.dptr(llh), _lib.dptr(out), llh.shape[0], _lib.stream_ptr()),
+    _lib.check(_call("llh2xyz", _lib.load().s1b_llh2xyz, _lib.dptr(llh), _lib.dptr(out), llh.shape[0], _lib.stream_ptr()),
                "s1b_llh2xyz")
+    return out
+
+
+def geo2rdr_offsets(plan: _lib.BurstPlan, lat: torch.Tensor, lon: torch.Tensor, hgt: torch.Tensor,
+                    az_off: torch.Tensor | None = None, rg_off: torch.Tensor | None = None):
+    """Secondary sample offsets (az_off, rg_off float32 [L, S]) of the reference
+    grid pixels whose float64 lat/lon/height rasters are given."""
+    _need_cuda(lat, lon, hgt, az_off, rg_off)
+    for t in (lat, lon, hgt):
+        if t.dtype != torch.float64 or not t.is_contiguous() or t.shape != lat.shape:
+            raise ValueError("lat/lon/hgt must be contiguous float64 rasters of one shape")
+    L, S = lat.shape
+    if az_off is None:
+        az_off = torch.empty((L, S), dtype=torch.float32, device=lat.device)
+    if rg_off is None:
+        rg_off = torch.empty((L, S), dtype=torch.float32, device=lat.device)
+    _lib.check(_call("geo2rdr_offsets", _lib.load().s1b_geo2rdr_offsets, ctypes.byref(plan), _lib.dptr(lat), _lib.dptr(lon), _lib.dptr(hgt),
+                                               L, S, _lib.dptr(az_off), _lib.dptr(rg_off), _lib.stream_ptr()),
+               "s1b_geo2rdr_offsets")
+    return az_off, rg_off
+
+
+def resample(plan: _lib.BurstPlan, sec: torch.Tensor, az_off: torch.Tensor, rg_off: torch.Tensor,
+             interp: str = "sinc8", out: torch.Tensor | None = None) -> torch.Tensor:
+    """Resample the secondary burst of ``plan`` onto the grid of the offsets."""
+    _need_cuda(sec, az_off, rg_off, out)
+    _c64(sec, "sec")
+    if sec.numel() != plan.lines * plan.samples:
+        raise ValueError("sec size does not match the plan")
+    if az_off.shape != rg_off.shape or az_off.dtype != torch.float32 or not az_off.is_contiguous() \
+            or not rg_off.is_contiguous():
+        raise ValueError("az_off/rg_off must be contiguous float32 rasters of one shape")
+    L, S = az_off.shape
+    if out is None:
+        out = torch.empty((L, S), dtype=torch.complex64, device=sec.device)
+    mode = {"sinc8": _lib.S1B_INTERP_SINC8, "bilinear": _lib.S1B_INTERP_BILINEAR}[interp]
+    _lib.check(_call("resample", _lib.load().s1b_resample, ctypes.byref(plan), _lib.dptr(sec), _lib.dptr(az_off), _lib.dptr(rg_off),
+                                        L, S, mode, _lib.dptr(out), _lib.stream_ptr()), "s1b_resample")
+    return out
+
+
+def box_coherence(ref: torch.Tensor, sec: torch.Tensor, win: int = 5, out: torch.Tensor | None = None,
+                  status: torch.Tensor | None = None) -> torch.Tensor:
+    """Full-resolution win x win boxcar coherence of two co-registered SLCs."""
+    _need_cuda(ref, sec, out, status)
+    _c64(ref, "ref")
+    _c64(sec, "sec")
+    if ref.shape != sec.shape:
+        raise ValueError("ref and sec must have one shape")
+    L, S = ref.shape
+    if out is None:
+        out = torch.empty((L, S), dtype=torch.float32, device=ref.device)
+    if status is None:
+        status = torch.empty(1, dtype=torch.int32, device=ref.device)
+    _lib.check(_call("box_coherence", _lib.load().s1b_box_coherence, _lib.dptr(ref), _lib.dptr(sec), L, S, int(win), _lib.dptr(out),
+                                             _lib.dptr(status), _lib.stream_ptr()), "s1b_box_coherence")
     return out

@@ -492,3 +492,157 @@ def frame_pair(frame: PairScene, k: int, margin: int = 64) -> PairScene:
     return PairScene(name=f"frame[{k}]", seed=frame.seed, ref=[ref], sec=[sec], rsc=sub, dem=dem,
                      ref_slc=[frame.ref_slc[k]], sec_slc=[frame.sec_slc[k]], rowlook=frame.rowlook,
                      collook=frame.collook, alpha=frame.alpha, extra={"hmax": frame.extra["hmax"]})
+
+
+# ----------------------------------------------------------------------------
+# Radar-grid scenes (float64 lat/lon/height rasters of the reference grid)
+# ----------------------------------------------------------------------------
+
+def _xyz2llh_t(x, y, z):
+    """ECEF -> geodetic by fixed-point iteration (torch float64)."""
+    import torch
+    lon = torch.atan2(y, x)
+    p = torch.sqrt(x * x + y * y)
+    lat = torch.atan2(z, p * (1 - RE2))
+    for _ in range(5):
+        n = RA / torch.sqrt(1 - RE2 * torch.sin(lat) ** 2)
+        h = p / torch.cos(lat) - n
+        lat = torch.atan2(z, p * (1 - RE2 * n / (n + h)))
+    n = RA / torch.sqrt(1 - RE2 * torch.sin(lat) ** 2)
+    h = p / torch.cos(lat) - n
+    return torch.rad2deg(lat), torch.rad2deg(lon), h
+
+
+def rdr2geo_grid(orbit, radar, burst, height_fn, device="cpu", outer=4, steps=44):
+    """Ground point of every pixel of a burst: zero-Doppler plane at the line
+    time, slant range of the sample, on the terrain ``height_fn(lat, lon)``.
+
+    Bisection on the look angle in the plane orthogonal to the velocity
+    (right-looking), iterated ``outer`` times against the terrain height.
+    Returns float64 (lat, lon, hgt) tensors [lines, samples]."""
+    import torch
+
+    from . import plan as _plan
+    L, S = radar.lines_per_burst, radar.samples_per_burst
+    dtaz = 1.0 / radar.prf
+    t = burst.azimuth_time + dtaz * np.arange(L)
+    poly = _plan.orbit_poly(*orbit)
+    P, V = _plan.orbit_eval(poly, t)
+    P = torch.as_tensor(P, dtype=torch.float64, device=device)
+    V = torch.as_tensor(V, dtype=torch.float64, device=device)
+    d = -P / torch.linalg.norm(P, dim=1, keepdim=True)
+    d = d - (d * V).sum(1, keepdim=True) * V / (V * V).sum(1, keepdim=True)
+    d = d / torch.linalg.norm(d, dim=1, keepdim=True)
+    c = torch.cross(d, V, dim=1)
+    c = c / torch.linalg.norm(c, dim=1, keepdim=True)
+    r0 = radar.slant_range_time * SOL / 2.0
+    R = (r0 + (SOL / 2.0 / radar.range_sampling_rate) * torch.arange(S, dtype=torch.float64, device=device))[None, :]
+    h = torch.zeros((L, S), dtype=torch.float64, device=device)
+    for _ in range(outer):
+        lo = torch.zeros((L, S), dtype=torch.float64, device=device)
+        hi = torch.full((L, S), math.radians(80.0), dtype=torch.float64, device=device)
+        for _ in range(steps):
+            th = 0.5 * (lo + hi)
+            ct, st = torch.cos(th), torch.sin(th)
+            gx = P[:, 0:1] + R * (ct * d[:, 0:1] + st * c[:, 0:1])
+            gy = P[:, 1:2] + R * (ct * d[:, 1:2] + st * c[:, 1:2])
+            gz = P[:, 2:3] + R * (ct * d[:, 2:3] + st * c[:, 2:3])
+            _, _, hg = _xyz2llh_t(gx, gy, gz)
+            up = hg > h  # the ray rises with the angle
+            hi = torch.where(up, th, hi)
+            lo = torch.where(up, lo, th)
+        th = 0.5 * (lo + hi)
+        ct, st = torch.cos(th), torch.sin(th)
+        gx = P[:, 0:1] + R * (ct * d[:, 0:1] + st * c[:, 0:1])
+        gy = P[:, 1:2] + R * (ct * d[:, 1:2] + st * c[:, 1:2])
+        gz = P[:, 2:3] + R * (ct * d[:, 2:3] + st * c[:, 2:3])
+        lat, lon, hg = _xyz2llh_t(gx, gy, gz)
+        h = height_fn(lat, lon).to(torch.float64)
+    return lat.contiguous(), lon.contiguous(), hg.contiguous()
+
+
+def reflectivity(lat, lon, seed, lat0, lon0, n_waves=64, min_wavelength=60.0):
+    """Band-limited complex random field on the ground (torch complex64):
+    a sum of ``n_waves`` plane waves with random directions, wavelengths above
+    ``min_wavelength`` metres and random phases, normalised to unit power.
+    Both acquisitions sample it at their own ground points, so their images
+    of one scene are consistent up to resampling."""
+    import torch
+    rng = np.random.Generator(np.random.PCG64(seed))
+    north = (lat - lat0) * (math.pi / 180.0 * RA)
+    east = (lon - lon0) * (math.pi / 180.0 * RA * math.cos(math.radians(lat0)))
+    kmax = 2 * math.pi / min_wavelength
+    ang = rng.uniform(0, 2 * math.pi, n_waves)
+    kmag = kmax * np.sqrt(rng.uniform(0.0, 1.0, n_waves))
+    ph = rng.uniform(0, 2 * math.pi, n_waves)
+    amp = rng.standard_normal(n_waves) + 1j * rng.standard_normal(n_waves)
+    acc = torch.zeros(lat.shape, dtype=torch.complex128, device=lat.device)
+    for k in range(n_waves):
+        arg = kmag[k] * (math.cos(ang[k]) * north + math.sin(ang[k]) * east) + ph[k]
+        acc += complex(amp[k]) * torch.polar(torch.ones_like(arg), arg)
+    return (acc / math.sqrt(2.0 * n_waves)).to(torch.complex64)
+
+
+@dataclass
+class RadarPairScene:
+    """Reference/secondary burst pair for radar-grid coregistration."""
+    name: str
+    seed: int
+    ref: Acquisition
+    sec: Acquisition
+    lat: object  # float64 [L, S] of the reference grid
+    lon: object
+    hgt: object
+    ref_slc: object  # complex64 [L, S], TOPS-modulated
+    sec_slc: object
+    rowlook: int
+    collook: int
+    alpha: float
+    win: int = 5
+    n_win: int = 32
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def burst_pixels(self):
+        return int(self.ref_slc.shape[0]) * int(self.ref_slc.shape[1])
+
+
+def make_radar_pair(config="c1", seed=20261203, device="cpu", baseline=150.0, coherence=0.7,
+                    lines=None, samples=None, defo_amp=0.03, defo_sigma=5000.0):
+    """configs[0]/[1]-style pair: float64 lat/lon/height rasters of the
+    reference grid, a secondary with a perpendicular baseline, a band-limited
+    reflectivity seen by both, a Gaussian deformation (phase 4 pi d / lambda)
+    and coherence ``coherence`` against white noise."""
+    import torch
+    L, S, rl, cl, al, hmax, kt = CONFIGS[config]
+    L = int(lines or L)
+    S = int(samples or S)
+    t_c = ORBIT_T0 + 50.0
+    orbit_ref = make_orbit(t_c=t_c)
+    off = secondary_offset(orbit_ref, t_c, NEAR_RANGE + S * RANGE_SPACING / 2, baseline)
+    orbit_sec = make_orbit(t_c=t_c, offset=off)
+    radar = make_radar(L, S, hmin=-100.0, hmax=hmax + 100.0)
+    t_start = t_c - L * AZIMUTH_INTERVAL / 2
+    fm, dc = tops_tables(radar, t_c, kt)
+    burst = burst_meta(t_start, L, S, margin_l=4, margin_s=4)
+    ref = Acquisition(radar=radar, orbit=orbit_ref, fm=fm, dc=dc, bursts=[burst])
+    sec = Acquisition(radar=radar, orbit=orbit_sec, fm=fm.copy(), dc=dc.copy(), bursts=[burst])
+    hfun = lambda la, lo: fbm_height(la, lo, seed, hmax)
+    lat, lon, hgt = rdr2geo_grid(orbit_ref, radar, burst, hfun, device=device)
+    slat, slon, _ = rdr2geo_grid(orbit_sec, radar, burst, hfun, device=device)
+    lat0, lon0 = float(lat[L // 2, S // 2]), float(lon[L // 2, S // 2])
+    f_ref = reflectivity(lat, lon, seed, lat0, lon0)
+    f_sec = reflectivity(slat, slon, seed, lat0, lon0)
+    # deformation seen by the secondary: 2-D Gaussian in ground metres
+    north = (slat - lat0) * (math.pi / 180.0 * RA)
+    east = (slon - lon0) * (math.pi / 180.0 * RA * math.cos(math.radians(lat0)))
+    dphi = (4 * math.pi / WAVELENGTH) * defo_amp * torch.exp(-(north ** 2 + east ** 2) / (2 * defo_sigma ** 2))
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    noise = speckle(L, S, gen, device)
+    s_sec = coherence * f_sec * torch.polar(torch.ones_like(dphi), dphi).to(torch.complex64) + \
+        math.sqrt(1 - coherence ** 2) * noise
+    ref_slc = tops_modulate(f_ref, ref, burst).contiguous()
+    sec_slc = tops_modulate(s_sec.to(torch.complex64), sec, burst).contiguous()
+    return RadarPairScene(name=config, seed=seed, ref=ref, sec=sec, lat=lat, lon=lon, hgt=hgt, ref_slc=ref_slc,
+                          sec_slc=sec_slc, rowlook=rl, collook=cl, alpha=al, extra={"hmax": hmax})
