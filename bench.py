@@ -2,10 +2,10 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl s1b|reference] [--config frame|c1]
 
-A step is one pass of the chain over a full synthetic IW frame (default,
-configs[2]: 3 subswaths x 9 bursts of uneven size, lines 1480-1530, samples
+A step is one pass of the chain over a full synthetic IW frame (default:
+3 subswaths x 9 bursts of uneven size, lines 1480-1530, samples
 20000-25500, complex64, looks 4 x 20, Goldstein alpha 0.5, 32 x 32 patches)
-or over one IW burst pair (--config c1, configs[1]: 1500 x 21000, alpha 0.6):
+or over one IW burst pair (--config c1: 1500 x 21000, alpha 0.6):
 for every burst pair, TOPS deramp and FP64 geocoding of both SLCs onto the
 DEM grid, crossmul + multilook + amplitude looks + coherence, Goldstein.
 ``value`` = burst pixels (lines x samples of each reference burst, counted
@@ -243,7 +243,7 @@ def _workload(args, rank, dev):
         chain = FrameChain(sc.ref, sc.sec, sc.rsc, sc.rowlook, sc.collook, sc.alpha, device=dev)
         ins = (sc.ref_slc, sc.sec_slc, sc.dem)
         desc = (f"full IW frame: {len(sc.ref)} bursts (3 subswaths x 9) of uneven size, lines 1480-1530, samples "
-                f"20000-25500, 100-line overlap (configs[2])")
+                f"20000-25500, 100-line overlap")
         return sc, chain, lambda: chain.run(*ins), desc
     if args.config == "c1":
         from sentinel_gpu_processor_b200.chain import RadarChain
@@ -253,15 +253,14 @@ def _workload(args, rank, dev):
         ins = (sc.ref_slc, sc.sec_slc, sc.lat, sc.lon, sc.hgt)
         chain.capture(*ins)
         desc = (f"one IW burst pair {sc.ref_slc.shape[0]} x {sc.ref_slc.shape[1]} complex64 with float64 lat/lon/hgt "
-                "rasters of the reference grid; 8-tap sinc resampling, 5 x 5 coherence; one CUDA graph per step "
-                "(configs[1])")
+                "rasters of the reference grid; 8-tap sinc resampling, 5 x 5 coherence; one CUDA graph per step")
         return sc, chain, chain.replay, desc
     sc = make_scene("c1" if args.config == "c1geo" else args.config, 20261203 + 1000 + rank, dev)
     chain = PairChain(sc.ref[0], sc.sec[0], sc.rsc, sc.rowlook, sc.collook, sc.alpha, device=dev)
     ins = (sc.ref_slc[0], sc.sec_slc[0], sc.dem)
     p0 = chain.plans[0]
     desc = (f"one IW burst pair {p0.lines} x {p0.samples} complex64, geocoded on the DEM grid as the reference "
-            f"does (configs[1] sizes)") if args.config == "c1geo" else f"burst pair {p0.lines} x {p0.samples} ({args.config})"
+            f"does") if args.config == "c1geo" else f"burst pair {p0.lines} x {p0.samples} ({args.config})"
     return sc, chain, lambda: chain.run(*ins), desc
 
 
@@ -437,6 +436,8 @@ def run_s1b(args):
     torch.cuda.synchronize()
     if res is None or (isinstance(res, list) and any(r is None for r in res)):
         raise SystemExit("empty interferogram for the synthetic input")
+    if hasattr(chain, "staging_ok") and not chain.staging_ok():
+        raise SystemExit("a shared-memory staging copy did not complete")
     stream = torch.cuda.current_stream()
     clocks = Clocks(local)
     barrier(world)
@@ -541,7 +542,7 @@ def run_reference(args):
         base_sc.dem = base_sc.dem.cpu()
         base_sc.ref_slc = [t.cpu() for t in base_sc.ref_slc]
         base_sc.sec_slc = [t.cpu() for t in base_sc.sec_slc]
-        sample = "first burst pair of the frame (configs[2]) per step"
+        sample = "first burst pair of the frame per step"
     else:
         base_sc = make_scene(args.config, 20261203 + 1000, "cpu")
         sample = "one burst pair per step"

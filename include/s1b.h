@@ -255,10 +255,14 @@ int s1b_geo2rdr_offsets(const s1b_burst_plan_t *plan, const double *lat, const d
  * with an 8-tap windowed sinc (S1B_INTERP_SINC8: weights sinc(k-f) *
  * (0.5 + 0.5 cos(pi (k-f)/4)), k = -3..4, normalised) or bilinear, reramp with
  * the secondary's TOPS phase at the fractional position.  Pixels whose kernel
- * support leaves the burst are 0.  out: complex64 [lines * samples]. */
+ * support leaves the burst are 0.  out: complex64 [lines * samples];
+ * status: int32 device word, set to 1 if a tile's shared-memory staging did
+ * not complete (not expected).  When the rasters allow tensor maps (16-byte
+ * aligned bases, samples % 4 == 0, plan->samples even) tiles are staged by
+ * TMA in a persistent kernel; otherwise by plain loads. */
 int s1b_resample(const s1b_burst_plan_t *plan, const void *sec, const float *az_off,
                  const float *rg_off, int32_t lines, int32_t samples, int32_t interp, void *out,
-                 void *stream);
+                 int32_t *status, void *stream);
 
 /* Coherence |sum conj(ref) sec| / sqrt(sum |ref|^2 sum |sec|^2) over win x win
  * boxes at full resolution (win odd, <= 9; windows clipped at the raster

@@ -119,7 +119,7 @@ _SIGNATURES = {
     "s1b_geo2rdr_offsets": (c_int, [POINTER(BurstPlan), c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p,
                                     c_void_p, c_void_p]),
     "s1b_resample": (c_int, [POINTER(BurstPlan), c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p,
-                             c_void_p]),
+                             c_void_p, c_void_p]),
     "s1b_box_coherence": (c_int, [c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p, c_void_p, c_void_p]),
     "s1b_goldstein_scratch_bytes": (c_size_t, [c_int32, c_int32, c_int32]),
     "s1b_goldstein": (c_int, [c_void_p, c_void_p, c_int32, c_int32, c_int32, c_float, c_void_p, c_size_t,

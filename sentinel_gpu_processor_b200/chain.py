@@ -157,8 +157,8 @@ def process_pair_host(chain: PairChain, ref_host: torch.Tensor, sec_host: torch.
 
 
 class FrameChain:
-    """All burst pairs of a frame (configs[2]: subswaths x bursts of uneven
-    size) processed pair by pair with shared device buffers sized for the
+    """All burst pairs of a frame (subswaths x bursts of uneven size)
+    processed pair by pair with shared device buffers sized for the
     largest burst and DEM window."""
 
     def __init__(self, refs, secs, rsc, rowlook, collook, alpha, n_win=32, device="cuda", fill_seed=0):
@@ -234,7 +234,7 @@ class FrameChain:
 
 
 class RadarChain:
-    """Radar-grid chain for one burst pair (configs[0]/[1] processing):
+    """Radar-grid chain for one burst pair:
     secondary offsets from the reference grid's float64 lat/lon/height,
     TOPS-aware 8-tap sinc resampling of the secondary onto the reference grid,
     crossmul + multilook + amplitude looks, 5 x 5 full-resolution coherence,
@@ -256,7 +256,8 @@ class RadarChain:
         self.rg = torch.empty((L, S), dtype=torch.float32, device=self.dev)
         self.sec_rs = torch.empty((L, S), dtype=torch.complex64, device=self.dev)
         self.coh_full = torch.empty((L, S), dtype=torch.float32, device=self.dev)
-        self.status = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        # staging status words: [0] resample, [1] box coherence (1 = a tile's copy did not complete)
+        self.status = torch.zeros(2, dtype=torch.int32, device=self.dev)
         self.box = (0, 0, (S // self.collook) * self.collook, (L // self.rowlook) * self.rowlook)
         nml = (L // self.rowlook, S // self.collook)
         need = kernels.goldstein_scratch_bytes(nml[0], nml[1], self.n_win) if min(nml) >= self.n_win else 0
@@ -271,10 +272,11 @@ class RadarChain:
         ev = _start_event(self.geo_events)
         kernels.geo2rdr_offsets(self.sec_plan, lat, lon, hgt, self.az, self.rg)
         _end_event(self.geo_events, ev)
-        kernels.resample(self.sec_plan, sec_slc, self.az, self.rg, self.interp, out=self.sec_rs)
+        kernels.resample(self.sec_plan, sec_slc, self.az, self.rg, self.interp, out=self.sec_rs,
+                         status=self.status[0:1])
         outs = kernels.crossmul_looks(ref_slc, (0, 0), self.sec_rs, (0, 0), self.box, self.rowlook, self.collook,
                                       fill_seed=self.fill_seed)
-        kernels.box_coherence(ref_slc, self.sec_rs, self.win, out=self.coh_full, status=self.status)
+        kernels.box_coherence(ref_slc, self.sec_rs, self.win, out=self.coh_full, status=self.status[1:2])
         if self.filt.shape[0] >= self.n_win and self.filt.shape[1] >= self.n_win:
             kernels.goldstein(outs["ifg"], self.alpha, self.n_win, out=self.filt, scratch=self.scratch)
         outs["filt"] = self.filt
@@ -299,6 +301,10 @@ class RadarChain:
     def replay(self):
         self.graph.replay()
         return self.outs
+
+    def staging_ok(self) -> bool:
+        """True when no tile of the last step lost a shared-memory copy (synchronises)."""
+        return not bool(self.status.any().item())
 
     @staticmethod
     def launches_per_step():

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <climits>
 #include <mutex>
 
@@ -25,9 +26,77 @@ constexpr double kRaD = 6378137.0;
 constexpr double kRe2D = 0.00669437999015;
 
 // -------------------------------------------------------------- offsets
-// Same column walk as the geocoding kernel: thread = reference column, the
-// pixel above seeds the zero-Doppler Newton.
+// Same column walk as the geocoding kernel: thread = reference column, 16
+// rows per thread.  The first row's zero-Doppler time is solved on the
+// window polynomial from the burst centre; there the orbit is expanded to
+// third order (position, velocity, acceleration, jerk), and the other rows
+// solve on that cubic.  Over the segment (|t - t0| <= 16 lines ~ 0.035 s)
+// the dropped fourth-order term is snap |dt|^4 / 24 < 1e-12 m for an orbit
+// (snap ~ omega^4 r ~ 1e-5 m/s^4), far below the 1e-4 sample tolerance.
 constexpr int O_TX = 128, O_RY = 16;
+
+struct OrbitCubic {
+  double t0, x[3], v[3], a[3], j[3];
+};
+
+// Position and the first three derivatives of the window polynomial at t.
+__device__ __forceinline__ void orbit_cubic(const s1b_orbit_poly_t &P, double t, OrbitCubic &o) {
+  const int w = s1b_orbit_window(P, t) - 1;
+  const double tau = t - P.tc[w];
+  o.t0 = t;
+#pragma unroll
+  for (int comp = 0; comp < 3; ++comp) {
+    const double *c = P.c[w][comp];
+    double f = c[7], d = 0.0, dd = 0.0, ddd = 0.0;
+#pragma unroll
+    for (int k = 6; k >= 0; --k) {
+      ddd = fma(ddd, tau, dd);
+      dd = fma(dd, tau, d);
+      d = fma(d, tau, f);
+      f = fma(f, tau, c[k]);
+    }
+    o.x[comp] = f;
+    o.v[comp] = d;
+    o.a[comp] = 2.0 * dd;
+    o.j[comp] = 6.0 * ddd;
+  }
+}
+
+// Zero-Doppler Newton (same iteration and stopping rule as zero_doppler)
+// with the orbit state taken from the cubic expansion.
+__device__ __forceinline__ void zero_doppler_cubic(const OrbitCubic &o, const double p[3], double &t, double dr[3]) {
+  for (int it = 0; it < 51; ++it) {
+    const double h = t - o.t0;
+    double fn = 0.0, fp = 0.0, v[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const double a = fma(o.j[i], h, o.a[i]);
+      v[i] = fma(fma(0.5 * o.j[i], h, o.a[i]), h, o.v[i]);
+      const double x = fma(fma(fma(o.j[i] * (1.0 / 6.0), h, 0.5 * o.a[i]), h, o.v[i]), h, o.x[i]);
+      dr[i] = p[i] - x;
+      fn = fma(dr[i], v[i], fn);
+      fp = fma(dr[i], a, fp);
+      fp = fma(-v[i], v[i], fp);
+    }
+    const double step = fn / fp;
+    t -= step;
+    if (fabs(step) < 5.0e-9) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i) dr[i] = fma(step, v[i], dr[i]);
+      return;
+    }
+  }
+}
+
+__device__ __forceinline__ void llh_ecef(double lat_deg, double lon_deg, double h, double p[3]) {
+  double sl, cl, so, co;
+  sincospi(lat_deg * (1.0 / 180.0), &sl, &cl);
+  sincospi(lon_deg * (1.0 / 180.0), &so, &co);
+  const double re = kRaD * rsqrt(1. - kRe2D * sl * sl);  // orbit.cu:27-30
+  p[0] = (re + h) * cl * co;
+  p[1] = (re + h) * cl * so;
+  p[2] = (re * (1 - kRe2D) + h) * sl;
+}
 
 __global__ __launch_bounds__(O_TX) void offsets_kernel(const __grid_constant__ s1b_burst_plan_t P,
                                                        const double *__restrict__ lat,
@@ -39,31 +108,74 @@ __global__ __launch_bounds__(O_TX) void offsets_kernel(const __grid_constant__ s
   const int row0 = blockIdx.y * O_RY;
   if (col >= S) return;
   const double inv_dmrg = 1.0 / P.dmrg, prf = 1.0 / P.dtaz;
-  double t = P.tmid;
-  OrbitState st;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    st.x[i] = P.xmid[i];
-    st.v[i] = P.vmid[i];
-    st.a[i] = P.amid[i];
-  }
   const int rmax = min(O_RY, L - row0);
-  for (int r = 0; r < rmax; ++r) {
-    const int row = row0 + r;
-    const size_t i = (size_t)row * S + col;
-    double sl, cl, so, co;
-    sincospi(__ldcs(lat + i) * (1.0 / 180.0), &sl, &cl);
-    sincospi(__ldcs(lon + i) * (1.0 / 180.0), &so, &co);
-    const double h = __ldcs(hgt + i);
-    const double re = kRaD / sqrt(1. - kRe2D * sl * sl);  // orbit.cu:27-30
-    double p[3] = {(re + h) * cl * co, (re + h) * cl * so, (re * (1 - kRe2D) + h) * sl};
-    double dr[3];
+  size_t i = (size_t)row0 * S + col;
+  double la = __ldcs(lat + i), lo = __ldcs(lon + i), h = __ldcs(hgt + i);
+  double p[3], dr[3];
+  // first row: from the burst centre on the window polynomial
+  double t = P.tmid;
+  {
+    OrbitState st;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      st.x[k] = P.xmid[k];
+      st.v[k] = P.vmid[k];
+      st.a[k] = P.amid[k];
+    }
+    llh_ecef(la, lo, h, p);
     zero_doppler(P.orbit, p, t, st, dr);
+  }
+  OrbitCubic o;
+  orbit_cubic(P.orbit, t, o);
+  double tprev = t - P.dtaz;
+  // the next row's inputs are loaded one row ahead
+  if (rmax > 1) {
+    la = __ldcs(lat + i + S);
+    lo = __ldcs(lon + i + S);
+    h = __ldcs(hgt + i + S);
+  }
+  for (int r = 0;;) {
     const double rng = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
     // residuals relative to the pixel index keep float32 at ~1e-5 px
-    __stcs(az_off + i, (float)((t - P.tstart) * prf - row));
+    __stcs(az_off + i, (float)((t - P.tstart) * prf - (row0 + r)));
     __stcs(rg_off + i, (float)((rng - P.rngstart) * inv_dmrg - col));
+    if (++r >= rmax) break;
+    i += S;
+    llh_ecef(la, lo, h, p);
+    if (r + 1 < rmax) {
+      la = __ldcs(lat + i + S);
+      lo = __ldcs(lon + i + S);
+      h = __ldcs(hgt + i + S);
+    }
+    // seed: linear extrapolation down the column
+    const double tn = 2.0 * t - tprev;
+    tprev = t;
+    t = tn;
+    zero_doppler_cubic(o, p, t, dr);
   }
+}
+
+// ------------------------------------------------ TMA / mbarrier helpers
+// Bounded wait: try_wait suspends for a hardware time slice per call; after
+// kSpinLimit calls the caller treats the copy as lost.
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (uint32_t i = 0; i < kSpinLimit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
 }
 
 // ------------------------------------------------------------- resample
@@ -128,8 +240,10 @@ __device__ __forceinline__ void sinc8_weights(float f, float w[8]) {
   w[7] = fmaf(t, b1.w - a1.w, a1.w);
 }
 
-// TOPS coefficients at a continuous range sample: -pi kt and etaref
-// (geo2rdr.cu:533-541 with i the fractional sample).
+// TOPS coefficients at a continuous range sample, the phase in half-cycles
+// (units of pi rad): -kt, so that the deramp phase is pi (-kt) (eta -
+// etaref)^2, and etaref (geo2rdr.cu:533-541 with the sample index
+// fractional).  One division serves kt = ka ks / (ka - ks) and fnc / ka.
 __device__ __forceinline__ void tops_range(const s1b_burst_plan_t &P, double rs, double &mkt, double &etaref) {
   const double tr = P.slant_range_time + rs / P.range_sampling_rate;
   double dt = tr - P.fm[0];
@@ -138,7 +252,7 @@ __device__ __forceinline__ void tops_range(const s1b_burst_plan_t &P, double rs,
   const double fnc = P.dc[1] + dt * (P.dc[2] + P.dc[3] * dt);
   const double kmk = ka - P.ks;
   const double inv = 1.0 / (ka * kmk);
-  mkt = -kPiD * (ka * P.ks * (ka * inv));
+  mkt = -(ka * P.ks * (ka * inv));
   etaref = -fnc * (kmk * inv) - P.etac0;
 }
 
@@ -147,11 +261,44 @@ __device__ __forceinline__ float2 deramped_tap(const s1b_burst_plan_t &P, const 
   double mkt, etaref;
   tops_range(P, (double)c, mkt, etaref);
   const double d = (-P.lines * P.ati / 2. + r * P.ati) - etaref;
-  return cmul(v, phasor(mkt * d * d));
+  return cmul(v, phasor_pi(mkt * d * d));
 }
 
 __device__ __forceinline__ float2 fma2(float w, float2 v, float2 acc) {
   return __ffma2_rn(make_float2(w, w), v, acc);
+}
+
+// Secondary sample coordinate of one output pixel: the integer sample (na,
+// nr) at or below it, the fractions in [0, 1), and whether the kernel
+// support [n - lo, n + hi] lies inside the secondary burst.
+struct Coord {
+  int na, nr;
+  float fa, fr;
+  bool ok;
+};
+
+__device__ __forceinline__ Coord coord_of(const s1b_burst_plan_t &P, const float *az_off, const float *rg_off,
+                                          int row, int col, int S, int lo, int hi) {
+  Coord k;
+  const size_t i = (size_t)row * S + col;
+  const float a = __ldg(az_off + i), r = __ldg(rg_off + i);
+  // offsets of 2^20 samples or more (and NaN) leave any burst
+  k.ok = fabsf(a) < 0x1p20f && fabsf(r) < 0x1p20f;
+  const float fla = k.ok ? floorf(a) : 0.f, flr = k.ok ? floorf(r) : 0.f;
+  k.na = row + (int)fla;
+  k.nr = col + (int)flr;
+  // a - floor(a) is exact for a >= 0; for a small negative a it can round
+  // to 1.0f, which would put a sinc tap at distance 0 from the wrong sample
+  k.fa = fminf(a - fla, 0x1.fffffep-1f);
+  k.fr = fminf(r - flr, 0x1.fffffep-1f);
+  k.ok = k.ok && k.na - lo >= 0 && k.na + hi < P.lines && k.nr - lo >= 0 && k.nr + hi < P.samples;
+  return k;
+}
+
+// Restore the secondary's TOPS phase at the fractional position (az lines).
+__device__ __forceinline__ float2 reramp(const s1b_burst_plan_t &P, float2 v, double mkt, double eref, double az) {
+  const double d = fma(az, P.ati, -P.lines * P.ati / 2.) - eref;
+  return cmul(v, phasor_pi(-(mkt * d * d)));
 }
 
 __global__ __launch_bounds__(R_TX *R_TY, 2) void resample_kernel(const __grid_constant__ s1b_burst_plan_t P,
@@ -172,32 +319,21 @@ __global__ __launch_bounds__(R_TX *R_TY, 2) void resample_kernel(const __grid_co
     s_red[2] = INT_MAX;
     s_red[3] = INT_MIN;
   }
-  double az[R_RPT], rg[R_RPT];
-  int na[R_RPT], nr[R_RPT];
-  bool in[R_RPT], ok[R_RPT];
+  Coord k[R_RPT];
   int mna = INT_MAX, xna = INT_MIN, mnr = INT_MAX, xnr = INT_MIN;
 #pragma unroll
   for (int q = 0; q < R_RPT; ++q) {
     const int row = rowb + q;
-    in[q] = row < L && col < S;
-    ok[q] = false;
-    na[q] = 0;
-    nr[q] = 0;
-    if (in[q]) {
-      const size_t i = (size_t)row * S + col;
-      az[q] = row + (double)__ldg(az_off + i);
-      rg[q] = col + (double)__ldg(rg_off + i);
-      // the kernel support must lie inside the secondary burst
-      const double fa = floor(az[q]), fr = floor(rg[q]);
-      ok[q] = fa - lo >= 0.0 && fa + hi < (double)P.lines && fr - lo >= 0.0 && fr + hi < (double)P.samples;
-      if (ok[q]) {
-        na[q] = (int)fa;
-        nr[q] = (int)fr;
-        mna = min(mna, na[q]);
-        xna = max(xna, na[q]);
-        mnr = min(mnr, nr[q]);
-        xnr = max(xnr, nr[q]);
-      }
+    if (row < L && col < S) {
+      k[q] = coord_of(P, az_off, rg_off, row, col, S, lo, hi);
+    } else {
+      k[q] = Coord{0, 0, 0.f, 0.f, false};
+    }
+    if (k[q].ok) {
+      mna = min(mna, k[q].na);
+      xna = max(xna, k[q].na);
+      mnr = min(mnr, k[q].nr);
+      xnr = max(xnr, k[q].nr);
     }
   }
   __syncthreads();
@@ -212,7 +348,6 @@ __global__ __launch_bounds__(R_TX *R_TY, 2) void resample_kernel(const __grid_co
   const int nwr = s_red[1] + hi - wa0 + 1, nwc = s_red[3] + hi - wr0 + 1;
   const bool any = s_red[0] <= s_red[1];
   const bool staged = any && nwr <= R_WROWS && nwc <= R_WCOLS;  // block-uniform
-  const double eta0 = -P.lines * P.ati / 2.;
   if (staged) {
     // Deramp the window while staging it (the phase of geo2rdr.cu:151-152 at
     // every sample).  Threads own window columns and walk down row segments:
@@ -229,10 +364,10 @@ __global__ __launch_bounds__(R_TX *R_TY, 2) void resample_kernel(const __grid_co
       const int r0 = g * seg, r1 = min(nwr, r0 + seg);
       if (r0 < r1) {
         const double mkt = s_mkt[c], eref = s_eref[c];
-        const double u = (eta0 + (wa0 + r0) * P.ati) - eref;
-        float2 ph = phasor(mkt * u * u);
-        float2 step = phasor(mkt * P.ati * (2.0 * u + P.ati));
-        const float2 dstep = phasor(2.0 * mkt * P.ati * P.ati);
+        const double u = fma((double)(wa0 + r0), P.ati, -P.lines * P.ati / 2.) - eref;
+        float2 ph = phasor_pi(mkt * u * u);
+        float2 step = phasor_pi(mkt * P.ati * (2.0 * u + P.ati));
+        const float2 dstep = phasor_pi(2.0 * mkt * P.ati * P.ati);
         const float2 *src = sec + (size_t)(wa0 + r0) * P.samples + (wr0 + c);
 #pragma unroll 4
         for (int r = r0; r < r1; ++r) {
@@ -246,103 +381,461 @@ __global__ __launch_bounds__(R_TX *R_TY, 2) void resample_kernel(const __grid_co
     }
     __syncthreads();
   }
-  // fractions in [0, 1): a double fraction just below 1 can round to 1.0f,
-  // which would put a sinc tap at distance 0 from the wrong sample
-  float fa[R_RPT], fr[R_RPT];
-#pragma unroll
-  for (int q = 0; q < R_RPT; ++q) {
-    fa[q] = fminf((float)(az[q] - na[q]), 0x1.fffffep-1f);
-    fr[q] = fminf((float)(rg[q] - nr[q]), 0x1.fffffep-1f);
-  }
-  float2 acc[R_RPT];
-#pragma unroll
-  for (int q = 0; q < R_RPT; ++q) acc[q] = make_float2(0.f, 0.f);
-  const bool block4 = staged && sinc && ok[0] && ok[1] && ok[2] && ok[3] && na[1] == na[0] + 1 &&
-                      na[2] == na[0] + 2 && na[3] == na[0] + 3 && nr[1] == nr[0] && nr[2] == nr[0] &&
-                      nr[3] == nr[0];
+  const bool block4 = staged && sinc && k[0].ok && k[1].ok && k[2].ok && k[3].ok && k[1].na == k[0].na + 1 &&
+                      k[2].na == k[0].na + 2 && k[3].na == k[0].na + 3 && k[1].nr == k[0].nr &&
+                      k[2].nr == k[0].nr && k[3].nr == k[0].nr;
   if (block4) {
-    // four outputs on consecutive lines: 11 tap rows shared by all four
+    // four outputs on consecutive lines of one range sample: each of the 11
+    // tap rows is read once for all four
+    float2 acc[R_RPT];
     float wr[R_RPT][8], wa[R_RPT][8];
 #pragma unroll
     for (int q = 0; q < R_RPT; ++q) {
-      sinc8_weights(fr[q], wr[q]);
-      sinc8_weights(fa[q], wa[q]);
+      acc[q] = make_float2(0.f, 0.f);
+      sinc8_weights(k[q].fr, wr[q]);
+      sinc8_weights(k[q].fa, wa[q]);
     }
-    const float2 *base = &win[na[0] - 3 - wa0][nr[0] - 3 - wr0];
+    const float2 *base = &win[k[0].na - 3 - wa0][k[0].nr - 3 - wr0];
 #pragma unroll
     for (int rr = 0; rr < 8 + R_RPT - 1; ++rr) {
       float2 tap[8];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) tap[k] = base[rr * R_WCOLS + k];
+      for (int j = 0; j < 8; ++j) tap[j] = base[rr * R_WCOLS + j];
 #pragma unroll
       for (int q = 0; q < R_RPT; ++q) {
         const int ka = rr - q;  // tap row of output q
         if (ka < 0 || ka > 7) continue;
         float2 rs = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int k = 0; k < 8; ++k) rs = fma2(wr[q][k], tap[k], rs);
+        for (int j = 0; j < 8; ++j) rs = fma2(wr[q][j], tap[j], rs);
         acc[q] = fma2(wa[q][ka], rs, acc[q]);
       }
     }
-  } else {
-#pragma unroll 1
+    // -kt and etaref at the fractional sample from the staged per-column
+    // values (smooth in range: linear interpolation is exact to ~1e-7 rad)
+    const int c = k[0].nr - wr0;
+    const double m0 = s_mkt[c], dm = s_mkt[c + 1] - m0, e0 = s_eref[c], de = s_eref[c + 1] - e0;
+#pragma unroll
     for (int q = 0; q < R_RPT; ++q) {
-      if (!ok[q]) continue;
+      const double t = k[q].fr;
+      const float2 v = reramp(P, acc[q], fma(t, dm, m0), fma(t, de, e0), (double)k[q].na + (double)k[q].fa);
+      __stcs(out + (size_t)(rowb + q) * S + col, v);
+    }
+    return;
+  }
+  // Any other thread: one output at a time, its coordinate re-read (L1 hit)
+  // so that no per-output array is indexed by a loop variable.
+#pragma unroll 1
+  for (int q = 0; q < R_RPT; ++q) {
+    const int row = rowb + q;
+    if (row >= L || col >= S) break;
+    const Coord kq = coord_of(P, az_off, rg_off, row, col, S, lo, hi);
+    float2 v = make_float2(0.f, 0.f);
+    if (kq.ok) {
+      float2 acc = make_float2(0.f, 0.f);
       if (sinc) {
         float wr[8], wa[8];
-        sinc8_weights(fr[q], wr);
-        sinc8_weights(fa[q], wa);
+        sinc8_weights(kq.fr, wr);
+        sinc8_weights(kq.fa, wa);
         if (staged) {
-          const float2 *base = &win[na[q] - 3 - wa0][nr[q] - 3 - wr0];
+          const float2 *base = &win[kq.na - 3 - wa0][kq.nr - 3 - wr0];
 #pragma unroll
           for (int ka = 0; ka < 8; ++ka) {
             float2 rs = make_float2(0.f, 0.f);
 #pragma unroll
             for (int kr = 0; kr < 8; ++kr) rs = fma2(wr[kr], base[ka * R_WCOLS + kr], rs);
-            acc[q] = fma2(wa[ka], rs, acc[q]);
+            acc = fma2(wa[ka], rs, acc);
           }
         } else {
           for (int ka = 0; ka < 8; ++ka) {
             float2 rs = make_float2(0.f, 0.f);
-            for (int kr = 0; kr < 8; ++kr) rs = fma2(wr[kr], deramped_tap(P, sec, na[q] + ka - 3, nr[q] + kr - 3), rs);
-            acc[q] = fma2(wa[ka], rs, acc[q]);
+            for (int kr = 0; kr < 8; ++kr) rs = fma2(wr[kr], deramped_tap(P, sec, kq.na + ka - 3, kq.nr + kr - 3), rs);
+            acc = fma2(wa[ka], rs, acc);
           }
         }
       } else {
         float2 b[4];
         if (staged) {
 #pragma unroll
-          for (int k = 0; k < 4; ++k) b[k] = win[na[q] + (k >> 1) - wa0][nr[q] + (k & 1) - wr0];
+          for (int j = 0; j < 4; ++j) b[j] = win[kq.na + (j >> 1) - wa0][kq.nr + (j & 1) - wr0];
         } else {
-          for (int k = 0; k < 4; ++k) b[k] = deramped_tap(P, sec, na[q] + (k >> 1), nr[q] + (k & 1));
-        }
-        const float2 c1 = make_float2(fmaf(fr[q], b[1].x - b[0].x, b[0].x), fmaf(fr[q], b[1].y - b[0].y, b[0].y));
-        const float2 c2 = make_float2(fmaf(fr[q], b[3].x - b[2].x, b[2].x), fmaf(fr[q], b[3].y - b[2].y, b[2].y));
-        acc[q] = make_float2(fmaf(fa[q], c2.x - c1.x, c1.x), fmaf(fa[q], c2.y - c1.y, c1.y));
-      }
-    }
-  }
-  // reramp: restore the secondary's TOPS phase at the fractional position;
-  // -pi kt and etaref at the fractional sample from the staged per-column
-  // values (smooth in range: linear interpolation is exact to ~1e-7 rad)
 #pragma unroll
-  for (int q = 0; q < R_RPT; ++q) {
-    if (!in[q]) continue;
-    float2 v = make_float2(0.f, 0.f);
-    if (ok[q]) {
+          for (int j = 0; j < 4; ++j) b[j] = deramped_tap(P, sec, kq.na + (j >> 1), kq.nr + (j & 1));
+        }
+        const float fr = kq.fr, fa = kq.fa;
+        const float2 c1 = make_float2(fmaf(fr, b[1].x - b[0].x, b[0].x), fmaf(fr, b[1].y - b[0].y, b[0].y));
+        const float2 c2 = make_float2(fmaf(fr, b[3].x - b[2].x, b[2].x), fmaf(fr, b[3].y - b[2].y, b[2].y));
+        acc = make_float2(fmaf(fa, c2.x - c1.x, c1.x), fmaf(fa, c2.y - c1.y, c1.y));
+      }
       double mkt, eref;
       if (staged) {
-        const int c = nr[q] - wr0;
-        const double t = rg[q] - nr[q];
-        mkt = s_mkt[c] + t * (s_mkt[c + 1] - s_mkt[c]);
-        eref = s_eref[c] + t * (s_eref[c + 1] - s_eref[c]);
+        const int c = kq.nr - wr0;
+        const double t = kq.fr;
+        mkt = fma(t, s_mkt[c + 1] - s_mkt[c], s_mkt[c]);
+        eref = fma(t, s_eref[c + 1] - s_eref[c], s_eref[c]);
       } else {
-        tops_range(P, rg[q], mkt, eref);
+        tops_range(P, (double)kq.nr + (double)kq.fr, mkt, eref);
       }
-      const double d = (eta0 + az[q] * P.ati) - eref;
-      v = cmul(acc[q], phasor(-(mkt * d * d)));
+      v = reramp(P, acc, mkt, eref, (double)kq.na + (double)kq.fa);
     }
-    __stcs(out + (size_t)(rowb + q) * S + col, v);
+    __stcs(out + (size_t)row * S + col, v);
+  }
+}
+
+// ------------------------------------------------- resample, TMA pipeline
+// Persistent form of the resampler (one CTA per half SM, tiles of 64
+// columns x 16 rows taken round-robin) for rasters a tensor map can describe.
+// Everything a tile reads comes through shared memory by TMA
+// (cp.async.bulk.tensor, completion on an mbarrier):
+//   offsets  - the tile's az/rg offset blocks, issued two tiles ahead into
+//              one of three stages;
+//   window   - the raw secondary window of the tile, box RT_WC x RT_WR at an
+//              even column (16-byte rule), issued one tile ahead into one of
+//              two stages as soon as the tile's coordinate range is known;
+//   sinc LUT - copied once per CTA.
+// Per tile the CTA (1) reduces the next tile's coordinate range and issues
+// its window, (2) deramps the current window in place, (3) interpolates,
+// reramps and stores.  Waits are bounded; a wait that runs out sets *status,
+// lets the copies in flight land (again bounded) and ends the block.
+constexpr int RT_THREADS = R_TX * R_TY;           // 256: 64 columns x 4 row groups of 4 rows
+constexpr int RT_WR = 32, RT_WC = 96;             // window box rows x columns
+constexpr int RT_OFF_BYTES = 2 * R_TH * R_TX * 4; // az + rg blocks of one tile
+constexpr int RT_WIN_BYTES = RT_WR * RT_WC * 8;
+
+struct RtSmem {
+  float2 win[2][RT_WR][RT_WC];
+  float offs[3][2][R_TH][R_TX];
+  float lut[(SINC_BINS + 1) * 8];
+  double mkt[2][RT_WC], eref[2][RT_WC];  // per window stage
+  int red[RT_THREADS / 32][4];
+  uint64_t bar_off[3], bar_win[2];
+};
+
+__device__ __forceinline__ void sinc8_weights_lut(const float *lut, float f, float w[8]) {
+  const float pos = f * SINC_BINS;
+  const int b = min((int)pos, SINC_BINS - 1);
+  const float t = pos - (float)b;
+  const float4 *T = reinterpret_cast<const float4 *>(lut) + 2 * b;
+  const float4 a0 = T[0], a1 = T[1], b0 = T[2], b1 = T[3];
+  const float2 tt = make_float2(t, t), m1 = make_float2(-1.f, -1.f);
+  const float2 w01 = __ffma2_rn(tt, __ffma2_rn(m1, make_float2(a0.x, a0.y), make_float2(b0.x, b0.y)), make_float2(a0.x, a0.y));
+  const float2 w23 = __ffma2_rn(tt, __ffma2_rn(m1, make_float2(a0.z, a0.w), make_float2(b0.z, b0.w)), make_float2(a0.z, a0.w));
+  const float2 w45 = __ffma2_rn(tt, __ffma2_rn(m1, make_float2(a1.x, a1.y), make_float2(b1.x, b1.y)), make_float2(a1.x, a1.y));
+  const float2 w67 = __ffma2_rn(tt, __ffma2_rn(m1, make_float2(a1.z, a1.w), make_float2(b1.z, b1.w)), make_float2(a1.z, a1.w));
+  w[0] = w01.x; w[1] = w01.y; w[2] = w23.x; w[3] = w23.y;
+  w[4] = w45.x; w[5] = w45.y; w[6] = w67.x; w[7] = w67.y;
+}
+
+// Coordinate of one output from its offsets (as coord_of, values given).
+__device__ __forceinline__ Coord coord_from(const s1b_burst_plan_t &P, float a, float r, int row, int col, bool in,
+                                            int lo, int hi) {
+  Coord k;
+  k.ok = in && fabsf(a) < 0x1p20f && fabsf(r) < 0x1p20f;
+  const float fla = k.ok ? floorf(a) : 0.f, flr = k.ok ? floorf(r) : 0.f;
+  k.na = row + (int)fla;
+  k.nr = col + (int)flr;
+  k.fa = fminf(a - fla, 0x1.fffffep-1f);
+  k.fr = fminf(r - flr, 0x1.fffffep-1f);
+  k.ok = k.ok && k.na - lo >= 0 && k.na + hi < P.lines && k.nr - lo >= 0 && k.nr + hi < P.samples;
+  return k;
+}
+
+// Secondary window of a tile: origin (row wa0, even column wr0) and extent.
+struct Window {
+  int wa0, wr0, nwr, nwc;
+  bool staged;
+};
+
+__device__ __forceinline__ void mbar_init(uint64_t *b) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(b)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect(uint64_t *b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(b)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap &m, int x, int y, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(&m)), "r"(x), "r"(y), "r"(smem_addr(bar))
+      : "memory");
+}
+
+__global__ __launch_bounds__(RT_THREADS, 2) void resample_tma_kernel(
+    const __grid_constant__ s1b_burst_plan_t P, const __grid_constant__ CUtensorMap tsec,
+    const __grid_constant__ CUtensorMap taz, const __grid_constant__ CUtensorMap trg, const float2 *__restrict__ sec,
+    int L, int S, int sinc, int ntx, int ntiles, float2 *__restrict__ out, int *__restrict__ status) {
+  extern __shared__ __align__(1024) unsigned char rt_raw[];
+  RtSmem &sm = *reinterpret_cast<RtSmem *>(rt_raw);
+  const int tid = threadIdx.x, tx = tid % R_TX, ty = tid / R_TX, lane = tid % 32, warp = tid / 32;
+  const int lo = sinc ? 3 : 0, hi = sinc ? 4 : 1;
+  const int n = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  if (n == 0) return;
+  {
+    const float4 *g = reinterpret_cast<const float4 *>(g_sinc_table);
+    float4 *s = reinterpret_cast<float4 *>(sm.lut);
+    for (int i = tid; i < (SINC_BINS + 1) * 2; i += RT_THREADS) s[i] = g[i];
+  }
+  if (tid == 0) {
+    for (int i = 0; i < 3; ++i) mbar_init(&sm.bar_off[i]);
+    for (int i = 0; i < 2; ++i) mbar_init(&sm.bar_win[i]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  // copies in flight, tracked by thread 0 (bits 0-2 offsets, 3-4 windows),
+  // with the phase parity each offsets stage is waiting on
+  uint32_t pending = 0, opar = 0, wphase = 0;
+  auto tile_origin = [&](int j, int &row0, int &col0) {
+    const int t = blockIdx.x + j * gridDim.x;
+    row0 = (t / ntx) * R_TH;
+    col0 = (t % ntx) * R_TX;
+  };
+  auto issue_offsets = [&](int j) {  // thread 0 only
+    int row0, col0;
+    tile_origin(j, row0, col0);
+    const int s = j % 3;
+    mbar_expect(&sm.bar_off[s], RT_OFF_BYTES);
+    tma_load_2d(&sm.offs[s][0][0][0], taz, col0, row0, &sm.bar_off[s]);
+    tma_load_2d(&sm.offs[s][1][0][0], trg, col0, row0, &sm.bar_off[s]);
+    pending |= 1u << s;
+    opar = (opar & ~(1u << s)) | ((uint32_t)((j / 3) & 1) << s);
+  };
+  // Drain what thread 0 issued (bounded) and flag the failure.
+  auto abort_block = [&]() {
+    if (tid == 0) {
+      atomicExch(status, 1);
+      for (int s = 0; s < 3; ++s)
+        if (pending & (1u << s)) mbar_wait(smem_addr(&sm.bar_off[s]), (opar >> s) & 1);
+      for (int s = 0; s < 2; ++s)
+        if (pending & (8u << s)) mbar_wait(smem_addr(&sm.bar_win[s]), (wphase >> s) & 1);
+    }
+  };
+  // Coordinates of this thread's outputs of local tile j from its offsets stage.
+  auto coords = [&](int j, Coord k[R_RPT]) {
+    int row0, col0;
+    tile_origin(j, row0, col0);
+    const int s = j % 3, col = col0 + tx;
+#pragma unroll
+    for (int q = 0; q < R_RPT; ++q) {
+      const int r = ty * R_RPT + q, row = row0 + r;
+      k[q] = coord_from(P, sm.offs[s][0][r][tx], sm.offs[s][1][r][tx], row, col, row < L && col < S, lo, hi);
+    }
+  };
+  // Step b for local tile j: wait its offsets, reduce its coordinate range,
+  // issue its window and the offsets of tile j + 1.  Returns false on a
+  // failed wait (uniform over the block).
+  auto prepare = [&](int j, Window &w) -> bool {
+    const bool ok_wait = mbar_wait(smem_addr(&sm.bar_off[j % 3]), (j / 3) & 1);
+    if (tid == 0 && ok_wait) pending &= ~(1u << (j % 3));
+    int mna = INT_MAX, xna = INT_MIN, mnr = INT_MAX, xnr = INT_MIN;
+    if (ok_wait) {
+      Coord k[R_RPT];
+      coords(j, k);
+#pragma unroll
+      for (int q = 0; q < R_RPT; ++q)
+        if (k[q].ok) {
+          mna = min(mna, k[q].na);
+          xna = max(xna, k[q].na);
+          mnr = min(mnr, k[q].nr);
+          xnr = max(xnr, k[q].nr);
+        }
+    }
+    mna = __reduce_min_sync(0xffffffffu, mna);
+    xna = __reduce_max_sync(0xffffffffu, xna);
+    mnr = __reduce_min_sync(0xffffffffu, mnr);
+    xnr = __reduce_max_sync(0xffffffffu, xnr);
+    if (lane == 0) {
+      sm.red[warp][0] = mna;
+      sm.red[warp][1] = xna;
+      sm.red[warp][2] = mnr;
+      sm.red[warp][3] = xnr;
+    }
+    // generic-proxy writes to the stages that the copies below overwrite are
+    // ordered before them by this fence and the barrier
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (__syncthreads_or(!ok_wait)) return false;
+#pragma unroll
+    for (int i = 0; i < RT_THREADS / 32; ++i) {
+      mna = min(mna, sm.red[i][0]);
+      xna = max(xna, sm.red[i][1]);
+      mnr = min(mnr, sm.red[i][2]);
+      xnr = max(xnr, sm.red[i][3]);
+    }
+    w = Window{0, 0, 0, 0, false};
+    if (mna <= xna) {
+      w.wa0 = mna - lo;
+      w.wr0 = (mnr - lo) & ~1;
+      w.nwr = xna + hi - w.wa0 + 1;
+      w.nwc = xnr + hi - w.wr0 + 1;
+      w.staged = w.nwr <= RT_WR && w.nwc <= RT_WC;
+    }
+    if (tid == 0) {
+      if (w.staged) {
+        const int s = j & 1;
+        mbar_expect(&sm.bar_win[s], RT_WIN_BYTES);
+        tma_load_2d(&sm.win[s][0][0], tsec, w.wr0, w.wa0, &sm.bar_win[s]);
+        pending |= 8u << s;
+      }
+      if (j + 1 < n) issue_offsets(j + 1);
+    }
+    return true;
+  };
+
+  if (tid == 0) issue_offsets(0);
+  Window cur, nxt;
+  if (!prepare(0, cur)) {
+    abort_block();
+    return;
+  }
+  for (int i = 0; i < n; ++i) {
+    if (i + 1 < n && !prepare(i + 1, nxt)) {
+      abort_block();
+      return;
+    }
+    const int s = i & 1;
+    bool ok_wait = true;
+    if (cur.staged) {
+      ok_wait = mbar_wait(smem_addr(&sm.bar_win[s]), (wphase >> s) & 1);
+      if (ok_wait) {
+        wphase ^= 1u << s;
+        if (tid == 0) pending &= ~(8u << s);
+      }
+    }
+    if (cur.staged && ok_wait) {
+      // deramp the window in place: threads own columns and walk row
+      // segments with the phasor recurrence of the direct kernel
+      const int groups = max(1, RT_THREADS / cur.nwc);
+      const int seg = (cur.nwr + groups - 1) / groups;
+      const int g = tid / cur.nwc, c = tid - g * cur.nwc;
+      if (g < groups) {
+        double mkt, eref;
+        tops_range(P, (double)(cur.wr0 + c), mkt, eref);
+        if (g == 0) {
+          sm.mkt[s][c] = mkt;
+          sm.eref[s][c] = eref;
+        }
+        const int r0 = g * seg, r1 = min(cur.nwr, r0 + seg);
+        if (r0 < r1) {
+          const double u = fma((double)(cur.wa0 + r0), P.ati, -P.lines * P.ati / 2.) - eref;
+          float2 ph = phasor_pi(mkt * u * u);
+          float2 step = phasor_pi(mkt * P.ati * (2.0 * u + P.ati));
+          const float2 dstep = phasor_pi(2.0 * mkt * P.ati * P.ati);
+#pragma unroll 4
+          for (int r = r0; r < r1; ++r) {
+            sm.win[s][r][c] = cmul(sm.win[s][r][c], ph);
+            ph = cmul(ph, step);
+            step = cmul(step, dstep);
+          }
+        }
+      }
+    }
+    if (__syncthreads_or(!ok_wait)) {
+      abort_block();
+      return;
+    }
+    // interpolate, reramp and store tile i
+    int row0, col0;
+    tile_origin(i, row0, col0);
+    const int col = col0 + tx, rowb = row0 + ty * R_RPT;
+    Coord k[R_RPT];
+    coords(i, k);
+    const bool block4 = cur.staged && sinc && k[0].ok && k[1].ok && k[2].ok && k[3].ok &&
+                        k[1].na == k[0].na + 1 && k[2].na == k[0].na + 2 && k[3].na == k[0].na + 3 &&
+                        k[1].nr == k[0].nr && k[2].nr == k[0].nr && k[3].nr == k[0].nr;
+    if (block4) {
+      float2 acc[R_RPT];
+      float wr[R_RPT][8], wa[R_RPT][8];
+#pragma unroll
+      for (int q = 0; q < R_RPT; ++q) {
+        acc[q] = make_float2(0.f, 0.f);
+        sinc8_weights_lut(sm.lut, k[q].fr, wr[q]);
+        sinc8_weights_lut(sm.lut, k[q].fa, wa[q]);
+      }
+      const float2 *base = &sm.win[s][k[0].na - 3 - cur.wa0][k[0].nr - 3 - cur.wr0];
+#pragma unroll
+      for (int rr = 0; rr < 8 + R_RPT - 1; ++rr) {
+        float2 tap[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) tap[j] = base[rr * RT_WC + j];
+#pragma unroll
+        for (int q = 0; q < R_RPT; ++q) {
+          const int ka = rr - q;
+          if (ka < 0 || ka > 7) continue;
+          float2 rs = make_float2(0.f, 0.f);
+#pragma unroll
+          for (int j = 0; j < 8; ++j) rs = fma2(wr[q][j], tap[j], rs);
+          acc[q] = fma2(wa[q][ka], rs, acc[q]);
+        }
+      }
+      const int c = k[0].nr - cur.wr0;
+      const double m0 = sm.mkt[s][c], dm = sm.mkt[s][c + 1] - m0, e0 = sm.eref[s][c], de = sm.eref[s][c + 1] - e0;
+#pragma unroll
+      for (int q = 0; q < R_RPT; ++q) {
+        const double t = k[q].fr;
+        const float2 v = reramp(P, acc[q], fma(t, dm, m0), fma(t, de, e0), (double)k[q].na + (double)k[q].fa);
+        __stcs(out + (size_t)(rowb + q) * S + col, v);
+      }
+    } else {
+#pragma unroll 1
+      for (int q = 0; q < R_RPT; ++q) {
+        const int row = rowb + q;
+        if (row >= L || col >= S) break;
+        const int r = ty * R_RPT + q;
+        const Coord kq = coord_from(P, sm.offs[i % 3][0][r][tx], sm.offs[i % 3][1][r][tx], row, col, true, lo, hi);
+        float2 v = make_float2(0.f, 0.f);
+        if (kq.ok) {
+          float2 acc = make_float2(0.f, 0.f);
+          if (sinc) {
+            float wr[8], wa[8];
+            sinc8_weights_lut(sm.lut, kq.fr, wr);
+            sinc8_weights_lut(sm.lut, kq.fa, wa);
+            if (cur.staged) {
+              const float2 *base = &sm.win[s][kq.na - 3 - cur.wa0][kq.nr - 3 - cur.wr0];
+#pragma unroll
+              for (int ka = 0; ka < 8; ++ka) {
+                float2 rs = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int kr = 0; kr < 8; ++kr) rs = fma2(wr[kr], base[ka * RT_WC + kr], rs);
+                acc = fma2(wa[ka], rs, acc);
+              }
+            } else {
+              for (int ka = 0; ka < 8; ++ka) {
+                float2 rs = make_float2(0.f, 0.f);
+                for (int kr = 0; kr < 8; ++kr)
+                  rs = fma2(wr[kr], deramped_tap(P, sec, kq.na + ka - 3, kq.nr + kr - 3), rs);
+                acc = fma2(wa[ka], rs, acc);
+              }
+            }
+          } else {
+            float2 b[4];
+            if (cur.staged) {
+#pragma unroll
+              for (int j = 0; j < 4; ++j) b[j] = sm.win[s][kq.na + (j >> 1) - cur.wa0][kq.nr + (j & 1) - cur.wr0];
+            } else {
+#pragma unroll
+              for (int j = 0; j < 4; ++j) b[j] = deramped_tap(P, sec, kq.na + (j >> 1), kq.nr + (j & 1));
+            }
+            const float fr = kq.fr, fa = kq.fa;
+            const float2 c1 = make_float2(fmaf(fr, b[1].x - b[0].x, b[0].x), fmaf(fr, b[1].y - b[0].y, b[0].y));
+            const float2 c2 = make_float2(fmaf(fr, b[3].x - b[2].x, b[2].x), fmaf(fr, b[3].y - b[2].y, b[2].y));
+            acc = make_float2(fmaf(fa, c2.x - c1.x, c1.x), fmaf(fa, c2.y - c1.y, c1.y));
+          }
+          double mkt, eref;
+          if (cur.staged) {
+            const int c = kq.nr - cur.wr0;
+            const double t = kq.fr;
+            mkt = fma(t, sm.mkt[s][c + 1] - sm.mkt[s][c], sm.mkt[s][c]);
+            eref = fma(t, sm.eref[s][c + 1] - sm.eref[s][c], sm.eref[s][c]);
+          } else {
+            tops_range(P, (double)kq.nr + (double)kq.fr, mkt, eref);
+          }
+          v = reramp(P, acc, mkt, eref, (double)kq.na + (double)kq.fa);
+        }
+        __stcs(out + (size_t)row * S + col, v);
+      }
+    }
+    cur = nxt;
   }
 }
 
@@ -364,7 +857,6 @@ constexpr int C_MAXH = 4;                        // half window <= 4 (win <= 9)
 constexpr int C_IH = C_TH + 2 * C_MAXH;          // 40 staged rows
 constexpr int C_THREADS = 512, C_PARTS = C_THREADS / C_TW, C_ROWS = C_TH / C_PARTS;  // 4 parts x 8 rows
 constexpr int C_STAGE = 2 * C_IH * C_IW;         // float2 per stage (ref + sec)
-constexpr uint32_t kSpinLimit = 1u << 22;
 
 // Kahan compensated summation (W. Kahan, "Further remarks on reducing
 // truncation errors", CACM 1965).
@@ -378,24 +870,6 @@ struct Kahan {
   }
   __device__ __forceinline__ float value() const { return s; }
 };
-
-__device__ __forceinline__ uint32_t smem_addr(const void *p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (uint32_t i = 0; i < kSpinLimit; ++i) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
 
 __device__ __forceinline__ void tma_tile(float2 *dst_r, float2 *dst_s, const CUtensorMap &tr, const CUtensorMap &ts,
                                          int x0, int y0, uint32_t bar) {
@@ -565,20 +1039,49 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
-// 2-D tensor map over a complex64 raster (8-byte elements), box C_IW x C_IH,
-// zero fill outside.  False when the raster cannot be described (odd width,
-// unaligned base) or the driver lacks the entry point.
-bool make_tile_map(CUtensorMap *m, const void *base, int L, int S) {
-  if (S % 2 != 0 || (reinterpret_cast<uintptr_t>(base) % 16) != 0) return false;
+// 2-D tensor map over a row-major raster of `width` x `height` elements of
+// `esize` bytes (FLOAT32 or FLOAT64 elements; complex64 travels as one
+// 8-byte element), box bw x bh, zero fill outside.  False when the raster
+// cannot be described (row pitch not a multiple of 16 bytes, base not
+// 16-byte aligned) or the driver lacks the entry point.
+bool make_map_2d(CUtensorMap *m, const void *base, CUtensorMapDataType dtype, int esize, int width, int height,
+                 int bw, int bh) {
+  if (((size_t)width * esize) % 16 != 0 || (reinterpret_cast<uintptr_t>(base) % 16) != 0) return false;
   auto enc = tensor_map_encoder();
   if (!enc) return false;
-  cuuint64_t dims[2] = {(cuuint64_t)S, (cuuint64_t)L};
-  cuuint64_t strides[1] = {(cuuint64_t)S * sizeof(float2)};
-  cuuint32_t box[2] = {(cuuint32_t)C_IW, (cuuint32_t)C_IH};
+  cuuint64_t dims[2] = {(cuuint64_t)width, (cuuint64_t)height};
+  cuuint64_t strides[1] = {(cuuint64_t)width * esize};
+  cuuint32_t box[2] = {(cuuint32_t)bw, (cuuint32_t)bh};
   cuuint32_t estr[2] = {1, 1};
-  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void *>(base), dims, strides, box, estr,
-             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+  return enc(m, dtype, 2, const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+bool make_tile_map(CUtensorMap *m, const void *base, int L, int S) {
+  return make_map_2d(m, base, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, S, L, C_IW, C_IH);
+}
+
+// Resident CTAs of the persistent resampler per device (0: not usable).
+int resample_tma_slots() {
+  static std::mutex mu;
+  static int slots[64] = {};
+  static bool done[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!done[dev]) {
+    done[dev] = true;
+    int sms = 0, per_sm = 0;
+    if (cudaFuncSetAttribute(resample_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(RtSmem)) == cudaSuccess &&
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, resample_tma_kernel, RT_THREADS, sizeof(RtSmem)) ==
+            cudaSuccess)
+      slots[dev] = sms * per_sm;
+    cudaGetLastError();
+  }
+  return slots[dev];
 }
 
 }  // namespace
@@ -597,8 +1100,8 @@ extern "C" int s1b_geo2rdr_offsets(const s1b_burst_plan_t *plan, const double *l
 
 extern "C" int s1b_resample(const s1b_burst_plan_t *plan, const void *sec, const float *az_off,
                             const float *rg_off, int32_t lines, int32_t samples, int32_t interp, void *out,
-                            void *stream) {
-  if (!plan || !sec || !az_off || !rg_off || !out)
+                            int32_t *status, void *stream) {
+  if (!plan || !sec || !az_off || !rg_off || !out || !status)
     return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_resample: null argument");
   if (interp != S1B_INTERP_BILINEAR && interp != S1B_INTERP_SINC8)
     return s1b_fail(S1B_ERR_UNSUPPORTED, "s1b_resample: interp must be S1B_INTERP_BILINEAR or S1B_INTERP_SINC8");
@@ -606,12 +1109,29 @@ extern "C" int s1b_resample(const s1b_burst_plan_t *plan, const void *sec, const
     return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_resample: empty grid");
   int s = ensure_sinc_table();
   if (s) return s;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaMemsetAsync(status, 0, sizeof(int32_t), st);
+  if (e != cudaSuccess) return s1b_fail(S1B_ERR_CUDA, cudaGetErrorString(e));
+  const int ntx = (samples + R_TX - 1) / R_TX, nty = (lines + R_TH - 1) / R_TH;
+  const long long ntiles = (long long)ntx * nty;
+  const int sinc = interp == S1B_INTERP_SINC8 ? 1 : 0;
+  CUtensorMap msec, maz, mrg;
+  const int slots = resample_tma_slots();
+  if (slots > 0 && ntiles <= INT_MAX &&
+      make_map_2d(&msec, sec, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, plan->samples, plan->lines, RT_WC, RT_WR) &&
+      make_map_2d(&maz, az_off, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, samples, lines, R_TX, R_TH) &&
+      make_map_2d(&mrg, rg_off, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, samples, lines, R_TX, R_TH)) {
+    const int grid = (int)std::min<long long>(ntiles, slots);
+    resample_tma_kernel<<<grid, RT_THREADS, sizeof(RtSmem), st>>>(*plan, msec, maz, mrg, (const float2 *)sec, lines,
+                                                                  samples, sinc, ntx, (int)ntiles, (float2 *)out,
+                                                                  status);
+    return s1b_launch_status();
+  }
   dim3 block(R_TX, R_TY);
-  dim3 grid((samples + R_TX - 1) / R_TX, (lines + R_TH - 1) / R_TH);
+  dim3 grid(ntx, nty);
   if (grid.y > 65535) return s1b_fail(S1B_ERR_TOO_LARGE, "s1b_resample: grid too tall");
-  resample_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(*plan, (const float2 *)sec, az_off, rg_off, lines,
-                                                            samples, interp == S1B_INTERP_SINC8 ? 1 : 0,
-                                                            (float2 *)out);
+  resample_kernel<<<grid, block, 0, st>>>(*plan, (const float2 *)sec, az_off, rg_off, lines, samples, sinc,
+                                          (float2 *)out);
   return s1b_launch_status();
 }
 

@@ -45,6 +45,16 @@ __device__ __forceinline__ float2 phasor(double x) {
   return make_float2(c, s);
 }
 
+// Unit phasor exp(i pi h) of an FP64 phase h given in half-cycles (units of
+// pi rad).  h - 2 rint(h / 2) is exact in FP64 for |h| < 2^52, so the only
+// rounding is the final float conversion of a value in [-1, 1] (<= 6e-8).
+__device__ __forceinline__ float2 phasor_pi(double h) {
+  const double r = fma(-2.0, rint(0.5 * h), h);
+  float s, c;
+  sincospif((float)r, &s, &c);
+  return make_float2(c, s);
+}
+
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }

@@ -177,9 +177,13 @@ def geo2rdr_offsets(plan: _lib.BurstPlan, lat: torch.Tensor, lon: torch.Tensor, 
 
 
 def resample(plan: _lib.BurstPlan, sec: torch.Tensor, az_off: torch.Tensor, rg_off: torch.Tensor,
-             interp: str = "sinc8", out: torch.Tensor | None = None) -> torch.Tensor:
-    """Resample the secondary burst of ``plan`` onto the grid of the offsets."""
-    _need_cuda(sec, az_off, rg_off, out)
+             interp: str = "sinc8", out: torch.Tensor | None = None,
+             status: torch.Tensor | None = None) -> torch.Tensor:
+    """Resample the secondary burst of ``plan`` onto the grid of the offsets.
+
+    ``status`` (int32 device word) is set to 1 if a tile's staging did not
+    complete; one is allocated when not given."""
+    _need_cuda(sec, az_off, rg_off, out, status)
     _c64(sec, "sec")
     if sec.numel() != plan.lines * plan.samples:
         raise ValueError("sec size does not match the plan")
@@ -189,9 +193,11 @@ def resample(plan: _lib.BurstPlan, sec: torch.Tensor, az_off: torch.Tensor, rg_o
     L, S = az_off.shape
     if out is None:
         out = torch.empty((L, S), dtype=torch.complex64, device=sec.device)
+    if status is None:
+        status = torch.empty(1, dtype=torch.int32, device=sec.device)
     mode = {"sinc8": _lib.S1B_INTERP_SINC8, "bilinear": _lib.S1B_INTERP_BILINEAR}[interp]
     _lib.check(_call("resample", _lib.load().s1b_resample, ctypes.byref(plan), _lib.dptr(sec), _lib.dptr(az_off), _lib.dptr(rg_off),
-                                        L, S, mode, _lib.dptr(out), _lib.stream_ptr()), "s1b_resample")
+                                        L, S, mode, _lib.dptr(out), _lib.dptr(status), _lib.stream_ptr()), "s1b_resample")
     return out
 
 

@@ -609,7 +609,7 @@ class RadarPairScene:
 
 def make_radar_pair(config="c1", seed=20261203, device="cpu", baseline=150.0, coherence=0.7,
                     lines=None, samples=None, defo_amp=0.03, defo_sigma=5000.0):
-    """configs[0]/[1]-style pair: float64 lat/lon/height rasters of the
+    """Radar-grid burst pair: float64 lat/lon/height rasters of the
     reference grid, a secondary with a perpendicular baseline, a band-limited
     reflectivity seen by both, a Gaussian deformation (phase 4 pi d / lambda)
     and coherence ``coherence`` against white noise."""
