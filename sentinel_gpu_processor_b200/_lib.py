@@ -11,7 +11,8 @@ import os
 from ctypes import POINTER, c_char_p, c_double, c_float, c_int, c_int32, c_int64, c_size_t, c_uint64, c_void_p
 
 PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(PKG, "libs1b.so")
+# S1B_LIBRARY selects another build of the library (it must exist: there is no fallback)
+LIB_PATH = os.environ.get("S1B_LIBRARY") or os.path.join(PKG, "libs1b.so")
 
 S1B_OK = 0
 S1B_ERR_INVALID_ARGUMENT = 1

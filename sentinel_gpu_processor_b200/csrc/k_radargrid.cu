@@ -298,7 +298,7 @@ __device__ __forceinline__ Coord coord_of(const s1b_burst_plan_t &P, const float
 // Restore the secondary's TOPS phase at the fractional position (az lines).
 __device__ __forceinline__ float2 reramp(const s1b_burst_plan_t &P, float2 v, double mkt, double eref, double az) {
   const double d = fma(az, P.ati, -P.lines * P.ati / 2.) - eref;
-  return cmul(v, phasor_pi(-(mkt * d * d)));
+  return cmul(v, phasor_pi_fast(-(mkt * d * d)));
 }
 
 __global__ __launch_bounds__(R_TX *R_TY, 2) void resample_kernel(const __grid_constant__ s1b_burst_plan_t P,
@@ -705,9 +705,12 @@ __global__ __launch_bounds__(RT_THREADS, 2) void resample_tma_kernel(
     if (cur.staged && ok_wait) {
       // deramp the window in place: threads own columns and walk row
       // segments with the phasor recurrence of the direct kernel
-      const int groups = max(1, RT_THREADS / cur.nwc);
+      // tid / nwc and RT_THREADS / nwc by a float reciprocal: every quotient
+      // (i + 0.5) / nwc with i <= 256, nwc <= 96 is >= 0.005 from an integer
+      const float rn = __frcp_rn((float)cur.nwc);
+      const int groups = max(1, __float2int_rz((RT_THREADS + 0.5f) * rn));
       const int seg = (cur.nwr + groups - 1) / groups;
-      const int g = tid / cur.nwc, c = tid - g * cur.nwc;
+      const int g = __float2int_rz((tid + 0.5f) * rn), c = tid - g * cur.nwc;
       if (g < groups) {
         double mkt, eref;
         tops_range(P, (double)(cur.wr0 + c), mkt, eref);
