@@ -9,7 +9,7 @@
 //     divisions per call;
 //   * the zero-Doppler Newton uses the exact derivative (3 steps instead of
 //     7-11);
-//   * llh->ECEF trigonometry is computed once per DEM row / column per CTA;
+//   * llh->ECEF trigonometry is computed once per DEM row / column per warp;
 //   * FP64 phases are reduced mod 2 pi in FP64, then rotated in FP32;
 //   * the non-zero-row search is folded into the geocoding epilogue.
 #include <cuda_runtime.h>
@@ -81,12 +81,17 @@ __global__ __launch_bounds__(256) void deramp_kernel(const __grid_constant__ s1b
 }
 
 // ----------------------------------------------------------------- geo2rdr
-// CTA tile: G_TX columns x G_RY rows of the DEM window.  Each thread owns one
-// column and walks down the tile's rows: the zero-Doppler solution of the
-// pixel above seeds the Newton of the next one (adjacent rows are ~2 ms apart
-// in azimuth time, so one exact-Newton step lands below the 5e-9 s
-// tolerance and each pixel needs a single orbit evaluation).  Warps cover
-// 32 consecutive columns of a row, so DEM reads and output writes coalesce.
+// Tile: G_TX columns x G_RY rows of the DEM window, one thread per column
+// walking down the rows.  The zero-Doppler solution of the pixel above seeds
+// the Newton of the next one: the first pixel of a column solves on the
+// window polynomial from the burst centre (like the reference,
+// geo2rdr.cu:588-600), the others on the cubic orbit expansion at that
+// solution, seeded by linear extrapolation of the two pixels above.
+// Latitude terms depend only on the row: lanes 0..G_RY-1 of every warp form
+// them once and the warp shares them by shuffles (no block barrier);
+// longitude terms depend only on the column and stay in registers.  Warps
+// cover 32 consecutive columns of a row, so DEM reads and output writes
+// coalesce; the next row's DEM sample is loaded one row ahead.
 constexpr int G_TX = 128, G_RY = 16;
 
 __global__ void rows_init_kernel(int32_t *rows, int nrow) {
@@ -94,58 +99,59 @@ __global__ void rows_init_kernel(int32_t *rows, int nrow) {
   rows[1] = -1;
 }
 
-__global__ __launch_bounds__(G_TX) void geo2rdr_kernel(
-    const __grid_constant__ s1b_burst_plan_t P, const int16_t *__restrict__ dem, int64_t pitch,
-    const float2 *__restrict__ burst, float2 *__restrict__ out, int32_t *__restrict__ rows,
-    int nrow, int ncol) {
-  __shared__ double s_row[G_RY][3];  // sinlat, coslat, re (per row)
-  __shared__ double s_col[G_TX][2];  // sinlon, coslon (per column)
-  const int tx = threadIdx.x;
-  const int col = blockIdx.x * G_TX + tx;
-  const int row0 = blockIdx.y * G_RY;
-  // llh->ECEF trigonometry (orbit.cu:20-27) once per row / column of the tile
-  if (tx < G_RY) {
-    const double lat = (P.lat0 + (row0 + tx) * P.dlat) * kPiD / 180;
-    double s, c;
-    sincos(lat, &s, &c);
-    s_row[tx][0] = s;
-    s_row[tx][1] = c;
-    s_row[tx][2] = kRaD / sqrt(1. - kRe2D * s * s);
+__device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const int16_t *__restrict__ dem,
+                                             int64_t pitch, const float2 *__restrict__ burst,
+                                             float2 *__restrict__ out, int32_t *__restrict__ rows, int nrow,
+                                             int ncol, int tile_x, int tile_y) {
+  const int tx = threadIdx.x, lane = tx & 31;
+  const int col = tile_x * G_TX + tx;
+  const int row0 = tile_y * G_RY;
+  // llh->ECEF trigonometry (orbit.cu:20-27): row terms on lanes 0..15
+  double r_sin = 0.0, r_cos = 0.0, r_re = 0.0;
+  if (lane < G_RY) {
+    const double lat = (P.lat0 + (row0 + lane) * P.dlat) * kPiD / 180;
+    sincos(lat, &r_sin, &r_cos);
+    r_re = kRaD / sqrt(1. - kRe2D * r_sin * r_sin);
   }
-  {
-    const double lon = (P.lon0 + col * P.dlon) * kPiD / 180;
-    double s, c;
-    sincos(lon, &s, &c);
-    s_col[tx][0] = s;
-    s_col[tx][1] = c;
-  }
-  __syncthreads();
+  double sinlon, coslon;
+  sincos((P.lon0 + col * P.dlon) * kPiD / 180, &sinlon, &coslon);
   const bool colok = col < ncol;
-  const double sinlon = s_col[tx][0], coslon = s_col[tx][1];
   const double inv_dmrg = 1.0 / P.dmrg, prf = 1.0 / P.dtaz, two_over_c = 2.0 / kSolD;
-  // Newton state carried down the column; the first pixel starts at the
-  // burst centre like the reference (geo2rdr.cu:588-600)
-  double t = P.tmid;
-  OrbitState st;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    st.x[i] = P.xmid[i];
-    st.v[i] = P.vmid[i];
-    st.a[i] = P.amid[i];
-  }
+  double t = P.tmid, tprev = 0.0;
+  OrbitCubic oc;
   const int rmax = min(G_RY, nrow - row0);
+  int16_t hn = colok && rmax > 0 ? __ldg(dem + (int64_t)row0 * pitch + col) : 0;
   for (int r = 0; r < rmax; ++r) {
     const int row = row0 + r;
+    const double sinlat = __shfl_sync(0xffffffffu, r_sin, r);
+    const double coslat = __shfl_sync(0xffffffffu, r_cos, r);
+    const double re = __shfl_sync(0xffffffffu, r_re, r);
+    const double h = (double)hn;
+    if (colok && r + 1 < rmax) hn = __ldg(dem + (int64_t)(row + 1) * pitch + col);
     float2 res = make_float2(0.f, 0.f);
     if (colok) {
-      const double h = (double)__ldg(dem + (int64_t)row * pitch + col);
-      const double sinlat = s_row[r][0], coslat = s_row[r][1], re = s_row[r][2];
       double p[3];
       p[0] = (re + h) * coslat * coslon;
       p[1] = (re + h) * coslat * sinlon;
       p[2] = (re * (1 - kRe2D) + h) * sinlat;
       double dr[3];
-      zero_doppler(P.orbit, p, t, st, dr);
+      if (r == 0) {
+        OrbitState st;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          st.x[i] = P.xmid[i];
+          st.v[i] = P.vmid[i];
+          st.a[i] = P.amid[i];
+        }
+        zero_doppler(P.orbit, p, t, st, dr);
+        orbit_cubic(P.orbit, t, oc);
+        tprev = t - P.dtaz;
+      } else {
+        const double tn = 2.0 * t - tprev;
+        tprev = t;
+        t = tn;
+        zero_doppler_cubic(oc, p, t, dr);
+      }
       const double rng = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
       const double rgoff = (rng - P.rngstart) * inv_dmrg;
       const double azoff = (t - P.tstart) * prf;
@@ -186,11 +192,18 @@ __global__ __launch_bounds__(G_TX) void geo2rdr_kernel(
     }
     // first / last non-zero output row (geo2rdr.cu:86-128): one vote per warp
     const unsigned nz = __ballot_sync(0xffffffffu, colok && (res.x != 0.f || res.y != 0.f));
-    if (nz && (tx & 31) == 0 && rows) {
+    if (nz && lane == 0 && rows) {
       atomicMin(rows, row);
       atomicMax(rows + 1, row + 1);
     }
   }
+}
+
+__global__ __launch_bounds__(G_TX) void geo2rdr_kernel(
+    const __grid_constant__ s1b_burst_plan_t P, const int16_t *__restrict__ dem, int64_t pitch,
+    const float2 *__restrict__ burst, float2 *__restrict__ out, int32_t *__restrict__ rows,
+    int nrow, int ncol) {
+  geo2rdr_tile(P, dem, pitch, burst, out, rows, nrow, ncol, blockIdx.x, blockIdx.y);
 }
 
 // ------------------------------------------------- generic geometry kernels

@@ -27,66 +27,9 @@ constexpr double kRe2D = 0.00669437999015;
 
 // -------------------------------------------------------------- offsets
 // Same column walk as the geocoding kernel: thread = reference column, 16
-// rows per thread.  The first row's zero-Doppler time is solved on the
-// window polynomial from the burst centre; there the orbit is expanded to
-// third order (position, velocity, acceleration, jerk), and the other rows
-// solve on that cubic.  Over the segment (|t - t0| <= 16 lines ~ 0.035 s)
-// the dropped fourth-order term is snap |dt|^4 / 24 < 1e-12 m for an orbit
-// (snap ~ omega^4 r ~ 1e-5 m/s^4), far below the 1e-4 sample tolerance.
+// rows per thread; the first row solves on the window polynomial from the
+// burst centre, the others on the cubic expansion there (OrbitCubic).
 constexpr int O_TX = 128, O_RY = 16;
-
-struct OrbitCubic {
-  double t0, x[3], v[3], a[3], j[3];
-};
-
-// Position and the first three derivatives of the window polynomial at t.
-__device__ __forceinline__ void orbit_cubic(const s1b_orbit_poly_t &P, double t, OrbitCubic &o) {
-  const int w = s1b_orbit_window(P, t) - 1;
-  const double tau = t - P.tc[w];
-  o.t0 = t;
-#pragma unroll
-  for (int comp = 0; comp < 3; ++comp) {
-    const double *c = P.c[w][comp];
-    double f = c[7], d = 0.0, dd = 0.0, ddd = 0.0;
-#pragma unroll
-    for (int k = 6; k >= 0; --k) {
-      ddd = fma(ddd, tau, dd);
-      dd = fma(dd, tau, d);
-      d = fma(d, tau, f);
-      f = fma(f, tau, c[k]);
-    }
-    o.x[comp] = f;
-    o.v[comp] = d;
-    o.a[comp] = 2.0 * dd;
-    o.j[comp] = 6.0 * ddd;
-  }
-}
-
-// Zero-Doppler Newton (same iteration and stopping rule as zero_doppler)
-// with the orbit state taken from the cubic expansion.
-__device__ __forceinline__ void zero_doppler_cubic(const OrbitCubic &o, const double p[3], double &t, double dr[3]) {
-  for (int it = 0; it < 51; ++it) {
-    const double h = t - o.t0;
-    double fn = 0.0, fp = 0.0, v[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      const double a = fma(o.j[i], h, o.a[i]);
-      v[i] = fma(fma(0.5 * o.j[i], h, o.a[i]), h, o.v[i]);
-      const double x = fma(fma(fma(o.j[i] * (1.0 / 6.0), h, 0.5 * o.a[i]), h, o.v[i]), h, o.x[i]);
-      dr[i] = p[i] - x;
-      fn = fma(dr[i], v[i], fn);
-      fp = fma(dr[i], a, fp);
-      fp = fma(-v[i], v[i], fp);
-    }
-    const double step = fn / fp;
-    t -= step;
-    if (fabs(step) < 5.0e-9) {
-#pragma unroll
-      for (int i = 0; i < 3; ++i) dr[i] = fma(step, v[i], dr[i]);
-      return;
-    }
-  }
-}
 
 __device__ __forceinline__ void llh_ecef(double lat_deg, double lon_deg, double h, double p[3]) {
   double sl, cl, so, co;
