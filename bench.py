@@ -42,9 +42,13 @@ UNIT = "burst-px/s"
 # output (complex64) per geo pixel, the deramped burst read once.
 GEO_BYTES_PER_GEO_PX = 2 + 8
 GEO_BYTES_PER_BURST_PX = 8
-# DRAM bytes of one geocoding launch per geo pixel, from the ncu capture
-# summarised in profiles/geo2rdr_c1.md (dram__bytes_read.sum + write.sum).
-GEO_DRAM_BYTES_PER_GEO_PX = None
+# Measured DRAM traffic (ncu dram__bytes_read.sum + dram__bytes_write.sum of
+# one launch on the 1500 x 21000 burst pair, divided by the units it
+# processed): geocoding per geo pixel (16.06 M geo px: 274.0 + 92.2 MB) and
+# the TMA resampler per output pixel (31.5 M px: 550.9 + 228.7 MB).  Both
+# kernels stream their inputs once, so traffic scales with the unit count.
+GEO_DRAM_BYTES_PER_GEO_PX = 22.81
+RESAMPLE_DRAM_BYTES_PER_PX = 24.75
 
 
 def parse():
@@ -480,9 +484,11 @@ def run_s1b(args):
                  "geo_px_total": sum(p.nrow * p.ncol for p in chain.plans), "ifg_ml": list(res.ifg.shape)}
         launches = chain.launches_per_step()
     traffic = None
-    if top == "geo2rdr" and GEO_DRAM_BYTES_PER_GEO_PX is not None:
+    if top == "geo2rdr":
         pls = [p for pl in chain.pairs for p in pl] if args.config == "frame" else chain.plans
         traffic = GEO_DRAM_BYTES_PER_GEO_PX * sum(p.nrow * p.ncol for p in pls) / len(pls)
+    elif top == "resample":
+        traffic = RESAMPLE_DRAM_BYTES_PER_PX * chain.burst_pixels
     cfg = {"workload": desc, "looks": [sc.rowlook, sc.collook],
            "goldstein": {"alpha": sc.alpha, "n_win": 32, "step": 8},
            "l2": "inputs larger than L2 (>= 252 MB per SLC, read once per step)", "parallelism": f"replicas{world}"}
