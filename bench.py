@@ -57,7 +57,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="s1b", choices=["s1b", "reference"])
-    ap.add_argument("--config", default="frame", choices=["frame", "c1", "c1geo", "c0", "small"])
+    ap.add_argument("--config", default="frame", choices=["frame", "frame_pairs", "c1", "c1geo", "c0", "small"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -243,11 +243,26 @@ def _workload(args, rank, dev):
     from sentinel_gpu_processor_b200 import synth
     from sentinel_gpu_processor_b200.chain import FrameChain, PairChain
     if args.config == "frame":
+        import torch
+
+        from sentinel_gpu_processor_b200.chain import BatchedFrameChain
+        sc = synth.make_frame(seed=20261203 + 2000 + rank, device=dev)
+        chain = BatchedFrameChain(sc.ref, sc.sec, sc.rsc, sc.rowlook, sc.collook, sc.alpha, device=dev)
+        chain.load(sc.ref_slc, sc.sec_slc)
+        torch.cuda.synchronize()
+        sc.ref_slc = sc.sec_slc = None  # the frame's SLC buffer holds them now
+        chain.tuned = chain.autotune(sc.dem, reps=2)
+        chain.capture(sc.dem)
+        desc = (f"full IW frame: {chain.n_pairs} burst pairs (3 subswaths x 9) of uneven size, lines 1480-1530, "
+                f"samples 20000-25500, 100-line overlap; batched: one launch per stage over the descriptor table "
+                f"of all {2 * chain.n_pairs} bursts, one CUDA graph per step, tile shapes from the autotuner")
+        return sc, chain, chain.replay, desc
+    if args.config == "frame_pairs":
         sc = synth.make_frame(seed=20261203 + 2000 + rank, device=dev)
         chain = FrameChain(sc.ref, sc.sec, sc.rsc, sc.rowlook, sc.collook, sc.alpha, device=dev)
         ins = (sc.ref_slc, sc.sec_slc, sc.dem)
-        desc = (f"full IW frame: {len(sc.ref)} bursts (3 subswaths x 9) of uneven size, lines 1480-1530, samples "
-                f"20000-25500, 100-line overlap")
+        desc = (f"full IW frame: {len(sc.ref)} burst pairs (3 subswaths x 9) of uneven size, lines 1480-1530, "
+                f"samples 20000-25500, 100-line overlap; pair by pair (one host synchronisation per pair)")
         return sc, chain, lambda: chain.run(*ins), desc
     if args.config == "c1":
         from sentinel_gpu_processor_b200.chain import RadarChain
@@ -274,7 +289,9 @@ def _e2e(chain, sc, args, world):
     import torch
     if args.config == "c1":
         return _e2e_radar(chain, sc, args, world)
-    frame = args.config == "frame"
+    if args.config == "frame":
+        return _e2e_frame(chain, sc, args, world)
+    frame = args.config == "frame_pairs"
     refs = sc.ref_slc if frame else sc.ref_slc[:1]
     secs = sc.sec_slc if frame else sc.sec_slc[:1]
     ref_h = [t.cpu().pin_memory() for t in refs]
@@ -315,6 +332,43 @@ def _e2e(chain, sc, args, world):
     d2h = 0
     for _ in range(k_e2e):
         d2h = step()
+    t2.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(s2.elapsed_time(t2), world)
+    return world * k_e2e * chain.burst_pixels / (e2e_ms / 1e3), h2d, d2h
+
+
+def _e2e_frame(chain, sc, args, world):
+    """End to end for the batched frame: pinned H2D of every burst of both
+    acquisitions into the frame's SLC buffer and of the DEM, graph replay,
+    D2H of the product arrays (ifg, amplitudes, coherence, filtered ifg)."""
+    import torch
+    views = chain.ref_views + chain.sec_views
+    host_in = [v.cpu().pin_memory() for v in views]
+    dem_h = sc.dem.cpu().pin_memory()
+    outs = (chain.ifg, chain.amp1, chain.amp2, chain.coh, chain.filt)
+    host_out = [torch.empty(o.shape, dtype=o.dtype, pin_memory=True) for o in outs]
+    h2d = sum(t.numel() * t.element_size() for t in host_in) + dem_h.numel() * dem_h.element_size()
+    d2h = sum(t.numel() * t.element_size() for t in host_out)
+
+    def step():
+        sc.dem.copy_(dem_h, non_blocking=True)
+        for v, h in zip(views, host_in):
+            v.copy_(h, non_blocking=True)
+        chain.replay()
+        for h, o in zip(host_out, outs):
+            h.copy_(o, non_blocking=True)
+
+    step()
+    torch.cuda.synchronize()
+    k_e2e = max(3, args.steps // 4)
+    barrier(world)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    s2, t2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s2.record(stream)
+    for _ in range(k_e2e):
+        step()
     t2.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(s2.elapsed_time(t2), world)
@@ -403,14 +457,24 @@ def _kernel_table(chain, sc, args, times, peak):
         box_px = chain.box[2] * chain.box[3]
         bytes_per = {"geo2rdr_offsets": 32 * px, "resample": 24 * px, "crossmul_looks": 16 * box_px + 20 * ml,
                      "box_coherence": 20 * px, "goldstein": 16 * ml}
+    elif args.config == "frame":
+        # one launch per stage covers every burst / pair of the frame
+        pls = chain.plans
+        burst = sum(p.lines * p.samples for p in pls)
+        geo = sum(p.nrow * p.ncol for p in pls)
+        res = [r for r in chain.last if r is not None]
+        box_px = sum((r.box[2] - r.box[0]) * (r.box[3] - r.box[1]) for r in res)
+        ml = sum(r.ifg.numel() for r in res)
+        bytes_per = {"deramp": 16 * burst, "geo2rdr": GEO_BYTES_PER_GEO_PX * geo + GEO_BYTES_PER_BURST_PX * burst,
+                     "crossmul_looks": 16 * box_px + 20 * ml, "goldstein": 16 * ml}
     else:
-        pls = [p for pl in chain.pairs for p in pl] if args.config == "frame" else chain.plans
+        pls = [p for pl in chain.pairs for p in pl] if args.config == "frame_pairs" else chain.plans
         n = len(pls)
         burst = sum(p.lines * p.samples for p in pls) / n
         geo = sum(p.nrow * p.ncol for p in pls) / n
         bytes_per = {"deramp": 16 * burst, "geo2rdr": GEO_BYTES_PER_GEO_PX * geo + GEO_BYTES_PER_BURST_PX * burst}
-        if args.config == "frame":
-            res = chain.last
+        if args.config == "frame_pairs":
+            res = [r for r in chain.last if r is not None]
             box_px = sum((r.box[2] - r.box[0]) * (r.box[3] - r.box[1]) for r in res) / len(res)
             ml = sum(r.ifg.numel() for r in res) / len(res)
         else:
@@ -438,6 +502,8 @@ def run_s1b(args):
     for _ in range(warm):
         res = run()
     torch.cuda.synchronize()
+    if args.config == "frame":
+        res = chain.results()
     if res is None or (isinstance(res, list) and any(r is None for r in res)):
         raise SystemExit("empty interferogram for the synthetic input")
     if hasattr(chain, "staging_ok") and not chain.staging_ok():
@@ -451,7 +517,8 @@ def run_s1b(args):
     stop = torch.cuda.Event(enable_timing=True)
     start.record(stream)
     for _ in range(args.steps):
-        res = run()
+        out = run()
+        res = res if out is None else out
     stop.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
@@ -466,14 +533,26 @@ def run_s1b(args):
     else:
         chain.last = res
     peak, peak_kind = peaks()
-    times = _instrumented(run if args.config != "c1" else (lambda: chain.run(*_radar_inputs(sc))),
-                          max(2, min(args.steps, 10)))
+    if args.config == "frame":
+        times = {}
+        for _ in range(max(2, min(args.steps, 10))):
+            for name, ms in chain.profile(sc.dem).items():
+                times.setdefault(name, []).append(ms)
+    else:
+        times = _instrumented(run if args.config != "c1" else (lambda: chain.run(*_radar_inputs(sc))),
+                              max(2, min(args.steps, 10)))
     table = _kernel_table(chain, sc, args, times, peak)
     top = max(table, key=lambda n: table[n]["total_ms"])
     if args.config == "frame":
-        extra = {"bursts": len(chain.pairs), "burst_px_per_step": chain.burst_pixels,
+        extra = {"burst_pairs": chain.n_pairs, "burst_px_per_step": chain.burst_pixels,
                  "geo_px_total": sum(chain.geo_pixels()),
-                 "ifg_ml_shapes_first3": [list(r.ifg.shape) for r in res[:3]]}
+                 "ifg_ml_shapes_first3": [list(r.ifg.shape) for r in res[:3]],
+                 "batched": True, "cuda_graph": True, "tuning": chain.tuned}
+        launches = chain.launches_per_step()
+    elif args.config == "frame_pairs":
+        extra = {"burst_pairs": len(chain.pairs), "burst_px_per_step": chain.burst_pixels,
+                 "geo_px_total": sum(chain.geo_pixels()),
+                 "ifg_ml_shapes_first3": [list(r.ifg.shape) for r in res[:3]], "batched": False}
         launches = chain.launches_per_step()
     elif args.config == "c1":
         extra = {"lines": chain.L, "samples": chain.S, "ifg_ml": list(res["ifg"].shape), "interp": chain.interp,
@@ -485,8 +564,11 @@ def run_s1b(args):
         launches = chain.launches_per_step()
     traffic = None
     if top == "geo2rdr":
-        pls = [p for pl in chain.pairs for p in pl] if args.config == "frame" else chain.plans
-        traffic = GEO_DRAM_BYTES_PER_GEO_PX * sum(p.nrow * p.ncol for p in pls) / len(pls)
+        if args.config == "frame":  # one launch geocodes every burst
+            traffic = GEO_DRAM_BYTES_PER_GEO_PX * sum(p.nrow * p.ncol for p in chain.plans)
+        else:
+            pls = [p for pl in chain.pairs for p in pl] if args.config == "frame_pairs" else chain.plans
+            traffic = GEO_DRAM_BYTES_PER_GEO_PX * sum(p.nrow * p.ncol for p in pls) / len(pls)
     elif top == "resample":
         traffic = RESAMPLE_DRAM_BYTES_PER_PX * chain.burst_pixels
     cfg = {"workload": desc, "looks": [sc.rowlook, sc.collook],
@@ -504,7 +586,8 @@ def run_s1b(args):
         "roofline": {"bound": "hbm", "kernel": top, "achieved": t["achieved_gbs"], "peak": peak, "unit": "GB/s",
                      "frac": t["frac"], "traffic": traffic, "peak_kind": peak_kind,
                      "bytes_per_launch": t["bytes_per_launch"], "launch_ms": t["avg_ms"],
-                     "timed": "CUDA events around every launch of the entry point over instrumented eager steps",
+                     "timed": ("CUDA events between the stages of profiled frame runs" if args.config == "frame"
+                               else "CUDA events around every launch of the entry point over instrumented eager steps"),
                      "note": ("FP64-compute bound (zero-Doppler Newton): low HBM fraction by design"
                               if top in ("geo2rdr", "geo2rdr_offsets") else "HBM-bound")},
         "kernels": table,
@@ -539,7 +622,7 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "reference executables not built in oracle/_ref "
                                                               "(python oracle/build_ref.py)"}))
         return
-    if args.config == "frame":
+    if args.config in ("frame", "frame_pairs"):
         # a bounded sample of the frame: its first burst pair (the reference
         # runs geo2rdr once per burst for uneven burst sizes)
         frame = synth.make_frame(seed=20261203 + 2000, device="cuda")

@@ -310,6 +310,83 @@ int s1b_goldstein(const void *in, void *out, int32_t nrow, int32_t ncol, int32_t
 int s1b_goldstein_noalloc(const void *in, void *out, int32_t nrow, int32_t ncol, int32_t n_win,
                           float alpha, void *stream);
 
+/* ------------------------------------------------------------ batched frame
+ * All burst pairs of a frame (e.g. 3 subswaths x 9 bursts of uneven size)
+ * processed with one launch per stage over a per-burst descriptor table:
+ * deramp and geocoding are persistent kernels over the flat tile space of
+ * every burst; the crossmul box of each pair is formed on the device from the
+ * crop rows, so a run has no host synchronisation and can be captured in a
+ * CUDA graph.  Replaces running geo2rdr per burst, crossmul_daemon and
+ * goldstein per pair (csrc/src/geo2rdr.cu:316-651, crossmul_daemon.cu:566-975,
+ * goldstein.cu:328-408); the per-pair results are those of s1b_deramp,
+ * s1b_geo2rdr, s1b_crossmul_box, s1b_crossmul_looks and s1b_goldstein. */
+
+typedef struct s1b_frame s1b_frame_t;
+
+/* Per-pair result of a frame run, written on the device. */
+typedef struct {
+  int32_t ok;           /* 1: products valid; 0: a burst geocoded empty or the overlap is empty */
+  int32_t nrow_ml, ncol_ml;
+  int32_t filtered;     /* 1: Goldstein ran; 0: image smaller than n_win, filt = ifg */
+  int32_t header[6];    /* interferogram header words (crossmul_daemon.cu:660-666) */
+  int32_t box[4];       /* full-resolution box: left, top, right, bottom (DEM grid) */
+  int32_t gslc_rows[4]; /* crop rows of ref and sec: first, last (exclusive), window rows */
+} s1b_frame_pair_t;
+
+typedef struct {
+  size_t workspace_bytes;   /* device scratch: deramped bursts, geocoded windows, patches */
+  int64_t slc_elems;        /* complex64 elements of the SLC buffer: bursts back to back */
+  int64_t product_elems;    /* elements of each product array (all pairs' slots) */
+  int32_t max_nrow_ml, max_ncol_ml;
+} s1b_frame_sizes_t;
+
+/* Host only (uploads the descriptor tables; allocates them on the current
+ * device).  plans: n_bursts burst plans on one DEM grid (s1b_burst_plan with
+ * the same RSC); pair_ref/pair_sec: burst indices of each pair; n_win must
+ * be 32.  Bursts whose DEM window is empty return S1B_ERR_EMPTY. */
+int s1b_frame_create(const s1b_burst_plan_t *plans, int32_t n_bursts, const int32_t *pair_ref,
+                     const int32_t *pair_sec, int32_t n_pairs, int32_t rowlook, int32_t collook,
+                     int32_t n_win, float alpha, uint64_t fill_seed, s1b_frame_t **frame);
+void s1b_frame_destroy(s1b_frame_t *frame);
+int s1b_frame_sizes(const s1b_frame_t *frame, s1b_frame_sizes_t *sizes);
+/* Element offset of burst b in the SLC buffer (lines * samples of the bursts before it). */
+int s1b_frame_burst_offset(const s1b_frame_t *frame, int32_t burst, int64_t *slc_off);
+/* Slot of pair k in the product arrays: first element and capacity. */
+int s1b_frame_pair_slot(const s1b_frame_t *frame, int32_t pair, int64_t *ml_off, int32_t *max_nrow_ml,
+                        int32_t *max_ncol_ml);
+
+/* Enqueue one frame run on `stream` (no host synchronisation).
+ * slc: complex64 [slc_elems] device; dem: int16 RSC grid, row pitch in
+ * elements; workspace: workspace_bytes, 16-byte aligned; ifg/filt complex64
+ * and amp1/amp2/coh float32 [product_elems] (amp1/amp2/coh may be NULL);
+ * pairs: s1b_frame_pair_t [n_pairs] device.  Pair k's products are row-major
+ * [nrow_ml x ncol_ml] at its slot. */
+int s1b_frame_run(s1b_frame_t *frame, const void *slc, const int16_t *dem, int64_t dem_pitch,
+                  void *workspace, void *ifg, float *amp1, float *amp2, float *coh, void *filt,
+                  s1b_frame_pair_t *pairs, void *stream);
+
+/* Autotuner: times the candidate tile shapes and persistent grid sizes of
+ * the deramp and geocoding stages on these buffers (`reps` runs each, CUDA
+ * events on `stream`), keeps the fastest in the frame for later runs and
+ * synchronises the stream.  Not capturable.  Every candidate produces the
+ * same results. */
+int s1b_frame_autotune(s1b_frame_t *frame, const void *slc, const int16_t *dem, int64_t dem_pitch,
+                       void *workspace, void *ifg, float *amp1, float *amp2, float *coh, void *filt,
+                       s1b_frame_pair_t *pairs, int32_t reps, void *stream);
+
+/* One run with CUDA events between its stages (synchronises the stream):
+ * stage_ms[5] = deramp, geocoding, box, crossmul, Goldstein (patches and
+ * overlap-add), in milliseconds.  For measurement; not capturable. */
+int s1b_frame_profile(s1b_frame_t *frame, const void *slc, const int16_t *dem, int64_t dem_pitch,
+                      void *workspace, void *ifg, float *amp1, float *amp2, float *coh, void *filt,
+                      s1b_frame_pair_t *pairs, float *stage_ms, void *stream);
+
+/* Current tuning: [deramp rows per tile, deramp CTAs, geocoding columns per
+ * tile, geocoding CTAs] (CTAs 0 = whole device). */
+int s1b_frame_tuning(const s1b_frame_t *frame, int32_t tuning[4]);
+/* Set the tuning by hand (validated; S1B_ERR_UNSUPPORTED for a shape not built). */
+int s1b_frame_set_tuning(s1b_frame_t *frame, const int32_t tuning[4]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -95,6 +95,17 @@ class BurstPlan(ctypes.Structure):
 
 
 # name -> (restype, argtypes); the table is the C ABI of include/s1b.h
+class FramePair(ctypes.Structure):
+    """s1b_frame_pair_t: per-pair result of a frame run."""
+    _fields_ = [("ok", c_int32), ("nrow_ml", c_int32), ("ncol_ml", c_int32), ("filtered", c_int32),
+                ("header", c_int32 * 6), ("box", c_int32 * 4), ("gslc_rows", c_int32 * 4)]
+
+
+class FrameSizes(ctypes.Structure):
+    _fields_ = [("workspace_bytes", c_size_t), ("slc_elems", c_int64), ("product_elems", c_int64),
+                ("max_nrow_ml", c_int32), ("max_ncol_ml", c_int32)]
+
+
 _SIGNATURES = {
     "s1b_status_string": (c_char_p, [c_int]),
     "s1b_version": (c_int, []),
@@ -126,6 +137,20 @@ _SIGNATURES = {
     "s1b_goldstein": (c_int, [c_void_p, c_void_p, c_int32, c_int32, c_int32, c_float, c_void_p, c_size_t,
                               c_void_p]),
     "s1b_goldstein_noalloc": (c_int, [c_void_p, c_void_p, c_int32, c_int32, c_int32, c_float, c_void_p]),
+    "s1b_frame_create": (c_int, [POINTER(BurstPlan), c_int32, POINTER(c_int32), POINTER(c_int32), c_int32, c_int32,
+                                 c_int32, c_int32, c_float, c_uint64, POINTER(c_void_p)]),
+    "s1b_frame_destroy": (None, [c_void_p]),
+    "s1b_frame_sizes": (c_int, [c_void_p, POINTER(FrameSizes)]),
+    "s1b_frame_burst_offset": (c_int, [c_void_p, c_int32, POINTER(c_int64)]),
+    "s1b_frame_pair_slot": (c_int, [c_void_p, c_int32, POINTER(c_int64), POINTER(c_int32), POINTER(c_int32)]),
+    "s1b_frame_run": (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p,
+                              c_void_p, c_void_p, c_void_p, c_void_p]),
+    "s1b_frame_autotune": (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p,
+                                   c_void_p, c_void_p, c_void_p, c_int32, c_void_p]),
+    "s1b_frame_profile": (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p,
+                                  c_void_p, c_void_p, c_void_p, POINTER(c_float), c_void_p]),
+    "s1b_frame_tuning": (c_int, [c_void_p, POINTER(c_int32)]),
+    "s1b_frame_set_tuning": (c_int, [c_void_p, POINTER(c_int32)]),
 }
 
 _lib = None

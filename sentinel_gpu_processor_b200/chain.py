@@ -310,3 +310,190 @@ class RadarChain:
     def launches_per_step():
         # offsets, resample, crossmul, box coherence (+ status memset), goldstein patch + gather
         return 6
+
+
+class BatchedFrameChain:
+    """All burst pairs of a frame through one batched launch sequence
+    (``s1b_frame_run``): deramp and geocoding as persistent kernels over every
+    burst, the crossmul box of each pair formed on the device, crossmul and
+    Goldstein over all pairs.  No host synchronisation inside a run, so it is
+    captured in a CUDA graph (``capture``/``replay``).  Per-pair products are
+    those of :class:`FrameChain` (same kernels, same order of operations).
+
+    The SLCs live back to back in one device buffer; ``ref_views``/``sec_views``
+    are the per-burst views to fill.  ``autotune`` picks the deramp and
+    geocoding tile shapes and grid sizes on the actual frame.
+    """
+
+    def __init__(self, refs, secs, rsc, rowlook, collook, alpha, n_win=32, device="cuda", fill_seed=0):
+        import ctypes
+        self.dev = torch.device(device)
+        self.rowlook, self.collook, self.alpha, self.n_win = int(rowlook), int(collook), float(alpha), int(n_win)
+        self.fill_seed = int(fill_seed)
+        plans = []
+        for ra, sa in zip(refs, secs):
+            for a in (ra, sa):
+                p = _plan.burst_plan(a.radar, a.orbit, a.fm, a.dc, a.bursts[0], rsc)
+                if p.nrow <= 0 or p.ncol <= 0:
+                    raise _lib.S1BError(_lib.S1B_ERR_EMPTY, "BatchedFrameChain: burst outside the DEM grid")
+                plans.append(p)
+        self.plans = plans
+        self.n_pairs = len(refs)
+        lib = _lib.load()
+        arr = (_lib.BurstPlan * len(plans))(*plans)
+        pref = (ctypes.c_int32 * self.n_pairs)(*range(0, 2 * self.n_pairs, 2))
+        psec = (ctypes.c_int32 * self.n_pairs)(*range(1, 2 * self.n_pairs, 2))
+        handle = ctypes.c_void_p()
+        with torch.cuda.device(self.dev):
+            _lib.check(lib.s1b_frame_create(arr, len(plans), pref, psec, self.n_pairs, self.rowlook, self.collook,
+                                            self.n_win, self.alpha, self.fill_seed, ctypes.byref(handle)),
+                       "s1b_frame_create")
+        self._handle = handle
+        sz = _lib.FrameSizes()
+        _lib.check(lib.s1b_frame_sizes(handle, ctypes.byref(sz)), "s1b_frame_sizes")
+        self.sizes = sz
+        self.slc = torch.empty(int(sz.slc_elems), dtype=torch.complex64, device=self.dev)
+        self.workspace = torch.empty(int(sz.workspace_bytes), dtype=torch.uint8, device=self.dev)
+        n = int(sz.product_elems)
+        self.ifg = torch.empty(n, dtype=torch.complex64, device=self.dev)
+        self.filt = torch.empty(n, dtype=torch.complex64, device=self.dev)
+        self.amp1 = torch.empty(n, dtype=torch.float32, device=self.dev)
+        self.amp2 = torch.empty(n, dtype=torch.float32, device=self.dev)
+        self.coh = torch.empty(n, dtype=torch.float32, device=self.dev)
+        self.pair_size = ctypes.sizeof(_lib.FramePair)
+        self.pairs_dev = torch.zeros(self.n_pairs * self.pair_size, dtype=torch.uint8, device=self.dev)
+        self.pairs_host = torch.empty(self.n_pairs * self.pair_size, dtype=torch.uint8,
+                                      pin_memory=torch.cuda.is_available())
+        views = []
+        for b, p in enumerate(plans):
+            off = ctypes.c_int64()
+            _lib.check(lib.s1b_frame_burst_offset(handle, b, ctypes.byref(off)), "s1b_frame_burst_offset")
+            views.append(self.slc[off.value:off.value + p.lines * p.samples].view(p.lines, p.samples))
+        self.ref_views, self.sec_views = views[0::2], views[1::2]
+        self.slots = []
+        for k in range(self.n_pairs):
+            off, r, c = ctypes.c_int64(), ctypes.c_int32(), ctypes.c_int32()
+            _lib.check(lib.s1b_frame_pair_slot(handle, k, ctypes.byref(off), ctypes.byref(r), ctypes.byref(c)),
+                       "s1b_frame_pair_slot")
+            self.slots.append((off.value, r.value, c.value))
+        self.burst_pixels = sum(p.lines * p.samples for p in plans[0::2])
+        self.graph = None
+        self.geo_events = None
+
+    def __del__(self):
+        h = getattr(self, "_handle", None)
+        if h is not None and h.value:
+            try:
+                _lib.load().s1b_frame_destroy(h)
+            except Exception:
+                pass
+            self._handle = None
+
+    def _args(self, dem):
+        if dem.dtype != torch.int16 or dem.dim() != 2 or dem.stride(1) != 1 or dem.device != self.dev:
+            raise ValueError("dem must be an int16 [nlat, nlon] device raster with unit column stride")
+        if dem.shape[0] < max(p.win_bottom for p in self.plans) or dem.shape[1] < max(p.win_right for p in self.plans):
+            raise ValueError("dem does not cover every burst's DEM window")
+        return (self._handle, _lib.dptr(self.slc), _lib.dptr(dem), dem.stride(0), _lib.dptr(self.workspace),
+                _lib.dptr(self.ifg), _lib.dptr(self.amp1), _lib.dptr(self.amp2), _lib.dptr(self.coh),
+                _lib.dptr(self.filt), _lib.dptr(self.pairs_dev))
+
+    def load(self, ref_slcs, sec_slcs):
+        """Copy per-burst SLCs (device or pinned host tensors) into the frame buffer."""
+        for v, s in zip(self.ref_views + self.sec_views, list(ref_slcs) + list(sec_slcs)):
+            v.copy_(s.reshape(v.shape), non_blocking=True)
+
+    def run(self, dem):
+        """One frame run on the current stream (inputs already in ``slc``)."""
+        _lib.check(_call_frame("frame_run", _lib.load().s1b_frame_run, *self._args(dem), _lib.stream_ptr()),
+                   "s1b_frame_run")
+
+    def autotune(self, dem, reps=3):
+        """Time the tile-shape / grid candidates on this frame and keep the fastest."""
+        _lib.check(_lib.load().s1b_frame_autotune(*self._args(dem), int(reps), _lib.stream_ptr()),
+                   "s1b_frame_autotune")
+        return self.tuning()
+
+    def profile(self, dem):
+        """One run with CUDA events between stages: ms of deramp, geocoding, box,
+        crossmul, Goldstein (synchronises)."""
+        import ctypes
+        ms = (ctypes.c_float * 5)()
+        _lib.check(_lib.load().s1b_frame_profile(*self._args(dem), ms, _lib.stream_ptr()), "s1b_frame_profile")
+        return dict(zip(("deramp", "geo2rdr", "box", "crossmul_looks", "goldstein"), list(ms)))
+
+    def tuning(self):
+        import ctypes
+        t = (ctypes.c_int32 * 4)()
+        _lib.check(_lib.load().s1b_frame_tuning(self._handle, t), "s1b_frame_tuning")
+        return {"deramp_rows": t[0], "deramp_ctas": t[1], "geo_cols": t[2], "geo_ctas": t[3]}
+
+    def set_tuning(self, deramp_rows=16, deramp_ctas=0, geo_cols=128, geo_ctas=0):
+        import ctypes
+        t = (ctypes.c_int32 * 4)(deramp_rows, deramp_ctas, geo_cols, geo_ctas)
+        _lib.check(_lib.load().s1b_frame_set_tuning(self._handle, t), "s1b_frame_set_tuning")
+
+    def capture(self, dem):
+        """Record one frame run into a CUDA graph; ``replay()`` reruns it."""
+        self.run(dem)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(g, stream=s):
+                self.run(dem)
+        torch.cuda.current_stream().wait_stream(s)
+        self.graph = g
+
+    def replay(self):
+        self.graph.replay()
+
+    def pair_table(self):
+        """Per-pair results of the last run (synchronises): list of dicts."""
+        import ctypes
+        self.pairs_host.copy_(self.pairs_dev, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        raw = bytes(self.pairs_host.numpy())
+        out = []
+        for k in range(self.n_pairs):
+            r = _lib.FramePair.from_buffer_copy(raw[k * self.pair_size:(k + 1) * self.pair_size])
+            out.append({"ok": bool(r.ok), "nrow_ml": r.nrow_ml, "ncol_ml": r.ncol_ml, "filtered": bool(r.filtered),
+                        "header": list(r.header), "box": tuple(r.box), "gslc_rows": list(r.gslc_rows)})
+        return out
+
+    def results(self):
+        """PairResult per pair (views into the product arrays), None for empty pairs."""
+        res = []
+        for k, r in enumerate(self.pair_table()):
+            if not r["ok"]:
+                res.append(None)
+                continue
+            off = self.slots[k][0]
+            n = r["nrow_ml"] * r["ncol_ml"]
+            shape = (r["nrow_ml"], r["ncol_ml"])
+            p1, p2 = self.plans[2 * k], self.plans[2 * k + 1]
+            g = r["gslc_rows"]
+            hs = (formats.make_header(p1.rsc_nlat, p1.rsc_nlon, p1.win_left, p1.win_top + g[0], p1.win_right,
+                                      p1.win_top + g[1]),
+                  formats.make_header(p2.rsc_nlat, p2.rsc_nlon, p2.win_left, p2.win_top + g[2], p2.win_right,
+                                      p2.win_top + g[3]))
+            res.append(PairResult(header=formats.make_header(*r["header"]), box=r["box"],
+                                  ifg=self.ifg[off:off + n].view(shape), amp1=self.amp1[off:off + n].view(shape),
+                                  amp2=self.amp2[off:off + n].view(shape), coh=self.coh[off:off + n].view(shape),
+                                  filt=self.filt[off:off + n].view(shape), gslc_headers=hs))
+        return res
+
+    def launches_per_step(self):
+        # init, deramp, geocoding, box, crossmul, Goldstein patches, Goldstein gather
+        return 7
+
+    def geo_pixels(self):
+        return [p.nrow * p.ncol for p in self.plans]
+
+    def burst_pixels_all(self):
+        return [p.lines * p.samples for p in self.plans]
+
+
+def _call_frame(name, fn, *args):
+    return kernels._call(name, fn, *args)

@@ -16,6 +16,7 @@
 
 #include "s1b.h"
 #include "s1b_device.cuh"
+#include "s1b_frame.h"
 #include "s1b_internal.h"
 
 namespace {
@@ -50,13 +51,12 @@ struct XmArgs {
   uint64_t seed;
 };
 
-__global__ __launch_bounds__(XM_THREADS) void crossmul_looks_kernel(const XmArgs a) {
-  extern __shared__ float4 smem4[];
+// One CTA: multilooked row i, columns [chunk * m_per_cta, ...).
+__device__ __forceinline__ void crossmul_tile(const XmArgs &a, int i, int chunk, float4 *smem4) {
   const int W = a.m_per_cta * a.collook;  // full-res columns of this CTA
   float2 *sI = reinterpret_cast<float2 *>(smem4);
   float2 *sP = sI + W;  // (|ref|^2, |sec|^2) per column
-  const int i = blockIdx.x;
-  const int j0 = blockIdx.y * a.m_per_cta;
+  const int j0 = chunk * a.m_per_cta;
   const int mcta = min(a.m_per_cta, a.ncol_ml - j0);
   const int wcta = mcta * a.collook;
   const int64_t col0 = (int64_t)j0 * a.collook;
@@ -147,6 +147,94 @@ __global__ __launch_bounds__(XM_THREADS) void crossmul_looks_kernel(const XmArgs
   }
 }
 
+__global__ __launch_bounds__(XM_THREADS) void crossmul_looks_kernel(const XmArgs a) {
+  extern __shared__ float4 smem4[];
+  crossmul_tile(a, blockIdx.x, blockIdx.y, smem4);
+}
+
+// ------------------------------------------------------------ frame stages
+// Per pair, from the crop rows the geocoding stage voted: the two .gslc
+// headers (geo2rdr.cu:641-647), the overlap box aligned to the looks and the
+// interferogram header (crossmul_daemon.cu:612-666), and the multilooked size.
+__global__ void frame_box_kernel(const FrameDev d, s1b_frame_pair_t *pout) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= d.n_pairs) return;
+  const FramePair pr = d.pairs[k];
+  const s1b_burst_plan_t &p1 = d.plans[pr.ref], &p2 = d.plans[pr.sec];
+  s1b_frame_pair_t r;
+  r.ok = 0;
+  r.nrow_ml = r.ncol_ml = r.filtered = 0;
+  for (int q = 0; q < 6; ++q) r.header[q] = 0;
+  for (int q = 0; q < 4; ++q) r.box[q] = 0;
+  const int f1 = d.rows[2 * pr.ref], l1 = d.rows[2 * pr.ref + 1];
+  const int f2 = d.rows[2 * pr.sec], l2 = d.rows[2 * pr.sec + 1];
+  r.gslc_rows[0] = f1;
+  r.gslc_rows[1] = l1;
+  r.gslc_rows[2] = f2;
+  r.gslc_rows[3] = l2;
+  const bool rows_ok = f1 < d.bursts[pr.ref].nrow && l1 > f1 && f2 < d.bursts[pr.sec].nrow && l2 > f2;
+  if (rows_ok) {
+    // header words [nrow0, ncol0, left, top, right, bottom] of both .gslc
+    const int top1 = p1.win_top + f1, bot1 = p1.win_top + l1;
+    const int top2 = p2.win_top + f2, bot2 = p2.win_top + l2;
+    int left = max(p1.win_left, p2.win_left), right = min(p1.win_right, p2.win_right);
+    int top = max(top1, top2), bottom = min(bot1, bot2);
+    left = (left + d.collook - 1) / d.collook * d.collook;
+    right = right / d.collook * d.collook;
+    top = (top + d.rowlook - 1) / d.rowlook * d.rowlook;
+    bottom = bottom / d.rowlook * d.rowlook;
+    if (bottom - top > 0 && right - left > 0) {
+      r.ok = 1;
+      r.box[0] = left;
+      r.box[1] = top;
+      r.box[2] = right;
+      r.box[3] = bottom;
+      r.header[0] = p1.rsc_nlat / d.rowlook;
+      r.header[1] = p1.rsc_nlon / d.collook;
+      r.header[2] = left / d.collook;
+      r.header[3] = top / d.rowlook;
+      r.header[4] = right / d.collook;
+      r.header[5] = bottom / d.rowlook;
+      r.nrow_ml = min((bottom - top) / d.rowlook, pr.max_nrow_ml);
+      r.ncol_ml = min((right - left) / d.collook, pr.max_ncol_ml);
+      r.filtered = r.nrow_ml >= d.n_win && r.ncol_ml >= d.n_win;
+    }
+  }
+  pout[k] = r;
+}
+
+// Crossmul + looks of every pair: blockIdx.z = pair, x = multilooked row,
+// y = column chunk; CTAs outside a pair's box return at once.
+__global__ __launch_bounds__(XM_THREADS) void frame_crossmul_kernel(const FrameDev d, const FrameIO io,
+                                                                   int m_per_cta) {
+  extern __shared__ float4 smem4[];
+  const int k = blockIdx.z;
+  const s1b_frame_pair_t &r = io.pout[k];
+  if (!r.ok || (int)blockIdx.x >= r.nrow_ml || (int)blockIdx.y * m_per_cta >= r.ncol_ml) return;
+  const FramePair pr = d.pairs[k];
+  const s1b_burst_plan_t &p1 = d.plans[pr.ref], &p2 = d.plans[pr.sec];
+  const FrameBurst &b1 = d.bursts[pr.ref], &b2 = d.bursts[pr.sec];
+  XmArgs a;
+  a.ref = io.work + b1.geo_off;
+  a.sec = io.work + b2.geo_off;
+  a.ref_off = (int64_t)(r.box[1] - p1.win_top) * b1.ncol + (r.box[0] - p1.win_left);
+  a.sec_off = (int64_t)(r.box[1] - p2.win_top) * b2.ncol + (r.box[0] - p2.win_left);
+  a.ref_width = b1.ncol;
+  a.sec_width = b2.ncol;
+  a.nrow_ml = r.nrow_ml;
+  a.ncol_ml = r.ncol_ml;
+  a.rowlook = d.rowlook;
+  a.collook = d.collook;
+  a.m_per_cta = m_per_cta;
+  a.ifg = io.ifg + pr.ml_off;
+  a.amp1 = io.amp1 ? io.amp1 + pr.ml_off : nullptr;
+  a.amp2 = io.amp2 ? io.amp2 + pr.ml_off : nullptr;
+  a.coh = io.coh ? io.coh + pr.ml_off : nullptr;
+  a.phase = nullptr;
+  a.seed = d.fill_seed;
+  crossmul_tile(a, blockIdx.x, blockIdx.y, smem4);
+}
+
 }  // namespace
 
 extern "C" int s1b_crossmul_looks(const void *ref, int32_t ref_left, int32_t ref_top,
@@ -198,5 +286,26 @@ extern "C" int s1b_crossmul_looks(const void *ref, int32_t ref_left, int32_t ref
   if (nchunk > 65535) return s1b_fail(S1B_ERR_TOO_LARGE, "s1b_crossmul_looks: too many columns");
   dim3 grid(nrow_ml, nchunk);
   crossmul_looks_kernel<<<grid, XM_THREADS, smem, (cudaStream_t)stream>>>(a);
+  return s1b_launch_status();
+}
+
+int frame_launch_box(const FrameDev &d, const FrameIO &io, cudaStream_t st) {
+  frame_box_kernel<<<(d.n_pairs + 127) / 128, 128, 0, st>>>(d, io.pout);
+  return s1b_launch_status();
+}
+
+int frame_launch_crossmul(const FrameDev &d, const FrameIO &io, cudaStream_t st) {
+  if (d.collook > XM_MAX_COLLOOK) return s1b_fail(S1B_ERR_TOO_LARGE, "frame crossmul: collook above 4096");
+  if (d.max_nrow_ml <= 0 || d.max_ncol_ml <= 0) return S1B_OK;
+  const int m_per_cta = d.collook >= 512 ? 1 : 512 / d.collook;
+  const size_t smem = (size_t)m_per_cta * d.collook * 2 * sizeof(float2);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(frame_crossmul_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return s1b_fail(S1B_ERR_CUDA, cudaGetErrorString(e));
+  }
+  const int nchunk = (d.max_ncol_ml + m_per_cta - 1) / m_per_cta;
+  if (nchunk > 65535 || d.n_pairs > 65535) return s1b_fail(S1B_ERR_TOO_LARGE, "frame crossmul: grid too large");
+  dim3 grid(d.max_nrow_ml, nchunk, d.n_pairs);
+  frame_crossmul_kernel<<<grid, XM_THREADS, smem, st>>>(d, io, m_per_cta);
   return s1b_launch_status();
 }

@@ -16,6 +16,7 @@
 
 #include "s1b.h"
 #include "s1b_device.cuh"
+#include "s1b_frame.h"
 #include "s1b_internal.h"
 
 namespace {
@@ -24,18 +25,17 @@ constexpr double kRaD = 6378137.0;
 constexpr double kRe2D = 0.00669437999015;
 
 // ------------------------------------------------------------------ deramp
-// CTA: 256 threads x 2 columns = 512 columns, DERAMP_ROWS rows.  Per-column
-// TOPS coefficients are formed once per thread and reused down the rows.
+// Tile: 256 threads x 2 columns = 512 columns, ROWS rows.  Per-column TOPS
+// coefficients are formed once per thread and reused down the rows.
 constexpr int DERAMP_ROWS = 16;
 
-template <bool kVec>
-__global__ __launch_bounds__(256) void deramp_kernel(const __grid_constant__ s1b_burst_plan_t P,
-                                                     const float2 *__restrict__ in,
-                                                     float2 *__restrict__ out) {
+template <bool kVec, int ROWS>
+__device__ __forceinline__ void deramp_tile(const s1b_burst_plan_t &P, const float2 *__restrict__ in,
+                                            float2 *__restrict__ out, int tile_x, int tile_y) {
   const int S = P.samples, L = P.lines;
-  const int c0 = (blockIdx.x * 256 + threadIdx.x) * 2;
+  const int c0 = (tile_x * 256 + threadIdx.x) * 2;
   if (c0 >= S) return;
-  const int r0 = blockIdx.y * DERAMP_ROWS;
+  const int r0 = tile_y * ROWS;
   // geo2rdr.cu:533-541 for the thread's two columns: -pi*kt and etaref
   double mkt[2], etaref[2];
 #pragma unroll
@@ -53,7 +53,7 @@ __global__ __launch_bounds__(256) void deramp_kernel(const __grid_constant__ s1b
   const bool two = (c0 + 1) < S;
   const double eta0 = -L * P.ati / 2.;
 #pragma unroll 4
-  for (int rr = 0; rr < DERAMP_ROWS; ++rr) {
+  for (int rr = 0; rr < ROWS; ++rr) {
     const int r = r0 + rr;
     if (r >= L) break;
     const double eta = eta0 + r * P.ati;  // geo2rdr.cu:530-531
@@ -80,6 +80,13 @@ __global__ __launch_bounds__(256) void deramp_kernel(const __grid_constant__ s1b
   }
 }
 
+template <bool kVec>
+__global__ __launch_bounds__(256) void deramp_kernel(const __grid_constant__ s1b_burst_plan_t P,
+                                                     const float2 *__restrict__ in,
+                                                     float2 *__restrict__ out) {
+  deramp_tile<kVec, DERAMP_ROWS>(P, in, out, blockIdx.x, blockIdx.y);
+}
+
 // ----------------------------------------------------------------- geo2rdr
 // Tile: G_TX columns x G_RY rows of the DEM window, one thread per column
 // walking down the rows.  The zero-Doppler solution of the pixel above seeds
@@ -92,19 +99,20 @@ __global__ __launch_bounds__(256) void deramp_kernel(const __grid_constant__ s1b
 // longitude terms depend only on the column and stay in registers.  Warps
 // cover 32 consecutive columns of a row, so DEM reads and output writes
 // coalesce; the next row's DEM sample is loaded one row ahead.
-constexpr int G_TX = 128, G_RY = 16;
+constexpr int G_TX = 128, G_RY = 16;  // single-burst launch; the frame launch tunes the width
 
 __global__ void rows_init_kernel(int32_t *rows, int nrow) {
   rows[0] = nrow;
   rows[1] = -1;
 }
 
+template <int TX>
 __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const int16_t *__restrict__ dem,
                                              int64_t pitch, const float2 *__restrict__ burst,
                                              float2 *__restrict__ out, int32_t *__restrict__ rows, int nrow,
                                              int ncol, int tile_x, int tile_y) {
   const int tx = threadIdx.x, lane = tx & 31;
-  const int col = tile_x * G_TX + tx;
+  const int col = tile_x * TX + tx;
   const int row0 = tile_y * G_RY;
   // llh->ECEF trigonometry (orbit.cu:20-27): row terms on lanes 0..15
   double r_sin = 0.0, r_cos = 0.0, r_re = 0.0;
@@ -203,7 +211,100 @@ __global__ __launch_bounds__(G_TX) void geo2rdr_kernel(
     const __grid_constant__ s1b_burst_plan_t P, const int16_t *__restrict__ dem, int64_t pitch,
     const float2 *__restrict__ burst, float2 *__restrict__ out, int32_t *__restrict__ rows,
     int nrow, int ncol) {
-  geo2rdr_tile(P, dem, pitch, burst, out, rows, nrow, ncol, blockIdx.x, blockIdx.y);
+  geo2rdr_tile<G_TX>(P, dem, pitch, burst, out, rows, nrow, ncol, blockIdx.x, blockIdx.y);
+}
+
+// ------------------------------------------------------------ frame stages
+// Persistent kernels over the flat tile space of every burst of a frame.
+// Tiles are taken round-robin; the geocoding CTA copies the plan of the burst
+// it works on (orbit polynomials included) into shared memory when the burst
+// changes (consecutive tiles of a CTA usually stay in one burst).
+static_assert(G_RY == kFrameGeoRows, "geocoding tile rows");
+
+__global__ void frame_init_kernel(const FrameDev d, s1b_frame_pair_t *pout) {
+  for (int b = threadIdx.x; b < d.n_bursts; b += blockDim.x) {
+    d.rows[2 * b] = d.bursts[b].nrow;
+    d.rows[2 * b + 1] = -1;
+  }
+  for (int k = threadIdx.x; k < d.n_pairs; k += blockDim.x) pout[k].ok = 0;
+}
+
+// Burst owning flat tile `idx` (tile0 ascending); uniform over the CTA.
+template <bool kGeo>
+__device__ __forceinline__ int frame_burst_of(const FrameDev &d, int64_t idx) {
+  int lo = 0, hi = d.n_bursts - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    const int64_t s = kGeo ? d.bursts[mid].geo_tile0 : d.bursts[mid].deramp_tile0;
+    if (s <= idx) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// The plan table is an array of 8-byte-aligned structs whose size is a
+// multiple of 8 but not of 16: copy in 8-byte words.
+static_assert(sizeof(s1b_burst_plan_t) % 8 == 0 && alignof(s1b_burst_plan_t) == 8, "plan layout");
+
+__device__ __forceinline__ void frame_load_plan(s1b_burst_plan_t &sp, const s1b_burst_plan_t *src) {
+  __syncthreads();  // every thread is done with the previous burst's plan
+  const long long *s = reinterpret_cast<const long long *>(src);
+  long long *d = reinterpret_cast<long long *>(&sp);
+  for (int i = threadIdx.x; i < (int)(sizeof(s1b_burst_plan_t) / 8); i += blockDim.x) d[i] = s[i];
+  __syncthreads();
+}
+
+// Deramp reads a dozen plan fields once per tile (uniform loads), so it
+// takes the plan from the table directly.
+template <int ROWS>
+__global__ __launch_bounds__(256, 4) void frame_deramp_kernel(const FrameDev d, const FrameIO io) {
+  for (int64_t idx = blockIdx.x; idx < d.n_deramp_tiles; idx += gridDim.x) {
+    const int b = frame_burst_of<false>(d, idx);
+    const s1b_burst_plan_t &sp = d.plans[b];
+    const FrameBurst &fb = d.bursts[b];
+    const int tiles_x = (sp.samples + kFrameDerampCols - 1) / kFrameDerampCols;
+    const int64_t local = idx - fb.deramp_tile0;
+    const int ty = (int)(local / tiles_x), tx = (int)(local - (int64_t)ty * tiles_x);
+    const float2 *in = io.slc + fb.slc_off;
+    float2 *out = io.work + fb.der_off;
+    const bool vec = sp.samples % 2 == 0 && (reinterpret_cast<uintptr_t>(in) % 16) == 0 &&
+                     (reinterpret_cast<uintptr_t>(out) % 16) == 0;
+    if (vec)
+      deramp_tile<true, ROWS>(sp, in, out, tx, ty);
+    else
+      deramp_tile<false, ROWS>(sp, in, out, tx, ty);
+  }
+}
+
+template <int TX>
+__global__ __launch_bounds__(TX) void frame_geo2rdr_kernel(const FrameDev d, const FrameIO io) {
+  __shared__ __align__(16) s1b_burst_plan_t sp;
+  int cur = -1;
+  for (int64_t idx = blockIdx.x; idx < d.n_geo_tiles; idx += gridDim.x) {
+    const int b = frame_burst_of<true>(d, idx);
+    if (b != cur) {
+      frame_load_plan(sp, d.plans + b);
+      cur = b;
+    }
+    const FrameBurst &fb = d.bursts[b];
+    const int tiles_x = (fb.ncol + TX - 1) / TX;
+    const int64_t local = idx - fb.geo_tile0;
+    const int ty = (int)(local / tiles_x), tx = (int)(local - (int64_t)ty * tiles_x);
+    const int16_t *dem = io.dem + (int64_t)sp.win_top * io.dem_pitch + sp.win_left;
+    geo2rdr_tile<TX>(sp, dem, io.dem_pitch, io.work + fb.der_off, io.work + fb.geo_off, d.rows + 2 * b,
+                     fb.nrow, fb.ncol, tx, ty);
+  }
+}
+
+template <typename K>
+int resident_ctas(K kernel, int threads) {
+  int dev = 0, sms = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return sms * per_sm;
 }
 
 // ------------------------------------------------- generic geometry kernels
@@ -287,5 +388,57 @@ extern "C" int s1b_llh2xyz(const double *llh, double *xyz, int64_t n, void *stre
   if (n > 0 && (!llh || !xyz)) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_llh2xyz: null argument");
   if (n <= 0) return S1B_OK;
   llh2xyz_kernel<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(llh, xyz, n);
+  return s1b_launch_status();
+}
+
+// ------------------------------------------------------------ frame launchers
+int frame_launch_init(const FrameDev &d, const FrameIO &io, cudaStream_t st) {
+  frame_init_kernel<<<1, 256, 0, st>>>(d, io.pout);
+  return s1b_launch_status();
+}
+
+int frame_max_ctas_deramp(int rows) {
+  switch (rows) {
+    case 8: return resident_ctas(frame_deramp_kernel<8>, 256);
+    case 16: return resident_ctas(frame_deramp_kernel<16>, 256);
+    case 32: return resident_ctas(frame_deramp_kernel<32>, 256);
+    default: return 0;
+  }
+}
+
+int frame_max_ctas_geo2rdr(int cols) {
+  switch (cols) {
+    case 64: return resident_ctas(frame_geo2rdr_kernel<64>, 64);
+    case 128: return resident_ctas(frame_geo2rdr_kernel<128>, 128);
+    case 256: return resident_ctas(frame_geo2rdr_kernel<256>, 256);
+    default: return 0;
+  }
+}
+
+int frame_launch_deramp(const FrameDev &d, const FrameIO &io, int rows, int ctas, cudaStream_t st) {
+  const int full = frame_max_ctas_deramp(rows);
+  if (full <= 0) return s1b_fail(S1B_ERR_UNSUPPORTED, "frame deramp: tile rows must be 8, 16 or 32");
+  if (d.n_deramp_tiles == 0) return S1B_OK;
+  long long g = ctas > 0 && ctas < full ? ctas : full;
+  if (g > d.n_deramp_tiles) g = d.n_deramp_tiles;
+  switch (rows) {
+    case 8: frame_deramp_kernel<8><<<(unsigned)g, 256, 0, st>>>(d, io); break;
+    case 16: frame_deramp_kernel<16><<<(unsigned)g, 256, 0, st>>>(d, io); break;
+    default: frame_deramp_kernel<32><<<(unsigned)g, 256, 0, st>>>(d, io); break;
+  }
+  return s1b_launch_status();
+}
+
+int frame_launch_geo2rdr(const FrameDev &d, const FrameIO &io, int cols, int ctas, cudaStream_t st) {
+  const int full = frame_max_ctas_geo2rdr(cols);
+  if (full <= 0) return s1b_fail(S1B_ERR_UNSUPPORTED, "frame geo2rdr: tile columns must be 64, 128 or 256");
+  if (d.n_geo_tiles == 0) return S1B_OK;
+  long long g = ctas > 0 && ctas < full ? ctas : full;
+  if (g > d.n_geo_tiles) g = d.n_geo_tiles;
+  switch (cols) {
+    case 64: frame_geo2rdr_kernel<64><<<(unsigned)g, 64, 0, st>>>(d, io); break;
+    case 128: frame_geo2rdr_kernel<128><<<(unsigned)g, 128, 0, st>>>(d, io); break;
+    default: frame_geo2rdr_kernel<256><<<(unsigned)g, 256, 0, st>>>(d, io); break;
+  }
   return s1b_launch_status();
 }

@@ -19,6 +19,7 @@
 
 #include "s1b.h"
 #include "s1b_device.cuh"
+#include "s1b_frame.h"
 #include "s1b_internal.h"
 
 namespace {
@@ -106,19 +107,15 @@ __device__ __forceinline__ int patch_origin(int p, int n) {  // goldstein.cu:308
   return o + GN > n ? n - GN : o;
 }
 
-__global__ __launch_bounds__(32 * GWARPS) void goldstein_patch_kernel(
-    const float2 *__restrict__ in, float2 *__restrict__ patches, int nrow, int ncol, int n_win_i,
-    int n_win_j, float alpha) {
-  // one padded 32x33 tile per warp; |F| reuses it once the column FFT
-  // inputs have been read into registers
-  __shared__ float2 sT[GWARPS][GN][GN + 1];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int p = blockIdx.x * GWARPS + warp;
-  if (p >= n_win_i * n_win_j) return;  // warp-uniform; only __syncwarp below
+// Patch p of an nrow x ncol image, by one warp with its padded 32x33 tile
+// T; |F| reuses the tile once the column FFT inputs are in registers.
+__device__ __forceinline__ void goldstein_patch(const float2 *__restrict__ in, float2 *__restrict__ patches,
+                                                int nrow, int ncol, int n_win_j, float alpha, int p,
+                                                float2 (*T)[GN + 1]) {
+  const int lane = threadIdx.x & 31;
   const int i1 = patch_origin(p / n_win_j, nrow);
   const int j1 = patch_origin(p % n_win_j, ncol);
-  float2(*T)[GN + 1] = sT[warp];
-  float(*M)[GN + 1] = reinterpret_cast<float(*)[GN + 1]>(&sT[warp][0][0]);
+  float(*M)[GN + 1] = reinterpret_cast<float(*)[GN + 1]>(&T[0][0]);
 #pragma unroll 8
   for (int r = 0; r < GN; ++r) T[r][lane] = __ldg(in + (size_t)(i1 + r) * ncol + j1 + lane);
   __syncwarp();
@@ -193,12 +190,19 @@ __global__ __launch_bounds__(32 * GWARPS) void goldstein_patch_kernel(
   for (int r = 0; r < GN; ++r) __stcg(dst + r * GN + lane, T[r][lane]);
 }
 
-__global__ __launch_bounds__(256) void goldstein_gather_kernel(const float2 *__restrict__ patches,
-                                                               float2 *__restrict__ out, int nrow,
-                                                               int ncol, int n_win_i, int n_win_j) {
-  const int y = blockIdx.x;
-  const int x = blockIdx.y * 256 + threadIdx.x;
-  if (x >= ncol) return;
+__global__ __launch_bounds__(32 * GWARPS) void goldstein_patch_kernel(
+    const float2 *__restrict__ in, float2 *__restrict__ patches, int nrow, int ncol, int n_win_i,
+    int n_win_j, float alpha) {
+  __shared__ float2 sT[GWARPS][GN][GN + 1];
+  const int warp = threadIdx.x >> 5;
+  const int p = blockIdx.x * GWARPS + warp;
+  if (p >= n_win_i * n_win_j) return;  // warp-uniform; only __syncwarp below
+  goldstein_patch(in, patches, nrow, ncol, n_win_j, alpha, p, sT[warp]);
+}
+
+// Output pixel (y, x): fixed-order overlap-add of its covering patches.
+__device__ __forceinline__ void goldstein_gather(const float2 *__restrict__ patches, float2 *__restrict__ out,
+                                                 int nrow, int ncol, int n_win_i, int n_win_j, int y, int x) {
   float ax = 0.f, ay = 0.f, wsum = 0.f;
   const int pi0 = y >= GN - 1 ? (y - (GN - 1) + GSTEP - 1) / GSTEP : 0;
   const int pj0 = x >= GN - 1 ? (x - (GN - 1) + GSTEP - 1) / GSTEP : 0;
@@ -226,11 +230,53 @@ __global__ __launch_bounds__(256) void goldstein_gather_kernel(const float2 *__r
   out[(size_t)y * ncol + x] = make_float2(ax, ay);
 }
 
-void patch_grid(int nrow, int ncol, int &n_win_i, int &n_win_j) {  // goldstein.cu:335-340
+__global__ __launch_bounds__(256) void goldstein_gather_kernel(const float2 *__restrict__ patches,
+                                                               float2 *__restrict__ out, int nrow,
+                                                               int ncol, int n_win_i, int n_win_j) {
+  const int x = blockIdx.y * 256 + threadIdx.x;
+  if (x >= ncol) return;
+  goldstein_gather(patches, out, nrow, ncol, n_win_i, n_win_j, blockIdx.x, x);
+}
+
+__host__ __device__ inline void patch_grid(int nrow, int ncol, int &n_win_i, int &n_win_j) {  // goldstein.cu:335-340
   n_win_i = (int)ceilf((float)nrow / GSTEP) - 3;
   n_win_j = (int)ceilf((float)ncol / GSTEP) - 3;
   if (n_win_i <= 0) n_win_i = 1;
   if (n_win_j <= 0) n_win_j = 1;
+}
+
+
+// ------------------------------------------------------------ frame stages
+// Goldstein of every pair's interferogram: blockIdx.y = pair.  Pairs too
+// small to filter get filt = ifg from the gather kernel.
+__global__ __launch_bounds__(32 * GWARPS) void frame_goldstein_patch_kernel(const FrameDev d, const FrameIO io) {
+  __shared__ float2 sT[GWARPS][GN][GN + 1];
+  const int k = blockIdx.y;
+  const s1b_frame_pair_t &r = io.pout[k];
+  if (!r.ok || !r.filtered) return;
+  int ni, nj;
+  patch_grid(r.nrow_ml, r.ncol_ml, ni, nj);
+  const int warp = threadIdx.x >> 5;
+  const int p = blockIdx.x * GWARPS + warp;
+  if (p >= ni * nj) return;  // warp-uniform
+  const FramePair &pr = d.pairs[k];
+  goldstein_patch(io.ifg + pr.ml_off, io.work + pr.scratch_off, r.nrow_ml, r.ncol_ml, nj, d.alpha, p, sT[warp]);
+}
+
+__global__ __launch_bounds__(256) void frame_goldstein_gather_kernel(const FrameDev d, const FrameIO io) {
+  const int k = blockIdx.z;
+  const s1b_frame_pair_t &r = io.pout[k];
+  const int y = blockIdx.x, x = blockIdx.y * 256 + threadIdx.x;
+  if (!r.ok || y >= r.nrow_ml || x >= r.ncol_ml) return;
+  const FramePair &pr = d.pairs[k];
+  if (r.filtered) {
+    int ni, nj;
+    patch_grid(r.nrow_ml, r.ncol_ml, ni, nj);
+    goldstein_gather(io.work + pr.scratch_off, io.filt + pr.ml_off, r.nrow_ml, r.ncol_ml, ni, nj, y, x);
+  } else {
+    const size_t o = pr.ml_off + (size_t)y * r.ncol_ml + x;
+    io.filt[o] = io.ifg[o];
+  }
 }
 
 }  // namespace
@@ -333,5 +379,26 @@ extern "C" int s1b_goldstein_noalloc(const void *in, void *out, int32_t nrow, in
   if (s) return s;
   dim3 grid(nrow, (ncol + 255) / 256);
   goldstein_gather_kernel<<<grid, 256, 0, st>>>((const float2 *)scratch, (float2 *)out, nrow, ncol, ni, nj);
+  return s1b_launch_status();
+}
+
+int frame_goldstein_patch_grid(int nrow, int ncol, int *ni, int *nj) {
+  patch_grid(nrow, ncol, *ni, *nj);
+  return S1B_OK;
+}
+
+int frame_launch_goldstein(const FrameDev &d, const FrameIO &io, cudaStream_t st) {
+  if (d.max_nrow_ml <= 0 || d.max_ncol_ml <= 0) return S1B_OK;
+  if (d.n_win != GN) return s1b_fail(S1B_ERR_UNSUPPORTED, "frame goldstein: only n_win = 32 is implemented");
+  if (d.n_pairs > 65535 || (d.max_ncol_ml + 255) / 256 > 65535)
+    return s1b_fail(S1B_ERR_TOO_LARGE, "frame goldstein: grid too large");
+  if (d.max_patches > 0) {
+    dim3 g1((d.max_patches + GWARPS - 1) / GWARPS, d.n_pairs);
+    frame_goldstein_patch_kernel<<<g1, 32 * GWARPS, 0, st>>>(d, io);
+    int s = s1b_launch_status();
+    if (s) return s;
+  }
+  dim3 g2(d.max_nrow_ml, (d.max_ncol_ml + 255) / 256, d.n_pairs);
+  frame_goldstein_gather_kernel<<<g2, 256, 0, st>>>(d, io);
   return s1b_launch_status();
 }

@@ -40,3 +40,14 @@ def test_struct_layout_and_host_calls():
     # a device call without a GPU (or with bad args) reports a status, never exits
     st = lib.s1b_deramp(None, None, None, None)
     assert st == _lib.S1B_ERR_INVALID_ARGUMENT
+
+
+def test_frame_structs_and_argument_checks():
+    assert ctypes.sizeof(_lib.FramePair) == 72
+    assert ctypes.sizeof(_lib.FrameSizes) == 32
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    st = lib.s1b_frame_create(None, 0, None, None, 0, 1, 1, 32, 0.5, 0, ctypes.byref(h))
+    assert st == _lib.S1B_ERR_INVALID_ARGUMENT and not h.value
+    assert lib.s1b_frame_sizes(None, None) == _lib.S1B_ERR_INVALID_ARGUMENT
+    lib.s1b_frame_destroy(None)  # accepts NULL
