@@ -249,6 +249,18 @@ int s1b_geo2rdr_offsets(const s1b_burst_plan_t *plan, const double *lat, const d
                         const double *hgt, int32_t lines, int32_t samples, float *az_off,
                         float *rg_off, void *stream);
 
+/* s1b_geo2rdr_offsets plus the offsets' height sensitivities daz_dh, drg_dh
+ * (samples per metre, float32 [lines * samples]).  A height error moves the
+ * ground point of a reference pixel along the reference's zero-Doppler
+ * iso-range circle (dp = (rhat_r x V_r) / (up . (rhat_r x V_r)), the
+ * reference pixel being the reference sample (row, col) of ref_plan); the
+ * secondary's zero-Doppler time moves by (V.dp) / (|V|^2 - dr.A) and its
+ * range by rhat.(dp - V dt/dh).  Carries a DEM-error field into the offsets. */
+int s1b_geo2rdr_offsets_dh(const s1b_burst_plan_t *plan, const s1b_burst_plan_t *ref_plan,
+                           const double *lat, const double *lon, const double *hgt, int32_t lines,
+                           int32_t samples, float *az_off, float *rg_off, float *daz_dh, float *drg_dh,
+                           void *stream);
+
 /* Resample the secondary burst of `plan` (complex64 [plan->lines *
  * plan->samples], as acquired, TOPS-modulated) onto the reference grid:
  * deramp (geo2rdr.cu:138-158), interpolate at (row + az_off, col + rg_off)
@@ -386,6 +398,40 @@ int s1b_frame_profile(s1b_frame_t *frame, const void *slc, const int16_t *dem, i
 int s1b_frame_tuning(const s1b_frame_t *frame, int32_t tuning[4]);
 /* Set the tuning by hand (validated; S1B_ERR_UNSUPPORTED for a shape not built). */
 int s1b_frame_set_tuning(s1b_frame_t *frame, const int32_t tuning[4]);
+
+/* ------------------------------------------- coregistration refinement
+ * Coherence objective of radar-grid coregistration and its hand-written
+ * adjoint (no reference counterpart).  For n_bursts reference/secondary
+ * bursts of one size [lines x samples] (stacked back to back):
+ *   az = row + az0 + p0 + p1 xa + p2 xr + daz_dh dh,
+ *   rg = col + rg0 + p3 + p4 xa + p5 xr + drg_dh dh,
+ *   xa = (row - lines/2) / lines, xr = (col - samples/2) / samples;
+ * the secondary is resampled there (8-tap windowed sinc with TOPS deramp /
+ * reramp, as s1b_resample) and crossed with the reference; over the rowlook x
+ * collook windows of the multilook grid gamma = |sum conj(r) s| /
+ * sqrt(sum |r|^2 sum |s|^2); the objective is J = -mean gamma over every
+ * window of every burst.  params: float32 [n_bursts x 6] (p0..p5, samples);
+ * dh: float32 height error [n_bursts x lines x samples] (metres);
+ * daz_dh/drg_dh from s1b_geo2rdr_offsets_dh. */
+
+typedef struct s1b_adjoint s1b_adjoint_t;
+
+/* Host only.  sec_plans: the secondary burst plans (one size); rowlook must
+ * divide 16, collook <= 64. */
+int s1b_adjoint_create(const s1b_burst_plan_t *sec_plans, int32_t n_bursts, int32_t lines, int32_t samples,
+                       int32_t rowlook, int32_t collook, s1b_adjoint_t **adjoint);
+void s1b_adjoint_destroy(s1b_adjoint_t *adjoint);
+/* Device workspace bytes of s1b_adjoint_run (per-tile partial sums). */
+size_t s1b_adjoint_workspace_bytes(const s1b_adjoint_t *adjoint);
+
+/* J into objective (double, device).  With grad_params (float32 [n_bursts x
+ * 6]) and grad_dh (float32 like dh) also dJ/dparams and dJ/ddh, from one
+ * fused pass that recomputes the window sums.  Deterministic (fixed
+ * reduction order).  No host synchronisation. */
+int s1b_adjoint_run(s1b_adjoint_t *adjoint, const void *ref, const void *sec, const float *az0,
+                    const float *rg0, const float *daz_dh, const float *drg_dh, const float *params,
+                    const float *dh, double *objective, float *grad_params, float *grad_dh, void *workspace,
+                    size_t workspace_bytes, void *stream);
 
 #ifdef __cplusplus
 }

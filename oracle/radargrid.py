@@ -80,9 +80,10 @@ def tops_phase(radar, co: BurstCoeffs, az, rg):
     return -PI * kt * d * d
 
 
-def resample(sec, radar, co: BurstCoeffs, az, rg, interp="sinc8"):
+def resample(sec, radar, co: BurstCoeffs, az, rg, interp="sinc8", exact=False):
     """Deramp, interpolate at (az, rg), reramp; zero where the kernel leaves
-    the burst.  sec: complex64 [L, S] as acquired (TOPS-modulated)."""
+    the burst.  sec: complex64 [L, S] as acquired (TOPS-modulated).  Returns
+    complex64, or complex128 with ``exact``."""
     L, S = sec.shape
     rows = np.arange(L, dtype=np.float64)[:, None]
     cols = np.arange(S, dtype=np.float64)[None, :]
@@ -112,7 +113,7 @@ def resample(sec, radar, co: BurstCoeffs, az, rg, interp="sinc8"):
         out[ok] = c1 * (1 - a) + c2 * a
     out *= np.exp(-1j * tops_phase(radar, co, az, rg))
     out[~ok] = 0
-    return out.astype(np.complex64), ok
+    return (out if exact else out.astype(np.complex64)), ok
 
 
 def box_coherence(ref, sec, win=5):

@@ -130,6 +130,8 @@ _SIGNATURES = {
                                  POINTER(c_int32), POINTER(c_int32)]),
     "s1b_geo2rdr_offsets": (c_int, [POINTER(BurstPlan), c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p,
                                     c_void_p, c_void_p]),
+    "s1b_geo2rdr_offsets_dh": (c_int, [POINTER(BurstPlan), POINTER(BurstPlan), c_void_p, c_void_p, c_void_p,
+                                       c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "s1b_resample": (c_int, [POINTER(BurstPlan), c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p,
                              c_void_p, c_void_p]),
     "s1b_box_coherence": (c_int, [c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p, c_void_p, c_void_p]),
@@ -150,6 +152,12 @@ _SIGNATURES = {
     "s1b_frame_profile": (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p,
                                   c_void_p, c_void_p, c_void_p, POINTER(c_float), c_void_p]),
     "s1b_frame_tuning": (c_int, [c_void_p, POINTER(c_int32)]),
+    "s1b_adjoint_create": (c_int, [POINTER(BurstPlan), c_int32, c_int32, c_int32, c_int32, c_int32,
+                                   POINTER(c_void_p)]),
+    "s1b_adjoint_destroy": (None, [c_void_p]),
+    "s1b_adjoint_workspace_bytes": (c_size_t, [c_void_p]),
+    "s1b_adjoint_run": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
     "s1b_frame_set_tuning": (c_int, [c_void_p, POINTER(c_int32)]),
 }
 

@@ -31,7 +31,8 @@ constexpr double kRe2D = 0.00669437999015;
 // burst centre, the others on the cubic expansion there (OrbitCubic).
 constexpr int O_TX = 128, O_RY = 16;
 
-__device__ __forceinline__ void llh_ecef(double lat_deg, double lon_deg, double h, double p[3]) {
+// ECEF position of a geodetic point and the geodetic up vector dp/dh.
+__device__ __forceinline__ void llh_ecef(double lat_deg, double lon_deg, double h, double p[3], double up[3]) {
   double sl, cl, so, co;
   sincospi(lat_deg * (1.0 / 180.0), &sl, &cl);
   sincospi(lon_deg * (1.0 / 180.0), &so, &co);
@@ -39,14 +40,58 @@ __device__ __forceinline__ void llh_ecef(double lat_deg, double lon_deg, double 
   p[0] = (re + h) * cl * co;
   p[1] = (re + h) * cl * so;
   p[2] = (re * (1 - kRe2D) + h) * sl;
+  up[0] = cl * co;
+  up[1] = cl * so;
+  up[2] = sl;
 }
 
+// Height sensitivity of the secondary offsets of a reference-grid pixel.  A
+// height error moves the ground point along the reference's zero-Doppler
+// iso-range circle: dp = (rhat_r x V_r) / (up . (rhat_r x V_r)) per metre
+// (range to and Doppler of the reference unchanged, geodetic height +1).
+// The secondary then sees f(t, p) = (p - X(t)).V(t) = 0 move by dt/dh =
+// (V.dp) / (|V|^2 - dr.A) and its range by rhat.(dp - V dt/dh).
+__device__ __forceinline__ void height_sensitivity(const OrbitCubic &o, double t, const double dr[3],
+                                                   const double up[3], const double rr[3], const double vr[3],
+                                                   double &dt_dh, double &dR_dh) {
+  // c = dr_ref x V_ref (the unit of dr_ref cancels in the ratio)
+  const double c0 = rr[1] * vr[2] - rr[2] * vr[1];
+  const double c1 = rr[2] * vr[0] - rr[0] * vr[2];
+  const double c2 = rr[0] * vr[1] - rr[1] * vr[0];
+  const double inv = 1.0 / (up[0] * c0 + up[1] * c1 + up[2] * c2);
+  const double dp[3] = {c0 * inv, c1 * inv, c2 * inv};
+  const double h = t - o.t0;
+  double v[3], a[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    a[i] = fma(o.j[i], h, o.a[i]);
+    v[i] = fma(fma(0.5 * o.j[i], h, o.a[i]), h, o.v[i]);
+  }
+  const double vn = v[0] * dp[0] + v[1] * dp[1] + v[2] * dp[2];
+  const double den = (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) - (dr[0] * a[0] + dr[1] * a[1] + dr[2] * a[2]);
+  dt_dh = vn / den;
+  const double inv_r = rsqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+  dR_dh = inv_r * (dr[0] * (dp[0] - v[0] * dt_dh) + dr[1] * (dp[1] - v[1] * dt_dh) + dr[2] * (dp[2] - v[2] * dt_dh));
+}
+
+// Reference satellite state for the sensitivities: the reference pixel
+// (row, col) is the reference's own sample, so its zero-Doppler time is
+// tstart + row dtaz and no Newton is needed.
+struct RefOrbit {
+  s1b_orbit_poly_t orbit;
+  double tstart, dtaz;
+};
+
+template <bool kSens>
 __global__ __launch_bounds__(O_TX) void offsets_kernel(const __grid_constant__ s1b_burst_plan_t P,
+                                                       const __grid_constant__ RefOrbit R,
                                                        const double *__restrict__ lat,
                                                        const double *__restrict__ lon,
                                                        const double *__restrict__ hgt, int L, int S,
                                                        float *__restrict__ az_off,
-                                                       float *__restrict__ rg_off) {
+                                                       float *__restrict__ rg_off,
+                                                       float *__restrict__ daz_dh,
+                                                       float *__restrict__ drg_dh) {
   const int col = blockIdx.x * O_TX + threadIdx.x;
   const int row0 = blockIdx.y * O_RY;
   if (col >= S) return;
@@ -54,7 +99,7 @@ __global__ __launch_bounds__(O_TX) void offsets_kernel(const __grid_constant__ s
   const int rmax = min(O_RY, L - row0);
   size_t i = (size_t)row0 * S + col;
   double la = __ldcs(lat + i), lo = __ldcs(lon + i), h = __ldcs(hgt + i);
-  double p[3], dr[3];
+  double p[3], dr[3], up[3];
   // first row: from the burst centre on the window polynomial
   double t = P.tmid;
   {
@@ -65,7 +110,7 @@ __global__ __launch_bounds__(O_TX) void offsets_kernel(const __grid_constant__ s
       st.v[k] = P.vmid[k];
       st.a[k] = P.amid[k];
     }
-    llh_ecef(la, lo, h, p);
+    llh_ecef(la, lo, h, p, up);
     zero_doppler(P.orbit, p, t, st, dr);
   }
   OrbitCubic o;
@@ -82,9 +127,18 @@ __global__ __launch_bounds__(O_TX) void offsets_kernel(const __grid_constant__ s
     // residuals relative to the pixel index keep float32 at ~1e-5 px
     __stcs(az_off + i, (float)((t - P.tstart) * prf - (row0 + r)));
     __stcs(rg_off + i, (float)((rng - P.rngstart) * inv_dmrg - col));
+    if (kSens) {
+      OrbitState rs;
+      orbit_eval(R.orbit, R.tstart + (row0 + r) * R.dtaz, rs);
+      const double rr[3] = {p[0] - rs.x[0], p[1] - rs.x[1], p[2] - rs.x[2]};
+      double dt_dh, dR_dh;
+      height_sensitivity(o, t, dr, up, rr, rs.v, dt_dh, dR_dh);
+      __stcs(daz_dh + i, (float)(dt_dh * prf));
+      __stcs(drg_dh + i, (float)(dR_dh * inv_dmrg));
+    }
     if (++r >= rmax) break;
     i += S;
-    llh_ecef(la, lo, h, p);
+    llh_ecef(la, lo, h, p, up);
     if (r + 1 < rmax) {
       la = __ldcs(lat + i + S);
       lo = __ldcs(lon + i + S);
@@ -1040,7 +1094,26 @@ extern "C" int s1b_geo2rdr_offsets(const s1b_burst_plan_t *plan, const double *l
   if (lines < 1 || samples < 1) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_geo2rdr_offsets: empty grid");
   dim3 grid((samples + O_TX - 1) / O_TX, (lines + O_RY - 1) / O_RY);
   if (grid.y > 65535) return s1b_fail(S1B_ERR_TOO_LARGE, "s1b_geo2rdr_offsets: grid too tall");
-  offsets_kernel<<<grid, O_TX, 0, (cudaStream_t)stream>>>(*plan, lat, lon, hgt, lines, samples, az_off, rg_off);
+  offsets_kernel<false><<<grid, O_TX, 0, (cudaStream_t)stream>>>(*plan, RefOrbit{}, lat, lon, hgt, lines, samples,
+                                                                 az_off, rg_off, nullptr, nullptr);
+  return s1b_launch_status();
+}
+
+extern "C" int s1b_geo2rdr_offsets_dh(const s1b_burst_plan_t *plan, const s1b_burst_plan_t *ref_plan,
+                                      const double *lat, const double *lon, const double *hgt, int32_t lines,
+                                      int32_t samples, float *az_off, float *rg_off, float *daz_dh, float *drg_dh,
+                                      void *stream) {
+  if (!plan || !ref_plan || !lat || !lon || !hgt || !az_off || !rg_off || !daz_dh || !drg_dh)
+    return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_geo2rdr_offsets_dh: null argument");
+  if (lines < 1 || samples < 1) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_geo2rdr_offsets_dh: empty grid");
+  dim3 grid((samples + O_TX - 1) / O_TX, (lines + O_RY - 1) / O_RY);
+  if (grid.y > 65535) return s1b_fail(S1B_ERR_TOO_LARGE, "s1b_geo2rdr_offsets_dh: grid too tall");
+  RefOrbit ro;
+  ro.orbit = ref_plan->orbit;
+  ro.tstart = ref_plan->tstart;
+  ro.dtaz = ref_plan->dtaz;
+  offsets_kernel<true><<<grid, O_TX, 0, (cudaStream_t)stream>>>(*plan, ro, lat, lon, hgt, lines, samples, az_off,
+                                                                rg_off, daz_dh, drg_dh);
   return s1b_launch_status();
 }
 

@@ -176,6 +176,25 @@ def geo2rdr_offsets(plan: _lib.BurstPlan, lat: torch.Tensor, lon: torch.Tensor, 
     return az_off, rg_off
 
 
+def geo2rdr_offsets_dh(plan: _lib.BurstPlan, ref_plan: _lib.BurstPlan, lat: torch.Tensor, lon: torch.Tensor,
+                       hgt: torch.Tensor):
+    """Offsets as :func:`geo2rdr_offsets` plus their sensitivities to a
+    height error of the reference-grid pixels (the point moving along the
+    reference's iso-range zero-Doppler circle): returns (az_off, rg_off,
+    daz_dh, drg_dh), float32 [L, S] (samples per metre)."""
+    _need_cuda(lat, lon, hgt)
+    for t in (lat, lon, hgt):
+        if t.dtype != torch.float64 or not t.is_contiguous() or t.shape != lat.shape:
+            raise ValueError("lat/lon/hgt must be contiguous float64 rasters of one shape")
+    L, S = lat.shape
+    outs = [torch.empty((L, S), dtype=torch.float32, device=lat.device) for _ in range(4)]
+    _lib.check(_call("geo2rdr_offsets", _lib.load().s1b_geo2rdr_offsets_dh, ctypes.byref(plan),
+                     ctypes.byref(ref_plan), _lib.dptr(lat),
+                     _lib.dptr(lon), _lib.dptr(hgt), L, S, *[_lib.dptr(o) for o in outs], _lib.stream_ptr()),
+               "s1b_geo2rdr_offsets_dh")
+    return tuple(outs)
+
+
 def resample(plan: _lib.BurstPlan, sec: torch.Tensor, az_off: torch.Tensor, rg_off: torch.Tensor,
              interp: str = "sinc8", out: torch.Tensor | None = None,
              status: torch.Tensor | None = None) -> torch.Tensor:

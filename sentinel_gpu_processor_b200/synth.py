@@ -646,3 +646,110 @@ def make_radar_pair(config="c1", seed=20261203, device="cpu", baseline=150.0, co
     sec_slc = tops_modulate(s_sec.to(torch.complex64), sec, burst).contiguous()
     return RadarPairScene(name=config, seed=seed, ref=ref, sec=sec, lat=lat, lon=lon, hgt=hgt, ref_slc=ref_slc,
                           sec_slc=sec_slc, rowlook=rl, collook=cl, alpha=al, extra={"hmax": hmax})
+
+
+@dataclass
+class RefineStack:
+    """Bursts for coherence-maximising coregistration refinement: one radar
+    grid geometry shared by every burst, independent speckle, true offset
+    polynomials and height errors per burst."""
+    sec_plans: list
+    ref: object      # complex64 [n, L, S]
+    sec: object      # complex64 [n, lines, samples] (secondary bursts)
+    az0: object      # float32 [n, L, S] geometric offsets (from the heights in the rasters)
+    rg0: object
+    daz_dh: object   # float32 [n, L, S]
+    drg_dh: object
+    params_true: object  # float32 [n, 6]
+    dh_true: object      # float32 [n, L, S]
+    rowlook: int
+    collook: int
+    coherence: float
+    sec_acq: object = None   # the secondary Acquisition (radar, orbit, TOPS tables)
+    ref_acq: object = None   # the reference Acquisition
+    geometry: object = None  # (lat, lon, hgt) float64 rasters of the burst, kept when asked for
+    margin: int = 0          # reference grid = burst minus this many pixels on every side
+
+
+def gaussian_smooth(x, sigma):
+    """Separable Gaussian smoothing of [n, L, S] float32 (torch, edge padding)."""
+    import torch
+    r = int(3 * sigma)
+    t = torch.arange(-r, r + 1, dtype=torch.float32, device=x.device)
+    k = torch.exp(-0.5 * (t / sigma) ** 2)
+    k = k / k.sum()
+    y = x[:, None]
+    y = torch.nn.functional.pad(y, (r, r, 0, 0), mode="replicate")
+    y = torch.nn.functional.conv2d(y, k.view(1, 1, 1, -1))
+    y = torch.nn.functional.pad(y, (0, 0, r, r), mode="replicate")
+    y = torch.nn.functional.conv2d(y, k.view(1, 1, -1, 1))
+    return y[:, 0]
+
+
+def make_refine_stack(n_bursts=8, config="c1", seed=20261203 + 3000, device="cuda", param_sigma=0.05,
+                      dh_sigma=10.0, dh_smooth=31.0, coherence=0.7, lines=None, samples=None, keep_geometry=False,
+                      margin=0):
+    """Refinement stack (GPU).  The geometry is that of ``make_radar_pair``
+    (float64 lat/lon/height rasters of the reference grid, secondary orbit
+    with a 150 m baseline).  Per burst: the secondary is white speckle W,
+    TOPS-modulated so that deramping returns W; the true secondary coordinates
+    are the geometric offsets plus an offset polynomial params_true ~ N(0,
+    param_sigma) (samples) plus the height sensitivities times dh_true, a
+    N(0, 1) field smoothed by a ``dh_smooth``-pixel Gaussian and scaled to
+    ``dh_sigma`` metres rms; the reference is coherence * (secondary
+    resampled there with the 8-tap sinc) + sqrt(1 - coherence^2) * noise.
+    Refinement from zero should move toward (params_true, dh_true).
+    ``margin`` > 0 makes the reference grid the burst minus ``margin``
+    pixels on every side (offsets shifted accordingly), so that no pixel's
+    8 x 8 support reaches the secondary burst's edge."""
+    import torch
+
+    from . import kernels, plan as _plan
+    sc = make_radar_pair(config, seed=seed, device=device, lines=lines, samples=samples)
+    sp = _plan.burst_plan(sc.sec.radar, sc.sec.orbit, sc.sec.fm, sc.sec.dc, sc.sec.bursts[0], None)
+    rp = _plan.burst_plan(sc.ref.radar, sc.ref.orbit, sc.ref.fm, sc.ref.dc, sc.ref.bursts[0], None)
+    az0, rg0, daz, drg = kernels.geo2rdr_offsets_dh(sp, rp, sc.lat, sc.lon, sc.hgt)
+    m = int(margin)
+    if m > 0:
+        az0 = (az0[m:-m, m:-m] + m).contiguous()
+        rg0 = (rg0[m:-m, m:-m] + m).contiguous()
+        daz = daz[m:-m, m:-m].contiguous()
+        drg = drg[m:-m, m:-m].contiguous()
+    L, S = az0.shape
+    geometry = (sc.lat, sc.lon, sc.hgt) if keep_geometry else None
+    sc.lat = sc.lon = sc.hgt = None
+    rng = np.random.Generator(np.random.PCG64(seed + 1))
+    params = torch.tensor(rng.normal(0.0, param_sigma, (n_bursts, 6)), dtype=torch.float32, device=device)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed + 2)
+    dh = gaussian_smooth(torch.randn((n_bursts, L, S), generator=gen, device=device), dh_smooth)
+    dh = dh * (dh_sigma / dh.std())
+    rows = torch.arange(L, dtype=torch.float32, device=device)[:, None]
+    cols = torch.arange(S, dtype=torch.float32, device=device)[None, :]
+    xa, xr = (rows - 0.5 * L) / L, (cols - 0.5 * S) / S
+    # secondary deramp phase of every sample, -pi kt (eta - etaref)^2 (the
+    # resampler multiplies by exp(i phase) before interpolating)
+    kt, etaref, eta = tops_coefficients(sc.sec, sc.sec.bursts[0])
+    kt_t = torch.tensor(kt, dtype=torch.float64, device=device)[None, :]
+    er_t = torch.tensor(etaref, dtype=torch.float64, device=device)[None, :]
+    eta_t = torch.tensor(eta, dtype=torch.float64, device=device)[:, None]
+    phase = -math.pi * kt_t * (eta_t - er_t) ** 2
+    rot = torch.polar(torch.ones_like(phase), -phase).to(torch.complex64)
+    del phase
+    ref = torch.empty((n_bursts, L, S), dtype=torch.complex64, device=device)
+    Ls, Ss = rot.shape
+    sec = torch.empty((n_bursts, Ls, Ss), dtype=torch.complex64, device=device)
+    for b in range(n_bursts):
+        w = speckle(Ls, Ss, gen, device)
+        sec[b] = w * rot
+        p = params[b]
+        az_t = (az0 + p[0] + p[1] * xa + p[2] * xr + daz * dh[b]).contiguous()
+        rg_t = (rg0 + p[3] + p[4] * xa + p[5] * xr + drg * dh[b]).contiguous()
+        s_true = kernels.resample(sp, sec[b], az_t, rg_t)
+        ref[b] = coherence * s_true + math.sqrt(1 - coherence ** 2) * speckle(L, S, gen, device)
+    stack = RefineStack(sec_plans=[sp] * n_bursts, ref=ref, sec=sec,
+                        az0=az0.expand(n_bursts, L, S).contiguous(), rg0=rg0.expand(n_bursts, L, S).contiguous(),
+                        daz_dh=daz.expand(n_bursts, L, S).contiguous(), drg_dh=drg.expand(n_bursts, L, S).contiguous(),
+                        params_true=params, dh_true=dh.contiguous(), rowlook=sc.rowlook, collook=sc.collook,
+                        coherence=coherence, sec_acq=sc.sec, ref_acq=sc.ref, geometry=geometry, margin=m)
+    return stack
