@@ -45,10 +45,13 @@ def geocode_burst(plan, slc: torch.Tensor, dem: torch.Tensor, deramped: torch.Te
     return gslc_header(plan, first, last), full[first:last]
 
 
-def geo2rdr_files(db_path, out_prefix, slc_path=None):
-    """File-level drop-in for ``geo2rdr dbname slcoutfile [slcinfile]`` (geo2rdr.cu:704-734):
-    reads the parameter DB and the files it names, writes ``<out>_burst_<i>.gslc``.
-    Returns the list of written paths."""
+def geo2rdr_files(db_path, out_prefix, slc_path=None, stream=None):
+    """File-level drop-in for ``geo2rdr dbname slcoutfile [slcinfile] [--stdin]``
+    (geo2rdr.cu:704-734): reads the parameter DB and the files it names,
+    writes ``<out>_burst_<i>.gslc``.  With ``stream`` (a binary file object,
+    e.g. stdin) the bursts are read from it one after the other, every burst
+    before its window is checked (geo2rdr.cu:551-557); a short read raises
+    EOFError.  Returns the list of written paths."""
     from types import SimpleNamespace
     p = formats.read_db(db_path)
     radar = SimpleNamespace(samples_per_burst=int(p["samplesPerBurst"]), lines_per_burst=int(p["linesPerBurst"]),
@@ -69,16 +72,22 @@ def geo2rdr_files(db_path, out_prefix, slc_path=None):
     dc = formats.read_poly(p["dcinfo"])
     rsc = formats.read_rsc(p["rscfile"])
     dem = torch.from_numpy(np.fromfile(p["demfile"], dtype=np.int16).reshape(rsc.nlat, rsc.nlon)).cuda()
-    src = slc_path or p["slc_file"]
+    src = slc_path or p.get("slc_file")
     L, S = radar.lines_per_burst, radar.samples_per_burst
     written = []
     for i, b in enumerate(bursts):
+        if stream is not None:
+            buf = stream.read(L * S * 8)
+            if len(buf) != L * S * 8:
+                raise EOFError(f"expected {L * S * 8} bytes from stdin, got {len(buf)}")
+            raw = np.frombuffer(buf, dtype=np.complex64).copy()
         pl = _plan.burst_plan(radar, orbit, fm, dc, b, rsc)
         if pl.nrow <= 0 or pl.ncol <= 0:
             continue
-        raw = np.fromfile(src, dtype=np.complex64, count=L * S, offset=i * L * S * 8)
-        if raw.size != L * S:
-            raise IOError(f"{src}: short read for burst {i}")
+        if stream is None:
+            raw = np.fromfile(src, dtype=np.complex64, count=L * S, offset=i * L * S * 8)
+            if raw.size != L * S:
+                raise IOError(f"{src}: short read for burst {i}")
         res = geocode_burst(pl, torch.from_numpy(raw).cuda(), dem)
         if res is None:
             continue

@@ -6,18 +6,15 @@ check the s1b kernels against the same stored outputs.  The reference's
 row crop can drop rows with few non-zero pixels (a racy reduction in
 geo2rdr.cu:115-122), so crops are compared by containment.
 """
-import os
-from types import SimpleNamespace
 
 import numpy as np
 import pytest
 
-from helpers import phase_rms, rel_err
+from helpers import GOLD, golden_acq, golden_rsc, phase_rms, rel_err
 from oracle import crossmul as ox
 from oracle import geo2rdr as og2
 from oracle import goldstein as ogs
 
-GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_chain_tiny.npz")
 
 
 @pytest.fixture(scope="module")
@@ -25,21 +22,8 @@ def z():
     return np.load(GOLD)
 
 
-def _acq(z, prefix):
-    r = z[prefix + "radar"]
-    b = z[prefix + "burst"]
-    radar = og2.Radar(samples_per_burst=int(r[0]), lines_per_burst=int(r[1]), prf=r[2], wvl=r[3], hmin=r[4],
-                      hmax=r[5], range_sampling_rate=r[6], slant_range_time=r[7], azimuth_steering_rate=r[8],
-                      azimuth_time_interval=r[9], radar_frequency=r[10])
-    burst = og2.BurstMeta(azimuth_time=b[0], first_valid_line=int(b[1]), last_valid_line=int(b[2]),
-                          first_valid_sample=int(b[3]), last_valid_sample=int(b[4]))
-    orbit = (z[prefix + "tt"], z[prefix + "xx"], z[prefix + "vv"])
-    return SimpleNamespace(radar=radar, bursts=[burst], orbit=orbit, fm=z[prefix + "fm"], dc=z[prefix + "dc"])
-
-
-def _rsc(z):
-    r = z["rsc"]
-    return og2.Rsc(nlat=int(r[0]), nlon=int(r[1]), latmax=r[2], lonmin=r[3], dlat=r[4], dlon=r[5])
+_acq = golden_acq
+_rsc = golden_rsc
 
 
 def _compare_gslc(gh, gd, wh, wd):
