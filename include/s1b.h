@@ -322,6 +322,27 @@ int s1b_goldstein(const void *in, void *out, int32_t nrow, int32_t ncol, int32_t
 int s1b_goldstein_noalloc(const void *in, void *out, int32_t nrow, int32_t ncol, int32_t n_win,
                           float alpha, void *stream);
 
+/* ------------------------------------------------ amplitude / coherence files */
+
+/* Amplitude looks of one cropped geocoded SLC (complex64 [height x width],
+ * top-left pixel (left, top) of an nrow0 x ncol0 frame) into the full-frame
+ * float32 amplitude grid amp [nrow0/rowlook x ncol0/collook]: the
+ * look-aligned part of the crop, sqrt(mean |s|^2) (sqrt|s| for 1 x 1 looks,
+ * as s1proc's powlooks), written everywhere when `first`, else only where
+ * amp is 0 and the new value is not (s1proc/coherence.py:14-55). */
+int s1b_amp_looks(const void *slc, int32_t width, int32_t height, int32_t left, int32_t top, int32_t nrow0,
+                  int32_t ncol0, int32_t rowlook, int32_t collook, int32_t first, float *amp, void *stream);
+
+/* .cc raster of an interferogram: rows [amp1*amp2 | coherence], coherence =
+ * |ifg| / (amp1 + 1e-12) / (amp2 + 1e-12) with values above 1 replaced by a
+ * uniform [0,1) value of (fill_seed, pixel index) (s1proc/coherence.py:136-147).
+ * ifg complex64, amp1/amp2 float32 [nrow x ncol]; cc float32 [nrow x 2 ncol]. */
+int s1b_coherence_cc(const void *ifg, const float *amp1, const float *amp2, int32_t nrow, int32_t ncol,
+                     uint64_t fill_seed, float *cc, void *stream);
+
+/* ECEF -> geodetic (deg, deg, m), one-step Bowring (s1proc/geometry.py:166-193). */
+int s1b_xyz2llh(const double *xyz, double *llh, int64_t n, void *stream);
+
 /* ------------------------------------------------------------ batched frame
  * All burst pairs of a frame (e.g. 3 subswaths x 9 bursts of uneven size)
  * processed with one launch per stage over a per-burst descriptor table:

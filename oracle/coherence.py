@@ -120,3 +120,4 @@ def cc_rows(prod, c):
     out[:, :ncol] = prod
     out[:, ncol:] = c
     return out
+

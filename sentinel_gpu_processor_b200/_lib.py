@@ -139,6 +139,10 @@ _SIGNATURES = {
     "s1b_goldstein": (c_int, [c_void_p, c_void_p, c_int32, c_int32, c_int32, c_float, c_void_p, c_size_t,
                               c_void_p]),
     "s1b_goldstein_noalloc": (c_int, [c_void_p, c_void_p, c_int32, c_int32, c_int32, c_float, c_void_p]),
+    "s1b_amp_looks": (c_int, [c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32, c_int32, c_int32, c_int32,
+                              c_int32, c_void_p, c_void_p]),
+    "s1b_coherence_cc": (c_int, [c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_uint64, c_void_p, c_void_p]),
+    "s1b_xyz2llh": (c_int, [c_void_p, c_void_p, c_int64, c_void_p]),
     "s1b_frame_create": (c_int, [POINTER(BurstPlan), c_int32, POINTER(c_int32), POINTER(c_int32), c_int32, c_int32,
                                  c_int32, c_int32, c_float, c_uint64, POINTER(c_void_p)]),
     "s1b_frame_destroy": (None, [c_void_p]),

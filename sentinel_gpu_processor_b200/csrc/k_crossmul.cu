@@ -152,6 +152,46 @@ __global__ __launch_bounds__(XM_THREADS) void crossmul_looks_kernel(const XmArgs
   crossmul_tile(a, blockIdx.x, blockIdx.y, smem4);
 }
 
+// ----------------------------------------------- amplitude and coherence files
+// Amplitude looks of one cropped SLC into a full-frame amplitude grid
+// (s1proc/coherence.py:14-55): the crop's look-aligned part, sqrt of the
+// mean power over rl x cl (|s| when both looks are 1, powlooks,
+// s1proc/sario.py:416-420, so sqrt|s|), written where this is the first
+// image of the date or the grid is still 0 and the new value is not.
+__global__ void amp_looks_kernel(const float2 *__restrict__ slc, int width, int left, int top, int left_sm,
+                                 int top_sm, int nrow_sm_crop, int ncol_sm_crop, int ncol0_sm, int rowlook,
+                                 int collook, int first, float *__restrict__ amp) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+  if (j >= ncol_sm_crop) return;
+  const int r0 = (top_sm + i) * rowlook - top, c0 = (left_sm + j) * collook - left;
+  float p = 0.f;
+  for (int r = 0; r < rowlook; ++r)
+    for (int c = 0; c < collook; ++c) {
+      const float2 v = __ldg(slc + (int64_t)(r0 + r) * width + c0 + c);
+      p += v.x * v.x + v.y * v.y;
+    }
+  const float a = (rowlook == 1 && collook == 1) ? sqrtf(sqrtf(p)) : sqrtf(p / (float)collook / (float)rowlook);
+  float *dst = amp + (int64_t)(top_sm + i) * ncol0_sm + left_sm + j;
+  if (first || (*dst == 0.f && a != 0.f)) *dst = a;
+}
+
+// .cc rows [amp1 amp2 | coherence] (s1proc/coherence.py:136-147, sario.py:387-394):
+// coherence |ifg| / (amp1 + 1e-12) / (amp2 + 1e-12), values above 1 replaced
+// by a uniform [0, 1) value of (seed, pixel index).
+__global__ void coherence_cc_kernel(const float2 *__restrict__ ifg, const float *__restrict__ amp1,
+                                    const float *__restrict__ amp2, int nrow, int ncol, uint64_t seed,
+                                    float *__restrict__ cc) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+  if (j >= ncol) return;
+  const int64_t o = (int64_t)i * ncol + j;
+  const float2 v = ifg[o];
+  const float a1 = amp1[o], a2 = amp2[o];
+  float c = hypotf(v.x, v.y) / (a1 + 1e-12f) / (a2 + 1e-12f);
+  if (c > 1.f) c = fill_uniform(seed, (uint64_t)o);
+  cc[(int64_t)i * 2 * ncol + j] = a1 * a2;
+  cc[(int64_t)i * 2 * ncol + ncol + j] = c;
+}
+
 // ------------------------------------------------------------ frame stages
 // Per pair, from the crop rows the geocoding stage voted: the two .gslc
 // headers (geo2rdr.cu:641-647), the overlap box aligned to the looks and the
@@ -286,6 +326,38 @@ extern "C" int s1b_crossmul_looks(const void *ref, int32_t ref_left, int32_t ref
   if (nchunk > 65535) return s1b_fail(S1B_ERR_TOO_LARGE, "s1b_crossmul_looks: too many columns");
   dim3 grid(nrow_ml, nchunk);
   crossmul_looks_kernel<<<grid, XM_THREADS, smem, (cudaStream_t)stream>>>(a);
+  return s1b_launch_status();
+}
+
+extern "C" int s1b_amp_looks(const void *slc, int32_t width, int32_t height, int32_t left, int32_t top,
+                             int32_t nrow0, int32_t ncol0, int32_t rowlook, int32_t collook, int32_t first,
+                             float *amp, void *stream) {
+  if (!slc || !amp) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_amp_looks: null argument");
+  if (rowlook < 1 || collook < 1 || width < 0 || height < 0 || left < 0 || top < 0)
+    return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_amp_looks: bad looks or crop");
+  const int left_sm = (left + collook - 1) / collook, top_sm = (top + rowlook - 1) / rowlook;
+  const int right_sm = (left + width) / collook, bottom_sm = (top + height) / rowlook;
+  const int ncol0_sm = ncol0 / collook, nrow0_sm = nrow0 / rowlook;
+  if (right_sm > ncol0_sm || bottom_sm > nrow0_sm)
+    return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_amp_looks: crop outside the frame");
+  const int nr = bottom_sm - top_sm, nc = right_sm - left_sm;
+  if (nr <= 0 || nc <= 0) return S1B_OK;
+  if (nr > 65535) return s1b_fail(S1B_ERR_TOO_LARGE, "s1b_amp_looks: too many rows");
+  dim3 grid((nc + 255) / 256, nr);
+  amp_looks_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>((const float2 *)slc, width, left, top, left_sm, top_sm,
+                                                           nr, nc, ncol0_sm, rowlook, collook, first ? 1 : 0, amp);
+  return s1b_launch_status();
+}
+
+extern "C" int s1b_coherence_cc(const void *ifg, const float *amp1, const float *amp2, int32_t nrow, int32_t ncol,
+                                uint64_t fill_seed, float *cc, void *stream) {
+  if (!ifg || !amp1 || !amp2 || !cc) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_coherence_cc: null argument");
+  if (nrow < 0 || ncol < 0) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_coherence_cc: negative size");
+  if (nrow == 0 || ncol == 0) return S1B_OK;
+  if (nrow > 65535) return s1b_fail(S1B_ERR_TOO_LARGE, "s1b_coherence_cc: too many rows");
+  dim3 grid((ncol + 255) / 256, nrow);
+  coherence_cc_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>((const float2 *)ifg, amp1, amp2, nrow, ncol, fill_seed,
+                                                              cc);
   return s1b_launch_status();
 }
 

@@ -339,6 +339,27 @@ __global__ void llh2xyz_kernel(const double *llh, double *xyz, int64_t n) {
   xyz[3 * i + 2] = (re * (1 - kRe2D) + h) * sl;
 }
 
+// ECEF -> geodetic with the one-step Bowring formula of s1proc/geometry.py:166-193
+// (the form bounds.cu uses), degrees and metres.
+__global__ void xyz2llh_kernel(const double *xyz, double *llh, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
+  const double q2 = 1.0 / (1.0 - kRe2D), q = sqrt(q2), q3 = q2 - 1.0, b = kRaD * sqrt(1 - kRe2D);
+  double lon = atan2(y, x);
+  if (y < 0 && lon > 0) lon -= kPiD;
+  if (y > 0 && lon < 0) lon += kPiD;
+  const double rp = sqrt(x * x + y * y);
+  const double th = atan((z / rp) * q);
+  const double st = sin(th), ct = cos(th);
+  const double lat = atan((z + q3 * b * st * st * st) / (rp - kRe2D * kRaD * ct * ct * ct));
+  const double sl = sin(lat);
+  const double re = kRaD / sqrt(1.0 - kRe2D * sl * sl);
+  llh[3 * i] = lat * (180.0 / kPiD);
+  llh[3 * i + 1] = lon * (180.0 / kPiD);
+  llh[3 * i + 2] = rp / cos(lat) - re;
+}
+
 }  // namespace
 
 extern "C" int s1b_deramp(const s1b_burst_plan_t *plan, const void *in, void *out, void *stream) {
@@ -388,6 +409,13 @@ extern "C" int s1b_llh2xyz(const double *llh, double *xyz, int64_t n, void *stre
   if (n > 0 && (!llh || !xyz)) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_llh2xyz: null argument");
   if (n <= 0) return S1B_OK;
   llh2xyz_kernel<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(llh, xyz, n);
+  return s1b_launch_status();
+}
+
+extern "C" int s1b_xyz2llh(const double *xyz, double *llh, int64_t n, void *stream) {
+  if (n > 0 && (!xyz || !llh)) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_xyz2llh: null argument");
+  if (n <= 0) return S1B_OK;
+  xyz2llh_kernel<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(xyz, llh, n);
   return s1b_launch_status();
 }
 

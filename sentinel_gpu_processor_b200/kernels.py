@@ -157,6 +157,48 @@ def llh2xyz(llh: torch.Tensor) -> torch.Tensor:
     return out
 
 
+def xyz2llh(xyz: torch.Tensor) -> torch.Tensor:
+    """ECEF [n, 3] -> (deg, deg, m) [n, 3], float64."""
+    _need_cuda(xyz)
+    xyz = xyz.contiguous().to(torch.float64)
+    out = torch.empty_like(xyz)
+    _lib.check(_call("xyz2llh", _lib.load().s1b_xyz2llh, _lib.dptr(xyz), _lib.dptr(out), xyz.shape[0],
+                     _lib.stream_ptr()), "s1b_xyz2llh")
+    return out
+
+
+def amp_looks(slc: torch.Tensor, left: int, top: int, nrow0: int, ncol0: int, rowlook: int, collook: int,
+              first: bool, amp: torch.Tensor) -> torch.Tensor:
+    """Amplitude looks of a cropped geocoded SLC [h, w] (top-left (left, top))
+    into the frame grid ``amp`` float32 [nrow0//rowlook, ncol0//collook]."""
+    _need_cuda(slc, amp)
+    _c64(slc, "slc")
+    if amp.dtype != torch.float32 or tuple(amp.shape) != (nrow0 // rowlook, ncol0 // collook) or \
+            not amp.is_contiguous():
+        raise ValueError("amp must be contiguous float32 [nrow0//rowlook, ncol0//collook]")
+    h, w = slc.shape
+    _lib.check(_call("amp_looks", _lib.load().s1b_amp_looks, _lib.dptr(slc), w, h, int(left), int(top), int(nrow0),
+                     int(ncol0), int(rowlook), int(collook), 1 if first else 0, _lib.dptr(amp), _lib.stream_ptr()),
+               "s1b_amp_looks")
+    return amp
+
+
+def coherence_cc(ifg: torch.Tensor, amp1: torch.Tensor, amp2: torch.Tensor, fill_seed: int = 0,
+                 out: torch.Tensor | None = None) -> torch.Tensor:
+    """``.cc`` raster float32 [nrow, 2 ncol]: rows [amp1*amp2 | coherence]."""
+    _need_cuda(ifg, amp1, amp2, out)
+    _c64(ifg, "ifg")
+    nrow, ncol = ifg.shape
+    for a in (amp1, amp2):
+        if a.dtype != torch.float32 or tuple(a.shape) != (nrow, ncol) or not a.is_contiguous():
+            raise ValueError("amp1/amp2 must be contiguous float32 rasters of the interferogram's shape")
+    if out is None:
+        out = torch.empty((nrow, 2 * ncol), dtype=torch.float32, device=ifg.device)
+    _lib.check(_call("coherence_cc", _lib.load().s1b_coherence_cc, _lib.dptr(ifg), _lib.dptr(amp1), _lib.dptr(amp2),
+                     nrow, ncol, int(fill_seed), _lib.dptr(out), _lib.stream_ptr()), "s1b_coherence_cc")
+    return out
+
+
 def geo2rdr_offsets(plan: _lib.BurstPlan, lat: torch.Tensor, lon: torch.Tensor, hgt: torch.Tensor,
                     az_off: torch.Tensor | None = None, rg_off: torch.Tensor | None = None):
     """Secondary sample offsets (az_off, rg_off float32 [L, S]) of the reference
