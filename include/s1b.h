@@ -343,6 +343,35 @@ int s1b_coherence_cc(const void *ifg, const float *amp1, const float *amp2, int3
 /* ECEF -> geodetic (deg, deg, m), one-step Bowring (s1proc/geometry.py:166-193). */
 int s1b_xyz2llh(const double *xyz, double *llh, int64_t n, void *stream);
 
+/* ------------------------------------------------------------ burst stitching */
+
+/* One burst interferogram of a frame: `offset` = first element in the data
+ * buffer (bursts back to back, row-major [bottom - top x right - left]);
+ * left/top/right/bottom in frame pixels; subswath 1..3; `group` identifies
+ * the pair of burst ids (the overlap phase offset is estimated when it
+ * changes from the previous burst, s1proc/interfere.py:92-118). */
+typedef struct {
+  int64_t offset;
+  int32_t left, top, right, bottom;
+  int32_t subswath, group;
+} s1b_stitch_burst_t;
+
+/* Device workspace of s1b_stitch (subswath mosaics and tables). */
+size_t s1b_stitch_workspace_bytes(const s1b_stitch_burst_t *bursts, int32_t n, int32_t out_float);
+
+/* Stitch burst interferograms (complex64, or float32 phase with out_float)
+ * into the frame [nrow0 x ncol0] (s1proc/interfere.py:81-180): per subswath,
+ * bursts in order of top + bottom, overlap phase offset angle(mean(conj(old)
+ * new)) plus the median residual angle, removed from the new burst, which
+ * fills the mosaic where it is empty; subswaths 1..3 written in order where
+ * non-zero.  bursts: host array; offsets_host (optional, double [n]): the
+ * offset applied to each burst (synchronises the stream when given).  The
+ * union box of a subswath is that of its first and last burst, as the
+ * reference computes it; parts of middle bursts outside it are dropped. */
+int s1b_stitch(const s1b_stitch_burst_t *bursts, int32_t n, const void *data, int32_t out_float, int32_t nrow0,
+               int32_t ncol0, void *frame, double *offsets_host, void *workspace, size_t workspace_bytes,
+               void *stream);
+
 /* ------------------------------------------------------------ batched frame
  * All burst pairs of a frame (e.g. 3 subswaths x 9 bursts of uneven size)
  * processed with one launch per stage over a per-burst descriptor table:

@@ -95,6 +95,11 @@ class BurstPlan(ctypes.Structure):
 
 
 # name -> (restype, argtypes); the table is the C ABI of include/s1b.h
+class StitchBurst(ctypes.Structure):
+    _fields_ = [("offset", c_int64), ("left", c_int32), ("top", c_int32), ("right", c_int32), ("bottom", c_int32),
+                ("subswath", c_int32), ("group", c_int32)]
+
+
 class FramePair(ctypes.Structure):
     """s1b_frame_pair_t: per-pair result of a frame run."""
     _fields_ = [("ok", c_int32), ("nrow_ml", c_int32), ("ncol_ml", c_int32), ("filtered", c_int32),
@@ -143,6 +148,9 @@ _SIGNATURES = {
                               c_int32, c_void_p, c_void_p]),
     "s1b_coherence_cc": (c_int, [c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_uint64, c_void_p, c_void_p]),
     "s1b_xyz2llh": (c_int, [c_void_p, c_void_p, c_int64, c_void_p]),
+    "s1b_stitch_workspace_bytes": (c_size_t, [POINTER(StitchBurst), c_int32, c_int32]),
+    "s1b_stitch": (c_int, [POINTER(StitchBurst), c_int32, c_void_p, c_int32, c_int32, c_int32, c_void_p,
+                           POINTER(c_double), c_void_p, c_size_t, c_void_p]),
     "s1b_frame_create": (c_int, [POINTER(BurstPlan), c_int32, POINTER(c_int32), POINTER(c_int32), c_int32, c_int32,
                                  c_int32, c_int32, c_float, c_uint64, POINTER(c_void_p)]),
     "s1b_frame_destroy": (None, [c_void_p]),
