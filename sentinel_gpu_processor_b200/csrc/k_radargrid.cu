@@ -842,20 +842,23 @@ __global__ __launch_bounds__(RT_THREADS, 2) void resample_tma_kernel(
 // ------------------------------------------------------- box coherence
 // Persistent kernel, one CTA of 512 threads per SM, output tiles of 128
 // columns x 32 rows taken round-robin.  Both SLC tiles plus a halo are
-// brought into shared memory by TMA (cp.async.bulk.tensor, zero fill
-// outside the raster) through a two-stage pipeline: the next tile streams in
-// while the current one is reduced.  The conj product and both powers are
-// formed once per staged pixel in place; each thread then slides a window
-// down one column (8 output rows): horizontal sums per row, a ring of the last
-// `win` of them, and the vertical sum.  The vertical sum of the complex
-// channel slides (add the entering row, subtract the leaving one) with Kahan
-// compensation; the power sums, of non-negative terms, are summed directly.  Without a tensor map (odd width, unaligned base) tiles are staged
-// by plain loads.
+// brought into shared memory by TMA (cp.async.bulk.tensor, zero fill outside
+// the raster) through a two-stage pipeline: the next tile streams in while
+// the current one is reduced.  The conj product and both powers are formed
+// once per staged pixel in place, two pixels per 16-byte access.  Each thread
+// then slides the windows of two adjacent columns down 4 output rows:
+// horizontal sums per row from 16-byte reads (the taps the two windows share
+// summed once), a ring of the last `win` of them, and the vertical sums.  The
+// vertical sum of the complex channel slides (add the entering row, subtract
+// the leaving one) with Kahan compensation, re and im in paired FP32; the
+// power sums, of non-negative terms, are summed directly.  Without a tensor
+// map (odd width, unaligned base) tiles are staged by plain loads.
 constexpr int C_TW = 128, C_TH = 32, C_HX = 4;  // halo columns (even, >= half window)
 constexpr int C_IW = C_TW + 2 * C_HX;            // 136 staged columns
 constexpr int C_MAXH = 4;                        // half window <= 4 (win <= 9)
 constexpr int C_IH = C_TH + 2 * C_MAXH;          // 40 staged rows
-constexpr int C_THREADS = 512, C_PARTS = C_THREADS / C_TW, C_ROWS = C_TH / C_PARTS;  // 4 parts x 8 rows
+// 512 threads: 64 column pairs x 8 parts of 4 output rows
+constexpr int C_THREADS = 512, C_PAIRS = C_TW / 2, C_PARTS = C_THREADS / C_PAIRS, C_ROWS = C_TH / C_PARTS;
 constexpr int C_STAGE = 2 * C_IH * C_IW;         // float2 per stage (ref + sec)
 
 // Kahan compensated summation (W. Kahan, "Further remarks on reducing
@@ -869,6 +872,20 @@ struct Kahan {
     s = t;
   }
   __device__ __forceinline__ float value() const { return s; }
+};
+
+// Kahan summation of two independent sums at once (re and im of one complex
+// sum) with paired FP32 operations; nc holds the negated compensation.  Each
+// lane performs exactly the scalar Kahan steps.
+struct Kahan2 {
+  float2 s = make_float2(0.f, 0.f), nc = make_float2(0.f, 0.f);
+  __device__ __forceinline__ void step(float2 y) {
+    const float2 t = __fadd2_rn(s, y);
+    nc = __fadd2_rn(__ffma2_rn(t, make_float2(-1.f, -1.f), s), y);  // (s - t) + y
+    s = t;
+  }
+  __device__ __forceinline__ void add(float2 x) { step(__fadd2_rn(x, nc)); }
+  __device__ __forceinline__ void sub(float2 x) { step(__ffma2_rn(x, make_float2(-1.f, -1.f), nc)); }
 };
 
 __device__ __forceinline__ void tma_tile(float2 *dst_r, float2 *dst_s, const CUtensorMap &tr, const CUtensorMap &ts,
@@ -898,7 +915,7 @@ __global__ __launch_bounds__(C_THREADS, 1) void box_coherence_kernel(const __gri
   float2 *stage0 = reinterpret_cast<float2 *>(smem_raw);
   __shared__ __align__(8) uint64_t bars[2];
   constexpr int WIN = 2 * HALF + 1;
-  const int tx = threadIdx.x % C_TW, part = threadIdx.x / C_TW;
+  const int tp = threadIdx.x % C_PAIRS, part = threadIdx.x / C_PAIRS;
   if (kTma) {
     if (threadIdx.x == 0) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bars[0])) : "memory");
@@ -944,52 +961,100 @@ __global__ __launch_bounds__(C_THREADS, 1) void box_coherence_kernel(const __gri
       }
       __syncthreads();
     }
-    // products once per staged pixel, in place: sr <- conj(r) s, ss <- (|r|^2, |s|^2)
-    for (int idx = threadIdx.x; idx < C_IH * C_IW; idx += C_THREADS) {
-      const float2 a = sr[idx], b = ss[idx];
-      float2 cp = __fmul2_rn(make_float2(a.x, a.x), b);
-      cp = __ffma2_rn(make_float2(a.y, -a.y), make_float2(b.y, b.x), cp);
-      const float2 xx = make_float2(a.x, b.x), yy = make_float2(a.y, b.y);
-      sr[idx] = cp;
-      ss[idx] = __ffma2_rn(yy, yy, __fmul2_rn(xx, xx));
+    // products once per staged pixel, in place: sr <- conj(r) s, ss <- (|r|^2, |s|^2);
+    // two pixels per 16-byte access (rows are 16-byte aligned)
+    {
+      float4 *sr4 = reinterpret_cast<float4 *>(sr);
+      float4 *ss4 = reinterpret_cast<float4 *>(ss);
+      for (int idx = threadIdx.x; idx < C_IH * C_IW / 2; idx += C_THREADS) {
+        const float4 a4 = sr4[idx], b4 = ss4[idx];
+        float2 cp[2], pw[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const float2 a = h ? make_float2(a4.z, a4.w) : make_float2(a4.x, a4.y);
+          const float2 b = h ? make_float2(b4.z, b4.w) : make_float2(b4.x, b4.y);
+          cp[h] = __ffma2_rn(make_float2(a.y, -a.y), make_float2(b.y, b.x), __fmul2_rn(make_float2(a.x, a.x), b));
+          const float2 xx = make_float2(a.x, b.x), yy = make_float2(a.y, b.y);
+          pw[h] = __ffma2_rn(yy, yy, __fmul2_rn(xx, xx));
+        }
+        sr4[idx] = make_float4(cp[0].x, cp[0].y, cp[1].x, cp[1].y);
+        ss4[idx] = make_float4(pw[0].x, pw[0].y, pw[1].x, pw[1].y);
+      }
     }
     __syncthreads();
-    const int col = col0 + tx;
+    // Two output columns per thread, c and c + 1 of the tile: their windows
+    // cover staged columns s0 .. s0 + WIN, read as 16-byte pairs from the
+    // even column below s0; the WIN - 1 taps they share are summed once.
+    constexpr int O = HALF & 1;                   // s0 is odd exactly when HALF is
+    constexpr int NPX = (WIN + 1 + O + 1) & ~1;   // staged pixels read per row
+    const int c = 2 * tp;
     const int orow0 = part * C_ROWS;
     const int first = orow0 + C_MAXH - HALF;  // staged row of the first window row
-    // ring of the last WIN horizontal sums: (re, im) of conj(r)s and (|r|^2, |s|^2)
-    float2 rc[WIN], rp[WIN];
-    Kahan vre, vim;  // sliding, compensated sum of the complex channel
+    const int cs = c + C_HX - HALF - O;       // even staged column of the first pixel read
+    float2 rc[2][WIN], rp[2][WIN];            // rings of horizontal sums per column
+    Kahan2 vs[2];                             // sliding, compensated sums of the complex channel
 #pragma unroll
     for (int j = 0; j < C_ROWS + WIN - 1; ++j) {
-      const float2 *pr = sr + (first + j) * C_IW + tx + C_HX - HALF;
-      const float2 *pp = ss + (first + j) * C_IW + tx + C_HX - HALF;
-      float2 hc = pr[0], hp = pp[0];
+      const float4 *pr = reinterpret_cast<const float4 *>(sr + (first + j) * C_IW + cs);
+      const float4 *pp = reinterpret_cast<const float4 *>(ss + (first + j) * C_IW + cs);
+      float2 vr[NPX], vp[NPX];
 #pragma unroll
-      for (int dx = 1; dx < WIN; ++dx) {
-        hc = __fadd2_rn(hc, pr[dx]);
-        hp = __fadd2_rn(hp, pp[dx]);
+      for (int k = 0; k < NPX / 2; ++k) {
+        const float4 a = pr[k], b = pp[k];
+        vr[2 * k] = make_float2(a.x, a.y);
+        vr[2 * k + 1] = make_float2(a.z, a.w);
+        vp[2 * k] = make_float2(b.x, b.y);
+        vp[2 * k + 1] = make_float2(b.z, b.w);
       }
-      if (j >= WIN) {  // the row leaving the window
-        vre.add(-rc[j % WIN].x);
-        vim.add(-rc[j % WIN].y);
+      float2 ir = make_float2(0.f, 0.f), ip = ir;  // taps shared by both windows
+#pragma unroll
+      for (int k = 1; k < WIN; ++k) {
+        ir = k == 1 ? vr[O + 1] : __fadd2_rn(ir, vr[O + k]);
+        ip = k == 1 ? vp[O + 1] : __fadd2_rn(ip, vp[O + k]);
       }
-      rc[j % WIN] = hc;
-      rp[j % WIN] = hp;
-      vre.add(hc.x);
-      vim.add(hc.y);
+      float2 hc[2], hp[2];
+      if (WIN == 1) {
+        hc[0] = vr[O];
+        hc[1] = vr[O + 1];
+        hp[0] = vp[O];
+        hp[1] = vp[O + 1];
+      } else {
+        hc[0] = __fadd2_rn(vr[O], ir);
+        hc[1] = __fadd2_rn(ir, vr[O + WIN]);
+        hp[0] = __fadd2_rn(vp[O], ip);
+        hp[1] = __fadd2_rn(ip, vp[O + WIN]);
+      }
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        if (j >= WIN) vs[q].sub(rc[q][j % WIN]);  // the row leaving the window
+        rc[q][j % WIN] = hc[q];
+        rp[q][j % WIN] = hp[q];
+        vs[q].add(hc[q]);
+      }
       if (j >= WIN - 1) {
-        // powers: direct sums of non-negative terms (exact zeros stay zero)
-        float2 pw = rp[0];
-#pragma unroll
-        for (int q = 1; q < WIN; ++q) pw = __fadd2_rn(pw, rp[q]);
         const int orow = row0 + orow0 + (j - (WIN - 1));
-        if (col < S && orow < L) {
+        float out[2];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          // powers: direct sums of non-negative terms (exact zeros stay zero)
+          float2 pw = rp[q][0];
+#pragma unroll
+          for (int m = 1; m < WIN; ++m) pw = __fadd2_rn(pw, rp[q][m]);
           // |I| / sqrt(P1 P2) = sqrt(|I|^2) * rsqrt(P1 P2); 0 where a power is 0
           const float den2 = pw.x * pw.y;
-          const float re = vre.value(), im = vim.value();
-          const float num2 = fmaf(re, re, im * im);
-          __stcs(coh + (size_t)orow * S + col, den2 > 0.f ? sqrtf(num2) * rsqrtf(den2) : 0.f);
+          const float2 v = vs[q].s;
+          const float num2 = fmaf(v.x, v.x, v.y * v.y);
+          out[q] = den2 > 0.f ? sqrtf(num2) * rsqrtf(den2) : 0.f;
+        }
+        const int col = col0 + c;
+        if (orow < L) {
+          float *dst = coh + (size_t)orow * S + col;
+          if (kTma && col + 1 < S) {  // a tensor map implies an even width: 8-byte aligned pair
+            __stcs(reinterpret_cast<float2 *>(dst), make_float2(out[0], out[1]));
+          } else {
+            if (col < S) __stcs(dst, out[0]);
+            if (col + 1 < S) __stcs(dst + 1, out[1]);
+          }
         }
       }
     }
