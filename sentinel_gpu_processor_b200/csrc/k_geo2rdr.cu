@@ -89,11 +89,10 @@ __global__ __launch_bounds__(256) void deramp_kernel(const __grid_constant__ s1b
 
 // ----------------------------------------------------------------- geo2rdr
 // Tile: G_TX columns x G_RY rows of the DEM window, one thread per column
-// walking down the rows.  The zero-Doppler solution of the pixel above seeds
-// the Newton of the next one: the first pixel of a column solves on the
-// window polynomial from the burst centre (like the reference,
-// geo2rdr.cu:588-600), the others on the cubic orbit expansion at that
-// solution, seeded by linear extrapolation of the two pixels above.
+// walking down the rows.  Every pixel solves its zero-Doppler Newton on a
+// cubic orbit expansion shared by its warp; the first pixel of a column
+// starts from the warp's centre time, the others from the linear
+// extrapolation of the two pixels above.
 // Latitude terms depend only on the row: lanes 0..G_RY-1 of every warp form
 // them once and the warp shares them by shuffles (no block barrier);
 // longitude terms depend only on the column and stay in registers.  Warps
@@ -125,8 +124,72 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
   sincos((P.lon0 + col * P.dlon) * kPiD / 180, &sinlon, &coslon);
   const bool colok = col < ncol;
   const double inv_dmrg = 1.0 / P.dmrg, prf = 1.0 / P.dtaz, two_over_c = 2.0 / kSolD;
-  double t = P.tmid, tprev = 0.0;
-  OrbitCubic oc;
+  // One cubic orbit expansion per warp, at the zero-Doppler time of the
+  // warp's centre pixel, solved on the window polynomial from the burst
+  // centre (geo2rdr.cu:588-600).  The warp's 32 x 16 pixels lie within
+  // ~0.1 s of it, where the dropped fourth-order term is < 1e-9 m.  Lanes 1
+  // and 2 solve two opposite corners at the same time; the three solutions
+  // bound the warp's footprint in the burst, whose lines are prefetched into
+  // L2 before the per-pixel solves, so the bilinear gathers hit L2.
+  __shared__ OrbitCubic s_oc[TX / 32];
+  const int wid = tx >> 5;
+  double faz = 0.0, frg = 0.0;
+  if (lane < 3) {
+    const int c0 = tile_x * TX + wid * 32;
+    const int cr = lane == 0 ? min(row0 + G_RY / 2, nrow - 1) : (lane == 1 ? row0 : min(row0 + G_RY - 1, nrow - 1));
+    const int cc = lane == 0 ? min(c0 + 16, ncol - 1) : (lane == 1 ? min(c0, ncol - 1) : min(c0 + 31, ncol - 1));
+    double sla, cla, slo, clo;
+    sincos((P.lat0 + cr * P.dlat) * kPiD / 180, &sla, &cla);
+    sincos((P.lon0 + cc * P.dlon) * kPiD / 180, &slo, &clo);
+    const double hc = (double)__ldg(dem + (int64_t)cr * pitch + cc);
+    const double rc = kRaD / sqrt(1. - kRe2D * sla * sla);
+    const double pc[3] = {(rc + hc) * cla * clo, (rc + hc) * cla * slo, (rc * (1 - kRe2D) + hc) * sla};
+    OrbitState st;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      st.x[i] = P.xmid[i];
+      st.v[i] = P.vmid[i];
+      st.a[i] = P.amid[i];
+    }
+    double tc = P.tmid, drc[3];
+    zero_doppler(P.orbit, pc, tc, st, drc);
+    if (lane == 0) orbit_cubic(P.orbit, tc, s_oc[wid]);
+    faz = (tc - P.tstart) * prf;
+    frg = (sqrt(drc[0] * drc[0] + drc[1] * drc[1] + drc[2] * drc[2]) - P.rngstart) * inv_dmrg;
+  }
+  {
+    double a0 = faz, a1 = faz, g0 = frg, g1 = frg;
+#pragma unroll
+    for (int k = 1; k < 3; ++k) {
+      const double a = __shfl_sync(0xffffffffu, faz, k), g = __shfl_sync(0xffffffffu, frg, k);
+      a0 = fmin(a0, a);
+      a1 = fmax(a1, a);
+      g0 = fmin(g0, g);
+      g1 = fmax(g1, g);
+    }
+    a0 = __shfl_sync(0xffffffffu, a0, 0);
+    a1 = __shfl_sync(0xffffffffu, a1, 0);
+    g0 = __shfl_sync(0xffffffffu, g0, 0);
+    g1 = __shfl_sync(0xffffffffu, g1, 0);
+    // footprint with a margin of 2 samples, clamped to the burst; skipped when
+    // it is not a small patch (e.g. a warp far outside the burst)
+    const int l0 = max(0, (int)fmax(a0 - 2.0, -1.0)), l1 = min(P.lines - 1, (int)fmin(a1 + 3.0, 1e9));
+    const int s0 = max(0, (int)fmax(g0 - 2.0, -1.0)), s1 = min(P.samples - 1, (int)fmin(g1 + 3.0, 1e9));
+    const int nl = l1 - l0 + 1;
+    if (nl > 0 && nl <= 48 && s1 >= s0 && s1 - s0 < 256) {
+      const int nch = (((s1 - s0 + 1) * 8) + 127) / 128 + 1;  // 128-byte lines per burst line segment
+      for (int k = lane; k < nl * nch; k += 32) {
+        const int li = k / nch, ch = k - li * nch;
+        const float2 *ptr = burst + (size_t)(l0 + li) * P.samples + s0;
+        const char *line = reinterpret_cast<const char *>(ptr) + ch * 128;
+        if (line <= reinterpret_cast<const char *>(burst + (size_t)(l0 + li) * P.samples + s1))
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(line));
+      }
+    }
+  }
+  __syncwarp();  // lane 0's expansion is visible to the warp
+  const OrbitCubic &oc = s_oc[wid];
+  double t = oc.t0, tprev = 0.0, inv_fp = 0.0;
   const int rmax = min(G_RY, nrow - row0);
   int16_t hn = colok && rmax > 0 ? __ldg(dem + (int64_t)row0 * pitch + col) : 0;
   for (int r = 0; r < rmax; ++r) {
@@ -144,21 +207,22 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
       p[2] = (re * (1 - kRe2D) + h) * sinlat;
       double dr[3];
       if (r == 0) {
-        OrbitState st;
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-          st.x[i] = P.xmid[i];
-          st.v[i] = P.vmid[i];
-          st.a[i] = P.amid[i];
-        }
-        zero_doppler(P.orbit, p, t, st, dr);
-        orbit_cubic(P.orbit, t, oc);
+        zero_doppler_cubic(oc, p, t, dr);
         tprev = t - P.dtaz;
+        const double hh = t - oc.t0;
+        double fp = 0.0;
+        for (int i = 0; i < 3; ++i) {
+          const double a = fma(oc.j[i], hh, oc.a[i]);
+          const double v = fma(fma(0.5 * oc.j[i], hh, oc.a[i]), hh, oc.v[i]);
+          fp = fma(dr[i], a, fp);
+          fp = fma(-v, v, fp);
+        }
+        inv_fp = 1.0 / fp;
       } else {
         const double tn = 2.0 * t - tprev;
         tprev = t;
         t = tn;
-        zero_doppler_cubic(oc, p, t, dr);
+        zero_doppler_cubic_chord(oc, p, t, dr, inv_fp);
       }
       const double rng = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
       const double rgoff = (rng - P.rngstart) * inv_dmrg;

@@ -191,4 +191,27 @@ __device__ __forceinline__ void zero_doppler_cubic(const OrbitCubic &o, const do
   }
 }
 
+// zero_doppler_cubic with a fixed reciprocal derivative (chord Newton).
+__device__ __forceinline__ void zero_doppler_cubic_chord(const OrbitCubic &o, const double p[3], double &t,
+                                                         double dr[3], double inv_fp) {
+  for (int it = 0; it < 51; ++it) {
+    const double h = t - o.t0;
+    double fn = 0.0, v[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      v[i] = fma(fma(0.5 * o.j[i], h, o.a[i]), h, o.v[i]);
+      const double x = fma(fma(fma(o.j[i] * (1.0 / 6.0), h, 0.5 * o.a[i]), h, o.v[i]), h, o.x[i]);
+      dr[i] = p[i] - x;
+      fn = fma(dr[i], v[i], fn);
+    }
+    const double step = fn * inv_fp;
+    t -= step;
+    if (fabs(step) < 5.0e-9) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i) dr[i] = fma(step, v[i], dr[i]);
+      return;
+    }
+  }
+}
+
 #endif
