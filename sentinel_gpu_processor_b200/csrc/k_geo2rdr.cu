@@ -12,6 +12,7 @@
 //   * llh->ECEF trigonometry is computed once per DEM row / column per warp;
 //   * FP64 phases are reduced mod 2 pi in FP64, then rotated in FP32;
 //   * the non-zero-row search is folded into the geocoding epilogue.
+#include <climits>
 #include <cuda_runtime.h>
 
 #include "s1b.h"
@@ -192,6 +193,7 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
   double t = oc.t0, tprev = 0.0, inv_fp = 0.0;
   const int rmax = min(G_RY, nrow - row0);
   int16_t hn = colok && rmax > 0 ? __ldg(dem + (int64_t)row0 * pitch + col) : 0;
+  int rlo = INT_MAX, rhi = -1;
   for (int r = 0; r < rmax; ++r) {
     const int row = row0 + r;
     const double sinlat = __shfl_sync(0xffffffffu, r_sin, r);
@@ -262,12 +264,19 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
       }
       __stcs(out + (size_t)row * ncol + col, res);
     }
-    // first / last non-zero output row (geo2rdr.cu:86-128): one vote per warp
-    const unsigned nz = __ballot_sync(0xffffffffu, colok && (res.x != 0.f || res.y != 0.f));
-    if (nz && lane == 0 && rows) {
-      atomicMin(rows, row);
-      atomicMax(rows + 1, row + 1);
+    if (res.x != 0.f || res.y != 0.f) {
+      rlo = min(rlo, row);
+      rhi = row + 1;
     }
+  }
+  // first / last non-zero output row (geo2rdr.cu:86-128): the warp's extent
+  // over its 16 rows, one reduction pair per warp and tile (per-row
+  // reductions on one address serialise in its L2 slice)
+  rlo = __reduce_min_sync(0xffffffffu, rlo);
+  rhi = __reduce_max_sync(0xffffffffu, rhi);
+  if (lane == 0 && rows && rhi >= 0) {
+    atomicMin(rows, rlo);
+    atomicMax(rows + 1, rhi);
   }
 }
 
