@@ -32,6 +32,7 @@ struct s1b_frame {
   size_t workspace_bytes = 0;
   int64_t slc_elems = 0, product_elems = 0;
   int32_t tuning[4] = {16, 0, 128, 0};  // deramp rows, deramp CTAs, geocoding columns, geocoding CTAs
+  FrameDerampSplit split;               // bursts by deramp load width for the current buffers
 };
 
 namespace {
@@ -45,18 +46,24 @@ int cuda_fail(cudaError_t e) { return s1b_fail(S1B_ERR_CUDA, cudaGetErrorString(
 // Flat tile prefixes of the current tile shapes, uploaded to the device.
 int set_tiles(s1b_frame *f) {
   int64_t dt = 0, gt = 0;
+  int32_t dtx = 0, dty = 0;
   const int rows = f->tuning[0], cols = f->tuning[2];
   for (size_t b = 0; b < f->bursts.size(); ++b) {
     FrameBurst &fb = f->bursts[b];
     const s1b_burst_plan_t &p = f->plans[b];
     fb.deramp_tile0 = dt;
     fb.geo_tile0 = gt;
-    dt += (int64_t)((p.samples + kFrameDerampCols - 1) / kFrameDerampCols) * ((p.lines + rows - 1) / rows);
+    const int32_t tx = (p.samples + kFrameDerampCols - 1) / kFrameDerampCols, ty = (p.lines + rows - 1) / rows;
+    dt += (int64_t)tx * ty;
+    dtx = std::max(dtx, tx);
+    dty = std::max(dty, ty);
     gt += (int64_t)((fb.ncol + cols - 1) / cols) * ((fb.nrow + kFrameGeoRows - 1) / kFrameGeoRows);
   }
   f->dev.n_deramp_tiles = dt;
   f->dev.n_geo_tiles = gt;
   f->dev.deramp_rows = rows;
+  f->dev.deramp_tiles_x = dtx;
+  f->dev.deramp_tiles_y = dty;
   f->dev.geo_cols = cols;
   cudaError_t e = cudaMemcpy(f->d_bursts, f->bursts.data(), f->bursts.size() * sizeof(FrameBurst),
                              cudaMemcpyHostToDevice);
@@ -92,12 +99,20 @@ int make_io(s1b_frame *f, const void *slc, const int16_t *dem, int64_t dem_pitch
   io.coh = coh;
   io.filt = (float2 *)filt;
   io.pout = pairs;
+  f->split.vec.clear();
+  f->split.scalar.clear();
+  for (size_t b = 0; b < f->bursts.size(); ++b) {
+    const bool vec = f->plans[b].samples % 2 == 0 &&
+                     reinterpret_cast<uintptr_t>(io.slc + f->bursts[b].slc_off) % 16 == 0 &&
+                     reinterpret_cast<uintptr_t>(io.work + f->bursts[b].der_off) % 16 == 0;
+    (vec ? f->split.vec : f->split.scalar).push_back((int32_t)b);
+  }
   return S1B_OK;
 }
 
 int run_all(s1b_frame *f, const FrameIO &io, cudaStream_t st) {
   int s = frame_launch_init(f->dev, io, st);
-  if (!s) s = frame_launch_deramp(f->dev, io, f->tuning[0], f->tuning[1], st);
+  if (!s) s = frame_launch_deramp(f->dev, io, f->tuning[0], f->tuning[1], f->split, st);
   if (!s) s = frame_launch_geo2rdr(f->dev, io, f->tuning[2], f->tuning[3], st);
   if (!s) s = frame_launch_box(f->dev, io, st);
   if (!s) s = frame_launch_crossmul(f->dev, io, st);
@@ -308,7 +323,7 @@ extern "C" int s1b_frame_autotune(s1b_frame_t *f, const void *slc, const int16_t
     if (r) return r;
     for (int i = 0; i <= reps; ++i) {  // the first run is a warm-up
       if (i == 1 && (e = cudaEventRecord(a, st)) != cudaSuccess) return cuda_fail(e);
-      r = stage == 0 ? frame_launch_deramp(f->dev, io, shape, ctas, st)
+      r = stage == 0 ? frame_launch_deramp(f->dev, io, shape, ctas, f->split, st)
                      : frame_launch_geo2rdr(f->dev, io, shape, ctas, st);
       if (r) return r;
     }
@@ -325,9 +340,10 @@ extern "C" int s1b_frame_autotune(s1b_frame_t *f, const void *slc, const int16_t
     for (int shape : shapes[stage]) {
       const int full = stage == 0 ? frame_max_ctas_deramp(shape) : frame_max_ctas_geo2rdr(shape);
       const int per_sm = sms > 0 ? full / sms : 0;
-      // persistent grids of 1..per_sm CTAs per SM (0 = all resident)
-      for (int j = 1; j <= per_sm && !s; ++j) {
-        const int ctas = j == per_sm ? 0 : j * sms;
+      // persistent grids of 1..per_sm CTAs per SM; 0 = all resident
+      // (geocoding) or one CTA per tile (deramp, tried first)
+      for (int j = stage == 0 ? 0 : 1; j <= per_sm && !s; ++j) {
+        const int ctas = stage == 0 ? j * sms : (j == per_sm ? 0 : j * sms);
         float ms = 0.f;
         s = time_stage(stage, shape, ctas, ms);
         if (!s && ms < best) {
@@ -344,7 +360,7 @@ extern "C" int s1b_frame_autotune(s1b_frame_t *f, const void *slc, const int16_t
       t[stage * 2 + 1] = best_ctas;
       s = s1b_frame_set_tuning(f, t);
       // the geocoding candidates read the deramped bursts of the chosen deramp
-      if (!s && stage == 0) s = frame_launch_deramp(f->dev, io, f->tuning[0], f->tuning[1], st);
+      if (!s && stage == 0) s = frame_launch_deramp(f->dev, io, f->tuning[0], f->tuning[1], f->split, st);
     }
   }
   cudaEventDestroy(a);
@@ -372,7 +388,7 @@ extern "C" int s1b_frame_profile(s1b_frame_t *f, const void *slc, const int16_t 
   // stages: [init + deramp, geocoding, box, crossmul, Goldstein] between events
   s = frame_launch_init(f->dev, io, st);
   if (!s) e = cudaEventRecord(ev[0], st);
-  if (!s && e == cudaSuccess) s = frame_launch_deramp(f->dev, io, f->tuning[0], f->tuning[1], st);
+  if (!s && e == cudaSuccess) s = frame_launch_deramp(f->dev, io, f->tuning[0], f->tuning[1], f->split, st);
   if (!s && e == cudaSuccess) e = cudaEventRecord(ev[1], st);
   if (!s && e == cudaSuccess) s = frame_launch_geo2rdr(f->dev, io, f->tuning[2], f->tuning[3], st);
   if (!s && e == cudaSuccess) e = cudaEventRecord(ev[2], st);

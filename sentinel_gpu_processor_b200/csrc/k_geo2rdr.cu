@@ -348,6 +348,37 @@ __global__ __launch_bounds__(256, 4) void frame_deramp_kernel(const FrameDev d, 
   }
 }
 
+// One CTA per tile: blockIdx.z indexes a list of bursts that share a load
+// width, (x, y) is the tile inside the burst.  The grid spans the largest
+// burst; CTAs past a smaller one return at once.  No tile search and no
+// persistent loop, so each instantiation keeps the single-burst register
+// budget and the hardware keeps every SM full of streaming CTAs.
+template <bool kVec, int ROWS>
+__global__ __launch_bounds__(256) void frame_deramp_grid_kernel(const FrameDev d, const FrameIO io,
+                                                                const __grid_constant__ FrameBurstList list) {
+  const int b = list.idx[blockIdx.z];
+  const s1b_burst_plan_t &sp = d.plans[b];
+  if ((int)blockIdx.x * kFrameDerampCols >= sp.samples || (int)blockIdx.y * ROWS >= sp.lines) return;
+  const FrameBurst &fb = d.bursts[b];
+  deramp_tile<kVec, ROWS>(sp, io.slc + fb.slc_off, io.work + fb.der_off, blockIdx.x, blockIdx.y);
+}
+
+template <bool kVec>
+void launch_deramp_grid(const FrameDev &d, const FrameIO &io, int rows, const int32_t *bursts, int n,
+                        cudaStream_t st) {
+  for (int k0 = 0; k0 < n; k0 += kFrameListMax) {
+    FrameBurstList list;
+    list.n = n - k0 < kFrameListMax ? n - k0 : kFrameListMax;
+    for (int k = 0; k < list.n; ++k) list.idx[k] = bursts[k0 + k];
+    const dim3 grid((unsigned)d.deramp_tiles_x, (unsigned)d.deramp_tiles_y, (unsigned)list.n);
+    switch (rows) {
+      case 8: frame_deramp_grid_kernel<kVec, 8><<<grid, 256, 0, st>>>(d, io, list); break;
+      case 16: frame_deramp_grid_kernel<kVec, 16><<<grid, 256, 0, st>>>(d, io, list); break;
+      default: frame_deramp_grid_kernel<kVec, 32><<<grid, 256, 0, st>>>(d, io, list); break;
+    }
+  }
+}
+
 template <int TX>
 __global__ __launch_bounds__(TX) void frame_geo2rdr_kernel(const FrameDev d, const FrameIO io) {
   __shared__ __align__(16) s1b_burst_plan_t sp;
@@ -516,11 +547,17 @@ int frame_max_ctas_geo2rdr(int cols) {
   }
 }
 
-int frame_launch_deramp(const FrameDev &d, const FrameIO &io, int rows, int ctas, cudaStream_t st) {
+int frame_launch_deramp(const FrameDev &d, const FrameIO &io, int rows, int ctas, const FrameDerampSplit &split,
+                        cudaStream_t st) {
   const int full = frame_max_ctas_deramp(rows);
   if (full <= 0) return s1b_fail(S1B_ERR_UNSUPPORTED, "frame deramp: tile rows must be 8, 16 or 32");
   if (d.n_deramp_tiles == 0) return S1B_OK;
-  long long g = ctas > 0 && ctas < full ? ctas : full;
+  if (ctas == 0) {  // one CTA per tile, one launch per load width
+    launch_deramp_grid<true>(d, io, rows, split.vec.data(), (int)split.vec.size(), st);
+    launch_deramp_grid<false>(d, io, rows, split.scalar.data(), (int)split.scalar.size(), st);
+    return s1b_launch_status();
+  }
+  long long g = ctas < full ? ctas : full;
   if (g > d.n_deramp_tiles) g = d.n_deramp_tiles;
   switch (rows) {
     case 8: frame_deramp_kernel<8><<<(unsigned)g, 256, 0, st>>>(d, io); break;

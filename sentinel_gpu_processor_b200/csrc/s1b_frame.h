@@ -7,6 +7,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "s1b.h"
 
 // One burst of a frame, geocoded onto the frame's DEM grid.
@@ -40,6 +42,7 @@ struct FrameDev {
   uint64_t fill_seed;
   int32_t max_nrow_ml, max_ncol_ml, max_patches;
   int32_t deramp_rows, geo_cols;  // tile shapes the launches use
+  int32_t deramp_tiles_x, deramp_tiles_y;  // deramp tiles of the largest burst, per axis
 };
 
 // Run-time buffers of one frame launch sequence.
@@ -54,14 +57,29 @@ struct FrameIO {
   s1b_frame_pair_t *pout;
 };
 
+// Bursts of a frame by deramp load width: rows that start on 16 bytes (even
+// samples, aligned burst) take 16-byte loads.  Host side, per launch.
+struct FrameDerampSplit {
+  std::vector<int32_t> vec, scalar;
+};
+
+// A list of burst indices passed to a kernel by value.
+constexpr int kFrameListMax = 240;
+struct FrameBurstList {
+  int32_t n;
+  int32_t idx[kFrameListMax];
+};
+
 // Tile-space helpers shared by host and device.
 constexpr int kFrameDerampCols = 512;  // columns of a deramp tile (256 threads x 2)
 constexpr int kFrameGeoRows = 16;      // rows of a geocoding tile (column walk length)
 
 // Launchers (k_geo2rdr.cu, k_crossmul.cu, k_goldstein.cu).  `ctas` is the
-// persistent grid; 0 lets the launcher use the whole device.
+// persistent grid; 0 lets the launcher use the whole device (geocoding) or
+// one CTA per tile (deramp).
 int frame_launch_init(const FrameDev &d, const FrameIO &io, cudaStream_t st);
-int frame_launch_deramp(const FrameDev &d, const FrameIO &io, int rows_per_tile, int ctas, cudaStream_t st);
+int frame_launch_deramp(const FrameDev &d, const FrameIO &io, int rows_per_tile, int ctas,
+                        const FrameDerampSplit &split, cudaStream_t st);
 int frame_launch_geo2rdr(const FrameDev &d, const FrameIO &io, int cols_per_tile, int ctas, cudaStream_t st);
 int frame_max_ctas_deramp(int rows_per_tile);
 int frame_max_ctas_geo2rdr(int cols_per_tile);
