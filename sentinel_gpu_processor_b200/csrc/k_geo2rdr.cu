@@ -90,10 +90,13 @@ __global__ __launch_bounds__(256) void deramp_kernel(const __grid_constant__ s1b
 
 // ----------------------------------------------------------------- geo2rdr
 // Tile: G_TX columns x G_RY rows of the DEM window, one thread per column
-// walking down the rows.  Every pixel solves its zero-Doppler Newton on a
-// cubic orbit expansion shared by its warp; the first pixel of a column
-// starts from the warp's centre time, the others from the linear
-// extrapolation of the two pixels above.
+// walking down the rows.  Every pixel solves its zero-Doppler equation on the
+// warp's patch model (a quintic-truncated-to-cubic Doppler polynomial from
+// the cubic orbit expansion at the warp centre's zero-Doppler time): four dot
+// products per pixel, three FMA per chord-Newton step, and the range from the
+// same coefficients.  The first pixel of a column starts from the warp's
+// centre time, the others from the linear extrapolation of the two pixels
+// above.
 // Latitude terms depend only on the row: lanes 0..G_RY-1 of every warp form
 // them once and the warp shares them by shuffles (no block barrier);
 // longitude terms depend only on the column and stay in registers.  Warps
@@ -132,7 +135,7 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
   // and 2 solve two opposite corners at the same time; the three solutions
   // bound the warp's footprint in the burst, whose lines are prefetched into
   // L2 before the per-pixel solves, so the bilinear gathers hit L2.
-  __shared__ OrbitCubic s_oc[TX / 32];
+  __shared__ ZeroDopplerPatch s_zd[TX / 32];
   const int wid = tx >> 5;
   double faz = 0.0, frg = 0.0;
   if (lane < 3) {
@@ -154,7 +157,11 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
     }
     double tc = P.tmid, drc[3];
     zero_doppler(P.orbit, pc, tc, st, drc);
-    if (lane == 0) orbit_cubic(P.orbit, tc, s_oc[wid]);
+    if (lane == 0) {
+      OrbitCubic oc;
+      orbit_cubic(P.orbit, tc, oc);
+      zero_doppler_patch(oc, s_zd[wid]);
+    }
     faz = (tc - P.tstart) * prf;
     frg = (sqrt(drc[0] * drc[0] + drc[1] * drc[1] + drc[2] * drc[2]) - P.rngstart) * inv_dmrg;
   }
@@ -188,9 +195,10 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
       }
     }
   }
-  __syncwarp();  // lane 0's expansion is visible to the warp
-  const OrbitCubic &oc = s_oc[wid];
-  double t = oc.t0, tprev = 0.0, inv_fp = 0.0;
+  __syncwarp();  // lane 0's patch model is visible to the warp
+  const ZeroDopplerPatch &zd = s_zd[wid];
+  const double k4_wvl = 4.0 / P.wvl;  // two-way range phase, half-cycles per metre
+  double h = 0.0, hprev = 0.0, inv_c1 = 0.0;
   const int rmax = min(G_RY, nrow - row0);
   int16_t hn = colok && rmax > 0 ? __ldg(dem + (int64_t)row0 * pitch + col) : 0;
   int rlo = INT_MAX, rhi = -1;
@@ -199,34 +207,28 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
     const double sinlat = __shfl_sync(0xffffffffu, r_sin, r);
     const double coslat = __shfl_sync(0xffffffffu, r_cos, r);
     const double re = __shfl_sync(0xffffffffu, r_re, r);
-    const double h = (double)hn;
+    const double hgt = (double)hn;
     if (colok && r + 1 < rmax) hn = __ldg(dem + (int64_t)(row + 1) * pitch + col);
     float2 res = make_float2(0.f, 0.f);
     if (colok) {
       double p[3];
-      p[0] = (re + h) * coslat * coslon;
-      p[1] = (re + h) * coslat * sinlon;
-      p[2] = (re * (1 - kRe2D) + h) * sinlat;
-      double dr[3];
+      p[0] = (re + hgt) * coslat * coslon;
+      p[1] = (re + hgt) * coslat * sinlon;
+      p[2] = (re * (1 - kRe2D) + hgt) * sinlat;
+      const ZeroDopplerPoint q = zero_doppler_point(zd, p);
       if (r == 0) {
-        zero_doppler_cubic(oc, p, t, dr);
-        tprev = t - P.dtaz;
-        const double hh = t - oc.t0;
-        double fp = 0.0;
-        for (int i = 0; i < 3; ++i) {
-          const double a = fma(oc.j[i], hh, oc.a[i]);
-          const double v = fma(fma(0.5 * oc.j[i], hh, oc.a[i]), hh, oc.v[i]);
-          fp = fma(dr[i], a, fp);
-          fp = fma(-v, v, fp);
-        }
-        inv_fp = 1.0 / fp;
+        // the column's first point starts at the warp centre; its slope
+        // serves the whole column (f' changes by < 1e-4 over 16 rows)
+        inv_c1 = rcp_newton(q.c1);
+        hprev = -P.dtaz;
       } else {
-        const double tn = 2.0 * t - tprev;
-        tprev = t;
-        t = tn;
-        zero_doppler_cubic_chord(oc, p, t, dr, inv_fp);
+        const double hn2 = 2.0 * h - hprev;  // linear extrapolation from the two rows above
+        hprev = h;
+        h = hn2;
       }
-      const double rng = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+      const double rng = sqrt_heron(zero_doppler_solve(q, zd.c3, inv_c1, h));
+      if (r == 0) hprev = h - P.dtaz;
+      const double t = zd.t0 + h;
       const double rgoff = (rng - P.rngstart) * inv_dmrg;
       const double azoff = (t - P.tstart) * prf;
       // validity window, geo2rdr.cu:208-209
@@ -245,12 +247,11 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
         dt = tr - P.dc[0];
         const double fnc = P.dc[1] + dt * (P.dc[2] + P.dc[3] * dt);
         const double kmk = ka - P.ks;
-        const double inv = 1.0 / (ka * kmk);
+        const double inv = rcp_newton(ka * kmk);
         const double kt = ka * P.ks * (ka * inv);
         const double etaref = -fnc * (kmk * inv) - P.etac0;
         const double eta = -P.lines * P.dtaz / 2. + t - P.tstart;
         const double ed = eta - etaref;
-        const double reramp = -kPiD * kt * ed * ed;
         // bilinear interpolation of the deramped burst (geo2rdr.cu:220-237)
         const float fr = (float)(rgoff - intr), fa = (float)(azoff - inta);
         const size_t i1 = (size_t)inta * P.samples + intr;
@@ -259,8 +260,9 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
         const float2 c1 = make_float2(fmaf(fr, b2.x - b1.x, b1.x), fmaf(fr, b2.y - b1.y, b1.y));
         const float2 c2 = make_float2(fmaf(fr, b4.x - b3.x, b3.x), fmaf(fr, b4.y - b3.y, b3.y));
         const float2 v = make_float2(fmaf(fa, c2.x - c1.x, c1.x), fmaf(fa, c2.y - c1.y, c1.y));
-        // range phase and reramp (geo2rdr.cu:238-243)
-        res = cmul(v, phasor(P.k4pi_wvl * rng - reramp));
+        // range phase and reramp (geo2rdr.cu:238-243): 4 pi rng / wvl + pi kt ed^2
+        // rad, formed in half-cycles
+        res = cmul(v, phasor_pi(fma(kt, ed * ed, k4_wvl * rng)));
       }
       __stcs(out + (size_t)row * ncol + col, res);
     }

@@ -191,6 +191,92 @@ __device__ __forceinline__ void zero_doppler_cubic(const OrbitCubic &o, const do
   }
 }
 
+// Zero-Doppler model of a patch of ground points about t0, from the cubic
+// orbit expansion (x, v, a, j at t0) and u(h) = v h + a h^2/2 + j h^3/6:
+//   f(h) = (p - x(t0 + h)) . v(t0 + h) = d.u'(h) - (1/2) d|u|^2/dh,  d = p - x
+//        = c0 + c1 h + c2 h^2 + c3 h^3 + O(h^4)
+//   c0 = d.v,  c1 = d.a - |v|^2,  c2 = d.j/2 - (3/2) v.a,
+//   c3 = -(|a|^2/2 + (2/3) v.j)  (the same for every point),
+// and, since d|p - x|^2/dh = -2 f,
+//   |p - x(t0 + h)|^2 = |d|^2 - h (2 c0 + h (c1 + h ((2/3) c2 + h c3 / 2))).
+// The dropped h^4 term of f is (5/12)(a.j) h^4 < 1e-6 for |h| < 0.1 s
+// (a time error below 1e-14 s).  A point costs four dot products of d; each
+// Newton step three FMA.
+struct ZeroDopplerPatch {
+  double t0, x[3], v[3], a[3], jh[3];  // jh = j / 2
+  double vv, k2, c3;                   // |v|^2, (3/2) v.a, c3
+};
+
+__device__ __forceinline__ void zero_doppler_patch(const OrbitCubic &o, ZeroDopplerPatch &z) {
+  z.t0 = o.t0;
+  double vv = 0.0, va = 0.0, aa = 0.0, vj = 0.0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    z.x[i] = o.x[i];
+    z.v[i] = o.v[i];
+    z.a[i] = o.a[i];
+    z.jh[i] = 0.5 * o.j[i];
+    vv = fma(o.v[i], o.v[i], vv);
+    va = fma(o.v[i], o.a[i], va);
+    aa = fma(o.a[i], o.a[i], aa);
+    vj = fma(o.v[i], o.j[i], vj);
+  }
+  z.vv = vv;
+  z.k2 = 1.5 * va;
+  z.c3 = -(0.5 * aa + (2.0 / 3.0) * vj);
+}
+
+// Per-point coefficients of the patch model: c0, c1, c2 and |d|^2.
+struct ZeroDopplerPoint {
+  double c0, c1, c2, dd;
+};
+
+__device__ __forceinline__ ZeroDopplerPoint zero_doppler_point(const ZeroDopplerPatch &z, const double p[3]) {
+  const double d0 = p[0] - z.x[0], d1 = p[1] - z.x[1], d2 = p[2] - z.x[2];
+  ZeroDopplerPoint q;
+  q.c0 = fma(d0, z.v[0], fma(d1, z.v[1], d2 * z.v[2]));
+  q.c1 = fma(d0, z.a[0], fma(d1, z.a[1], fma(d2, z.a[2], -z.vv)));
+  q.c2 = fma(d0, z.jh[0], fma(d1, z.jh[1], fma(d2, z.jh[2], -z.k2)));
+  q.dd = fma(d0, d0, fma(d1, d1, d2 * d2));
+  return q;
+}
+
+// Chord Newton on f(h) = 0 from the seed h with the fixed reciprocal slope
+// inv_c1 (= 1 / f'(0)); stops as the reference's iteration does, once a step
+// is below 5e-9 s (csrc/src/orbit.cu:259-274).  Returns the squared range.
+__device__ __forceinline__ double zero_doppler_solve(const ZeroDopplerPoint &q, double c3, double inv_c1,
+                                                     double &h) {
+  for (int it = 0; it < 51; ++it) {
+    const double f = fma(fma(fma(c3, h, q.c2), h, q.c1), h, q.c0);
+    const double step = f * inv_c1;
+    h -= step;
+    if (fabs(step) < 5.0e-9) break;
+  }
+  return fma(-h, fma(fma(fma(0.5 * c3, h, (2.0 / 3.0) * q.c2), h, q.c1), h, 2.0 * q.c0), q.dd);
+}
+
+// sqrt(s) for normal s in float range, to FP64 accuracy: Heron's method
+// (Newton on r^2 = s) from the FP32 estimate y ~ 1/sqrt(s) with y held fixed,
+// r <- r + (s - r^2) y / 2.  With y = (1 + e)/sqrt(s), r = s y has relative
+// error e, the first step leaves 1.5 e^2 and the second 1.5 e^3 (e < 3e-7:
+// below 1e-19), so the result is within an ulp of the rounded square root.
+__device__ __forceinline__ double sqrt_heron(double s) {
+  const float y = rsqrtf((float)s);
+  const double hy = 0.5 * (double)y;
+  double r = s * (double)y;
+  r = fma(fma(-r, r, s), hy, r);
+  return fma(fma(-r, r, s), hy, r);
+}
+
+// 1 / x for normal x in float range, to FP64 accuracy: Newton's iteration
+// r <- r + r (1 - x r) from an FP32 estimate; each step squares the relative
+// error (3e-7 -> 1e-13 -> 1e-26).
+__device__ __forceinline__ double rcp_newton(double x) {
+  double r = (double)__fdividef(1.0f, (float)x);
+  r = fma(r, fma(-x, r, 1.0), r);
+  return fma(r, fma(-x, r, 1.0), r);
+}
+
 // zero_doppler_cubic with a fixed reciprocal derivative (chord Newton).
 __device__ __forceinline__ void zero_doppler_cubic_chord(const OrbitCubic &o, const double p[3], double &t,
                                                          double dr[3], double inv_fp) {
