@@ -375,8 +375,9 @@ int s1b_stitch(const s1b_stitch_burst_t *bursts, int32_t n, const void *data, in
 /* ------------------------------------------------------------ batched frame
  * All burst pairs of a frame (e.g. 3 subswaths x 9 bursts of uneven size)
  * processed with one launch per stage over a per-burst descriptor table:
- * deramp and geocoding are persistent kernels over the flat tile space of
- * every burst; the crossmul box of each pair is formed on the device from the
+ * deramp and geocoding run one CTA per tile over (tile x, tile y, burst)
+ * grids, or as persistent kernels over the flat tile space of every burst
+ * (the autotuner picks); the crossmul box of each pair is formed on the device from the
  * crop rows, so a run has no host synchronisation and can be captured in a
  * CUDA graph.  Replaces running geo2rdr per burst, crossmul_daemon and
  * goldstein per pair (csrc/src/geo2rdr.cu:316-651, crossmul_daemon.cu:566-975,
@@ -427,7 +428,8 @@ int s1b_frame_run(s1b_frame_t *frame, const void *slc, const int16_t *dem, int64
                   void *workspace, void *ifg, float *amp1, float *amp2, float *coh, void *filt,
                   s1b_frame_pair_t *pairs, void *stream);
 
-/* Autotuner: times the candidate tile shapes and persistent grid sizes of
+/* Autotuner: times the candidate tile shapes and grids (one CTA per tile, or
+ * persistent grids of 1..n CTAs per SM) of
  * the deramp and geocoding stages on these buffers (`reps` runs each, CUDA
  * events on `stream`), keeps the fastest in the frame for later runs and
  * synchronises the stream.  Not capturable.  Every candidate produces the
@@ -444,7 +446,7 @@ int s1b_frame_profile(s1b_frame_t *frame, const void *slc, const int16_t *dem, i
                       s1b_frame_pair_t *pairs, float *stage_ms, void *stream);
 
 /* Current tuning: [deramp rows per tile, deramp CTAs, geocoding columns per
- * tile, geocoding CTAs] (CTAs 0 = whole device). */
+ * tile, geocoding CTAs] (CTAs 0 = one CTA per tile, else a persistent grid). */
 int s1b_frame_tuning(const s1b_frame_t *frame, int32_t tuning[4]);
 /* Set the tuning by hand (validated; S1B_ERR_UNSUPPORTED for a shape not built). */
 int s1b_frame_set_tuning(s1b_frame_t *frame, const int32_t tuning[4]);

@@ -312,10 +312,13 @@ class RadarChain:
         return 6
 
 
+FRAME_LIST_MAX = 240  # bursts per deramp launch (kFrameListMax, csrc/s1b_frame.h)
+
+
 class BatchedFrameChain:
     """All burst pairs of a frame through one batched launch sequence
-    (``s1b_frame_run``): deramp and geocoding as persistent kernels over every
-    burst, the crossmul box of each pair formed on the device, crossmul and
+    (``s1b_frame_run``): deramp and geocoding over every burst (one CTA per
+    tile, or persistent grids; the autotuner picks), the crossmul box of each pair formed on the device, crossmul and
     Goldstein over all pairs.  No host synchronisation inside a run, so it is
     captured in a CUDA graph (``capture``/``replay``).  Per-pair products are
     those of :class:`FrameChain` (same kernels, same order of operations).
@@ -364,10 +367,11 @@ class BatchedFrameChain:
         self.pairs_dev = torch.zeros(self.n_pairs * self.pair_size, dtype=torch.uint8, device=self.dev)
         self.pairs_host = torch.empty(self.n_pairs * self.pair_size, dtype=torch.uint8,
                                       pin_memory=torch.cuda.is_available())
-        views = []
+        views, self.burst_offsets = [], []
         for b, p in enumerate(plans):
             off = ctypes.c_int64()
             _lib.check(lib.s1b_frame_burst_offset(handle, b, ctypes.byref(off)), "s1b_frame_burst_offset")
+            self.burst_offsets.append(off.value)
             views.append(self.slc[off.value:off.value + p.lines * p.samples].view(p.lines, p.samples))
         self.ref_views, self.sec_views = views[0::2], views[1::2]
         self.slots = []
@@ -485,8 +489,18 @@ class BatchedFrameChain:
         return res
 
     def launches_per_step(self):
-        # init, deramp, geocoding, box, crossmul, Goldstein patches, Goldstein gather
-        return 7
+        """Kernels one run launches: init, geocoding, box, crossmul, Goldstein
+        patches and gather, plus the deramp: one persistent launch, or one
+        CTA-per-tile launch per load width (16-byte rows or not) and per list
+        of up to FRAME_LIST_MAX bursts."""
+        t = self.tuning()
+        if t["deramp_ctas"]:
+            return 7
+        base = self.slc.data_ptr()
+        vec = sum(1 for p, off in zip(self.plans, self.burst_offsets)
+                  if p.samples % 2 == 0 and (base + 8 * off) % 16 == 0)
+        per = FRAME_LIST_MAX
+        return 6 + -(-vec // per) + -(-(len(self.plans) - vec) // per)
 
     def geo_pixels(self):
         return [p.nrow * p.ncol for p in self.plans]

@@ -1,9 +1,10 @@
 // Batched frame: host side of s1b_frame_* (descriptor tables, workspace and
 // product layout, the launch sequence of one run, the autotuner).
 //
-// A run is seven launches on one stream with no host synchronisation:
-//   init (crop rows), deramp of every burst, geocoding of every burst
-//   (persistent kernels over the flat tile space of the frame), per-pair box
+// A run is six to eight launches on one stream with no host synchronisation:
+//   init (crop rows), deramp of every burst (one launch per load width),
+//   geocoding of every burst (one CTA per tile, or persistent kernels over
+//   the flat tile space of the frame), per-pair box
 //   and headers from the crop rows, crossmul + looks of every pair, Goldstein
 //   patches and overlap-add of every pair.
 // The reference runs geo2rdr once per burst and crossmul_daemon / goldstein
@@ -46,7 +47,7 @@ int cuda_fail(cudaError_t e) { return s1b_fail(S1B_ERR_CUDA, cudaGetErrorString(
 // Flat tile prefixes of the current tile shapes, uploaded to the device.
 int set_tiles(s1b_frame *f) {
   int64_t dt = 0, gt = 0;
-  int32_t dtx = 0, dty = 0;
+  int32_t dtx = 0, dty = 0, gtx = 0, gty = 0;
   const int rows = f->tuning[0], cols = f->tuning[2];
   for (size_t b = 0; b < f->bursts.size(); ++b) {
     FrameBurst &fb = f->bursts[b];
@@ -57,7 +58,10 @@ int set_tiles(s1b_frame *f) {
     dt += (int64_t)tx * ty;
     dtx = std::max(dtx, tx);
     dty = std::max(dty, ty);
-    gt += (int64_t)((fb.ncol + cols - 1) / cols) * ((fb.nrow + kFrameGeoRows - 1) / kFrameGeoRows);
+    const int32_t gx = (fb.ncol + cols - 1) / cols, gy = (fb.nrow + kFrameGeoRows - 1) / kFrameGeoRows;
+    gt += (int64_t)gx * gy;
+    gtx = std::max(gtx, gx);
+    gty = std::max(gty, gy);
   }
   f->dev.n_deramp_tiles = dt;
   f->dev.n_geo_tiles = gt;
@@ -65,6 +69,8 @@ int set_tiles(s1b_frame *f) {
   f->dev.deramp_tiles_x = dtx;
   f->dev.deramp_tiles_y = dty;
   f->dev.geo_cols = cols;
+  f->dev.geo_tiles_x = gtx;
+  f->dev.geo_tiles_y = gty;
   cudaError_t e = cudaMemcpy(f->d_bursts, f->bursts.data(), f->bursts.size() * sizeof(FrameBurst),
                              cudaMemcpyHostToDevice);
   return e == cudaSuccess ? S1B_OK : cuda_fail(e);
@@ -340,10 +346,9 @@ extern "C" int s1b_frame_autotune(s1b_frame_t *f, const void *slc, const int16_t
     for (int shape : shapes[stage]) {
       const int full = stage == 0 ? frame_max_ctas_deramp(shape) : frame_max_ctas_geo2rdr(shape);
       const int per_sm = sms > 0 ? full / sms : 0;
-      // persistent grids of 1..per_sm CTAs per SM; 0 = all resident
-      // (geocoding) or one CTA per tile (deramp, tried first)
-      for (int j = stage == 0 ? 0 : 1; j <= per_sm && !s; ++j) {
-        const int ctas = stage == 0 ? j * sms : (j == per_sm ? 0 : j * sms);
+      // one CTA per tile (0), then persistent grids of 1..per_sm CTAs per SM
+      for (int j = 0; j <= per_sm && !s; ++j) {
+        const int ctas = j * sms;
         float ms = 0.f;
         s = time_stage(stage, shape, ctas, ms);
         if (!s && ms < best) {

@@ -401,6 +401,21 @@ __global__ __launch_bounds__(TX) void frame_geo2rdr_kernel(const FrameDev d, con
   }
 }
 
+// One CTA per tile: blockIdx.z is the burst, (x, y) the tile in its DEM
+// window; the plan is read through the table (uniform, L1-resident loads)
+// instead of a shared-memory copy, which keeps the single-burst register
+// budget.  The grid spans the largest window; CTAs past a smaller one return.
+template <int TX>
+__global__ __launch_bounds__(TX) void frame_geo2rdr_grid_kernel(const FrameDev d, const FrameIO io) {
+  const int b = blockIdx.z;
+  const s1b_burst_plan_t &sp = d.plans[b];
+  const FrameBurst &fb = d.bursts[b];
+  if ((int)blockIdx.x * TX >= fb.ncol || (int)blockIdx.y * G_RY >= fb.nrow) return;
+  const int16_t *dem = io.dem + (int64_t)sp.win_top * io.dem_pitch + sp.win_left;
+  geo2rdr_tile<TX>(sp, dem, io.dem_pitch, io.work + fb.der_off, io.work + fb.geo_off, d.rows + 2 * b,
+                   fb.nrow, fb.ncol, blockIdx.x, blockIdx.y);
+}
+
 template <typename K>
 int resident_ctas(K kernel, int threads) {
   int dev = 0, sms = 0, per_sm = 0;
@@ -573,7 +588,16 @@ int frame_launch_geo2rdr(const FrameDev &d, const FrameIO &io, int cols, int cta
   const int full = frame_max_ctas_geo2rdr(cols);
   if (full <= 0) return s1b_fail(S1B_ERR_UNSUPPORTED, "frame geo2rdr: tile columns must be 64, 128 or 256");
   if (d.n_geo_tiles == 0) return S1B_OK;
-  long long g = ctas > 0 && ctas < full ? ctas : full;
+  if (ctas == 0) {  // one CTA per tile
+    const dim3 grid((unsigned)d.geo_tiles_x, (unsigned)d.geo_tiles_y, (unsigned)d.n_bursts);
+    switch (cols) {
+      case 64: frame_geo2rdr_grid_kernel<64><<<grid, 64, 0, st>>>(d, io); break;
+      case 128: frame_geo2rdr_grid_kernel<128><<<grid, 128, 0, st>>>(d, io); break;
+      default: frame_geo2rdr_grid_kernel<256><<<grid, 256, 0, st>>>(d, io); break;
+    }
+    return s1b_launch_status();
+  }
+  long long g = ctas < full ? ctas : full;
   if (g > d.n_geo_tiles) g = d.n_geo_tiles;
   switch (cols) {
     case 64: frame_geo2rdr_kernel<64><<<(unsigned)g, 64, 0, st>>>(d, io); break;

@@ -43,6 +43,7 @@ struct FrameDev {
   int32_t max_nrow_ml, max_ncol_ml, max_patches;
   int32_t deramp_rows, geo_cols;  // tile shapes the launches use
   int32_t deramp_tiles_x, deramp_tiles_y;  // deramp tiles of the largest burst, per axis
+  int32_t geo_tiles_x, geo_tiles_y;        // geocoding tiles of the largest window, per axis
 };
 
 // Run-time buffers of one frame launch sequence.
@@ -75,8 +76,7 @@ constexpr int kFrameDerampCols = 512;  // columns of a deramp tile (256 threads 
 constexpr int kFrameGeoRows = 16;      // rows of a geocoding tile (column walk length)
 
 // Launchers (k_geo2rdr.cu, k_crossmul.cu, k_goldstein.cu).  `ctas` is the
-// persistent grid; 0 lets the launcher use the whole device (geocoding) or
-// one CTA per tile (deramp).
+// persistent grid; 0 launches one CTA per tile over (tile x, tile y, burst).
 int frame_launch_init(const FrameDev &d, const FrameIO &io, cudaStream_t st);
 int frame_launch_deramp(const FrameDev &d, const FrameIO &io, int rows_per_tile, int ctas,
                         const FrameDerampSplit &split, cudaStream_t st);
