@@ -171,6 +171,21 @@ int s1b_orbit_eval_host(const s1b_orbit_poly_t *orbit, const double *t, int64_t 
  * (in == out allowed).  Phase in FP64, reduced mod 2 pi, FP32 rotation. */
 int s1b_deramp(const s1b_burst_plan_t *plan, const void *in, void *out, void *stream);
 
+/* Sample types of SLC input: complex64 (what the reference's geo2rdr reads
+ * from its stdin pipe) or complex int16 (re, im int16 pairs: the sample type
+ * of the Sentinel-1 measurement TIFF, which the reference widens to complex64
+ * on the host with GDAL before piping it, s1proc/sentinel_scene.py:164-207). */
+#define S1B_SAMPLES_C64 0
+#define S1B_SAMPLES_CI16 1
+
+/* s1b_deramp on complex int16 input: in int16 [lines * samples * 2] device
+ * (re, im), out complex64 [lines * samples] device.  The widening to float is
+ * exact, so the result equals s1b_deramp on the widened complex64 burst bit
+ * for bit.  Ingest boundary: replaces the host-side widening and the 8-byte
+ * samples of the stdin pipe (s1proc/sentinel_scene.py:164-207,
+ * geo2rdr.cu:545-557) with 4-byte samples widened on the device. */
+int s1b_deramp_ci16(const s1b_burst_plan_t *plan, const void *in, void *out, void *stream);
+
 /* Geocode a deramped burst onto the plan's DEM window: per DEM pixel FP64
  * llh->ECEF, zero-Doppler Newton, validity window, bilinear interpolation,
  * reramp and range phase.  Replaces reproject + find_nonzero_rows,
@@ -398,7 +413,7 @@ typedef struct {
 
 typedef struct {
   size_t workspace_bytes;   /* device scratch: deramped bursts, geocoded windows, patches */
-  int64_t slc_elems;        /* complex64 elements of the SLC buffer: bursts back to back */
+  int64_t slc_elems;        /* samples of the SLC buffer: bursts back to back */
   int64_t product_elems;    /* elements of each product array (all pairs' slots) */
   int32_t max_nrow_ml, max_ncol_ml;
 } s1b_frame_sizes_t;
@@ -414,12 +429,18 @@ void s1b_frame_destroy(s1b_frame_t *frame);
 int s1b_frame_sizes(const s1b_frame_t *frame, s1b_frame_sizes_t *sizes);
 /* Element offset of burst b in the SLC buffer (lines * samples of the bursts before it). */
 int s1b_frame_burst_offset(const s1b_frame_t *frame, int32_t burst, int64_t *slc_off);
+/* Sample type of the SLC buffer later runs read: S1B_SAMPLES_C64 (the
+ * default; 8 bytes per element) or S1B_SAMPLES_CI16 (4 bytes per element,
+ * widened in the deramp stage).  Offsets and slc_elems count samples either
+ * way.  Products are identical for the same integer-valued samples. */
+int s1b_frame_set_sample_format(s1b_frame_t *frame, int32_t format);
 /* Slot of pair k in the product arrays: first element and capacity. */
 int s1b_frame_pair_slot(const s1b_frame_t *frame, int32_t pair, int64_t *ml_off, int32_t *max_nrow_ml,
                         int32_t *max_ncol_ml);
 
 /* Enqueue one frame run on `stream` (no host synchronisation).
- * slc: complex64 [slc_elems] device; dem: int16 RSC grid, row pitch in
+ * slc: [slc_elems] samples of the frame's sample format (complex64 unless
+ * set otherwise) device; dem: int16 RSC grid, row pitch in
  * elements; workspace: workspace_bytes, 16-byte aligned; ifg/filt complex64
  * and amp1/amp2/coh float32 [product_elems] (amp1/amp2/coh may be NULL);
  * pairs: s1b_frame_pair_t [n_pairs] device.  Pair k's products are row-major

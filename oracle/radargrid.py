@@ -131,7 +131,9 @@ def box_coherence(ref, sec, win=5):
         return (c[win:win + n0, win:win + n1] - c[:n0, win:win + n1] - c[win:win + n0, :n1] + c[:n0, :n1])
 
     num = np.abs(box(np.conj(r) * s))
-    den = np.sqrt(box(np.abs(r) ** 2).real * box(np.abs(s) ** 2).real)
+    # the cumulative-sum differences can leave tiny negative residues where a
+    # box is all zeros
+    den = np.sqrt(np.maximum(box(np.abs(r) ** 2).real, 0) * np.maximum(box(np.abs(s) ** 2).real, 0))
     with np.errstate(invalid="ignore", divide="ignore"):
         g = np.where(den > 0, num / np.where(den > 0, den, 1), 0.0)
     return g

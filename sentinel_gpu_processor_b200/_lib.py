@@ -24,6 +24,8 @@ S1B_ERR_UNSUPPORTED = 6
 MAX_STATE_VECTORS = 64
 S1B_INTERP_BILINEAR = 0
 S1B_INTERP_SINC8 = 1
+S1B_SAMPLES_C64 = 0
+S1B_SAMPLES_CI16 = 1
 MAX_WIN = MAX_STATE_VECTORS - 3
 
 
@@ -125,6 +127,7 @@ _SIGNATURES = {
     "s1b_orbit_eval_host": (c_int, [POINTER(OrbitPoly), POINTER(c_double), c_int64, POINTER(c_double),
                                     POINTER(c_double)]),
     "s1b_deramp": (c_int, [POINTER(BurstPlan), c_void_p, c_void_p, c_void_p]),
+    "s1b_deramp_ci16": (c_int, [POINTER(BurstPlan), c_void_p, c_void_p, c_void_p]),
     "s1b_geo2rdr": (c_int, [POINTER(BurstPlan), c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p]),
     "s1b_zero_doppler": (c_int, [POINTER(OrbitPoly), c_void_p, c_int64, c_double, c_void_p, c_void_p, c_void_p]),
     "s1b_llh2xyz": (c_int, [c_void_p, c_void_p, c_int64, c_void_p]),
@@ -171,6 +174,7 @@ _SIGNATURES = {
     "s1b_adjoint_run": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                 c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
     "s1b_frame_set_tuning": (c_int, [c_void_p, POINTER(c_int32)]),
+    "s1b_frame_set_sample_format": (c_int, [c_void_p, c_int32]),
 }
 
 _lib = None

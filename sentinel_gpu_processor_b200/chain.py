@@ -324,12 +324,20 @@ class BatchedFrameChain:
     those of :class:`FrameChain` (same kernels, same order of operations).
 
     The SLCs live back to back in one device buffer; ``ref_views``/``sec_views``
-    are the per-burst views to fill.  ``autotune`` picks the deramp and
-    geocoding tile shapes and grid sizes on the actual frame.
+    are the per-burst views to fill.  ``sample_format="ci16"`` keeps them as
+    the measurement TIFF's complex int16 samples (int16 [lines, samples, 2],
+    half the bytes to move and to read), widened in the deramp stage; the
+    products equal those of the complex64 buffer holding the same values.
+    ``autotune`` picks the deramp and geocoding tile shapes and grid sizes on
+    the actual frame.
     """
 
-    def __init__(self, refs, secs, rsc, rowlook, collook, alpha, n_win=32, device="cuda", fill_seed=0):
+    def __init__(self, refs, secs, rsc, rowlook, collook, alpha, n_win=32, device="cuda", fill_seed=0,
+                 sample_format="c64"):
         import ctypes
+        if sample_format not in ("c64", "ci16"):
+            raise ValueError("sample_format must be 'c64' (complex64) or 'ci16' (complex int16)")
+        self.sample_format = sample_format
         self.dev = torch.device(device)
         self.rowlook, self.collook, self.alpha, self.n_win = int(rowlook), int(collook), float(alpha), int(n_win)
         self.fill_seed = int(fill_seed)
@@ -352,10 +360,15 @@ class BatchedFrameChain:
                                             self.n_win, self.alpha, self.fill_seed, ctypes.byref(handle)),
                        "s1b_frame_create")
         self._handle = handle
+        if sample_format == "ci16":
+            _lib.check(lib.s1b_frame_set_sample_format(handle, _lib.S1B_SAMPLES_CI16), "s1b_frame_set_sample_format")
         sz = _lib.FrameSizes()
         _lib.check(lib.s1b_frame_sizes(handle, ctypes.byref(sz)), "s1b_frame_sizes")
         self.sizes = sz
-        self.slc = torch.empty(int(sz.slc_elems), dtype=torch.complex64, device=self.dev)
+        if sample_format == "ci16":
+            self.slc = torch.empty((int(sz.slc_elems), 2), dtype=torch.int16, device=self.dev)
+        else:
+            self.slc = torch.empty(int(sz.slc_elems), dtype=torch.complex64, device=self.dev)
         self.workspace = torch.empty(int(sz.workspace_bytes), dtype=torch.uint8, device=self.dev)
         n = int(sz.product_elems)
         self.ifg = torch.empty(n, dtype=torch.complex64, device=self.dev)
@@ -372,7 +385,8 @@ class BatchedFrameChain:
             off = ctypes.c_int64()
             _lib.check(lib.s1b_frame_burst_offset(handle, b, ctypes.byref(off)), "s1b_frame_burst_offset")
             self.burst_offsets.append(off.value)
-            views.append(self.slc[off.value:off.value + p.lines * p.samples].view(p.lines, p.samples))
+            v = self.slc[off.value:off.value + p.lines * p.samples]
+            views.append(v.view(p.lines, p.samples, 2) if sample_format == "ci16" else v.view(p.lines, p.samples))
         self.ref_views, self.sec_views = views[0::2], views[1::2]
         self.slots = []
         for k in range(self.n_pairs):
@@ -497,8 +511,9 @@ class BatchedFrameChain:
         if t["deramp_ctas"]:
             return 7
         base = self.slc.data_ptr()
+        es = 4 if self.sample_format == "ci16" else 8
         vec = sum(1 for p, off in zip(self.plans, self.burst_offsets)
-                  if p.samples % 2 == 0 and (base + 8 * off) % 16 == 0)
+                  if p.samples % 2 == 0 and (base + es * off) % (2 * es) == 0)
         per = FRAME_LIST_MAX
         return 6 + -(-vec // per) + -(-(len(self.plans) - vec) // per)
 

@@ -3,6 +3,9 @@ arguments, stdout lines, exit codes and files, so that s1proc finds them
 through ``get_bin_path`` unchanged (the stubs in ``bin/``):
 
     geo2rdr dbname slcoutfile [slcinfile] [--stdin] [--gpu N]          geo2rdr.cu:704-734
+            [--tiff FILE[::MEMBER]]  (extension: bursts straight from the
+            measurement TIFF, or a member of the SAFE zip, instead of the
+            pipe s1proc/sentinel_scene.py:164-207, 419-437 feeds)
     crossmul_daemon --rowlook R --collook C [--out-float] [--verbose]
                     --tasks-file F [--io-workers .. --max-slots]       crossmul_daemon.cu:1744-1911
     crossmul input_file rowlook collook out_float [--gpu N]            crossmul.cu:285-298
@@ -22,6 +25,8 @@ import numpy as np
 
 USAGE_GEO2RDR = ("Usage: geo2rdr dbname slcoutfile [slcinfile] [--stdin] [--gpu DEVICE_ID]\n"
                  "  --stdin  Read original SLC burst data from stdin")
+# Extension of this build (not printed, so the usage text stays the reference's):
+#   --tiff FILE[::MEMBER]  read the bursts from a measurement TIFF (or a member of a zip)
 USAGE_CROSSMUL = "Usage: crossmul input_file rowlook collook out_float [--gpu DEVICE_ID]"
 USAGE_GOLDSTEIN = "Usage: goldstein in_str nrow ncol n_win alpha [out_str] [--gpu DEVICE_ID]"
 TUNING = ("--io-workers", "--cpu-workers", "--streams-per-gpu", "--gpu-workers", "--max-slots")
@@ -58,12 +63,19 @@ def geo2rdr_main(argv=None, stdin=None):
     _set_gpu(argv)
     db, out = argv[1], argv[2]
     slcin = None
-    if len(argv) > 3 and argv[3] not in ("--stdin", "--gpu", "-g"):
+    if len(argv) > 3 and argv[3] not in ("--stdin", "--gpu", "-g", "--tiff"):
         slcin = argv[3]
+    tiff_arg = _get_arg(argv, "--tiff", None)
     from .geo2rdr import geo2rdr_files
     try:
-        geo2rdr_files(db, out, slcin, stream=(stdin or sys.stdin.buffer) if use_stdin else None)
-    except EOFError as e:
+        if tiff_arg is not None:
+            from .ingest import MeasurementTiff
+            path, _, member = tiff_arg.partition("::")
+            with MeasurementTiff(path, member or None) as tif:
+                geo2rdr_files(db, out, tiff=tif)
+        else:
+            geo2rdr_files(db, out, slcin, stream=(stdin or sys.stdin.buffer) if use_stdin else None)
+    except (EOFError, ValueError, OSError, KeyError) as e:
         print(f"Error: {e}", file=sys.stderr)
         return 1
     return 0

@@ -95,7 +95,7 @@ int make_io(s1b_frame *f, const void *slc, const int16_t *dem, int64_t dem_pitch
     return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_frame_run: workspace must be 16-byte aligned");
   for (const s1b_burst_plan_t &p : f->plans)
     if (dem_pitch < p.win_right) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_frame_run: dem_pitch below a window");
-  io.slc = (const float2 *)slc;
+  io.slc = slc;
   io.dem = dem;
   io.dem_pitch = dem_pitch;
   io.work = (float2 *)workspace;
@@ -108,8 +108,10 @@ int make_io(s1b_frame *f, const void *slc, const int16_t *dem, int64_t dem_pitch
   f->split.vec.clear();
   f->split.scalar.clear();
   for (size_t b = 0; b < f->bursts.size(); ++b) {
+    // two samples per load: 16 bytes (complex64) or 8 (complex int16)
+    const size_t es = f->dev.sample_format == S1B_SAMPLES_CI16 ? 4 : 8;
     const bool vec = f->plans[b].samples % 2 == 0 &&
-                     reinterpret_cast<uintptr_t>(io.slc + f->bursts[b].slc_off) % 16 == 0 &&
+                     (reinterpret_cast<uintptr_t>(io.slc) + es * (uint64_t)f->bursts[b].slc_off) % (2 * es) == 0 &&
                      reinterpret_cast<uintptr_t>(io.work + f->bursts[b].der_off) % 16 == 0;
     (vec ? f->split.vec : f->split.scalar).push_back((int32_t)b);
   }
@@ -287,6 +289,14 @@ extern "C" int s1b_frame_run(s1b_frame_t *f, const void *slc, const int16_t *dem
 extern "C" int s1b_frame_tuning(const s1b_frame_t *f, int32_t tuning[4]) {
   if (!f || !tuning) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_frame_tuning: null argument");
   std::memcpy(tuning, f->tuning, sizeof(f->tuning));
+  return S1B_OK;
+}
+
+extern "C" int s1b_frame_set_sample_format(s1b_frame_t *f, int32_t format) {
+  if (!f) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_frame_set_sample_format: null frame");
+  if (format != S1B_SAMPLES_C64 && format != S1B_SAMPLES_CI16)
+    return s1b_fail(S1B_ERR_UNSUPPORTED, "s1b_frame_set_sample_format: S1B_SAMPLES_C64 or S1B_SAMPLES_CI16");
+  f->dev.sample_format = format;
   return S1B_OK;
 }
 

@@ -27,11 +27,31 @@ constexpr double kRe2D = 0.00669437999015;
 
 // ------------------------------------------------------------------ deramp
 // Tile: 256 threads x 2 columns = 512 columns, ROWS rows.  Per-column TOPS
-// coefficients are formed once per thread and reused down the rows.
+// coefficients are formed once per thread and reused down the rows.  Input
+// samples are complex64 (float2) or the measurement TIFF's complex int16
+// (short2: re, im), widened exactly to float in registers.
 constexpr int DERAMP_ROWS = 16;
 
-template <bool kVec, int ROWS>
-__device__ __forceinline__ void deramp_tile(const s1b_burst_plan_t &P, const float2 *__restrict__ in,
+// Two adjacent samples from an address aligned to their size (16 bytes for
+// complex64, 8 for complex int16), streamed.
+__device__ __forceinline__ void load_pair(const float2 *p, float2 &a0, float2 &a1) {
+  const float4 v = __ldcs(reinterpret_cast<const float4 *>(p));
+  a0 = make_float2(v.x, v.y);
+  a1 = make_float2(v.z, v.w);
+}
+__device__ __forceinline__ void load_pair(const short2 *p, float2 &a0, float2 &a1) {
+  const short4 v = __ldcs(reinterpret_cast<const short4 *>(p));
+  a0 = make_float2((float)v.x, (float)v.y);
+  a1 = make_float2((float)v.z, (float)v.w);
+}
+__device__ __forceinline__ float2 load_one(const float2 *p) { return __ldcs(p); }
+__device__ __forceinline__ float2 load_one(const short2 *p) {
+  const short2 v = __ldcs(p);
+  return make_float2((float)v.x, (float)v.y);
+}
+
+template <bool kVec, int ROWS, typename TIn>
+__device__ __forceinline__ void deramp_tile(const s1b_burst_plan_t &P, const TIn *__restrict__ in,
                                             float2 *__restrict__ out, int tile_x, int tile_y) {
   const int S = P.samples, L = P.lines;
   const int c0 = (tile_x * 256 + threadIdx.x) * 2;
@@ -61,12 +81,10 @@ __device__ __forceinline__ void deramp_tile(const s1b_burst_plan_t &P, const flo
     const size_t base = (size_t)r * S + c0;
     float2 a0, a1;
     if (kVec) {
-      const float4 v = __ldcs(reinterpret_cast<const float4 *>(in + base));
-      a0 = make_float2(v.x, v.y);
-      a1 = make_float2(v.z, v.w);
+      load_pair(in + base, a0, a1);
     } else {
-      a0 = __ldcs(in + base);
-      a1 = two ? __ldcs(in + base + 1) : make_float2(0.f, 0.f);
+      a0 = load_one(in + base);
+      a1 = two ? load_one(in + base + 1) : make_float2(0.f, 0.f);
     }
     const double d0 = eta - etaref[0];
     const double d1 = eta - etaref[1];
@@ -81,9 +99,9 @@ __device__ __forceinline__ void deramp_tile(const s1b_burst_plan_t &P, const flo
   }
 }
 
-template <bool kVec>
+template <bool kVec, typename TIn>
 __global__ __launch_bounds__(256) void deramp_kernel(const __grid_constant__ s1b_burst_plan_t P,
-                                                     const float2 *__restrict__ in,
+                                                     const TIn *__restrict__ in,
                                                      float2 *__restrict__ out) {
   deramp_tile<kVec, DERAMP_ROWS>(P, in, out, blockIdx.x, blockIdx.y);
 }
@@ -330,7 +348,7 @@ __device__ __forceinline__ void frame_load_plan(s1b_burst_plan_t &sp, const s1b_
 
 // Deramp reads a dozen plan fields once per tile (uniform loads), so it
 // takes the plan from the table directly.
-template <int ROWS>
+template <int ROWS, typename TIn>
 __global__ __launch_bounds__(256, 4) void frame_deramp_kernel(const FrameDev d, const FrameIO io) {
   for (int64_t idx = blockIdx.x; idx < d.n_deramp_tiles; idx += gridDim.x) {
     const int b = frame_burst_of<false>(d, idx);
@@ -339,9 +357,9 @@ __global__ __launch_bounds__(256, 4) void frame_deramp_kernel(const FrameDev d, 
     const int tiles_x = (sp.samples + kFrameDerampCols - 1) / kFrameDerampCols;
     const int64_t local = idx - fb.deramp_tile0;
     const int ty = (int)(local / tiles_x), tx = (int)(local - (int64_t)ty * tiles_x);
-    const float2 *in = io.slc + fb.slc_off;
+    const TIn *in = static_cast<const TIn *>(io.slc) + fb.slc_off;
     float2 *out = io.work + fb.der_off;
-    const bool vec = sp.samples % 2 == 0 && (reinterpret_cast<uintptr_t>(in) % 16) == 0 &&
+    const bool vec = sp.samples % 2 == 0 && (reinterpret_cast<uintptr_t>(in) % (2 * sizeof(TIn))) == 0 &&
                      (reinterpret_cast<uintptr_t>(out) % 16) == 0;
     if (vec)
       deramp_tile<true, ROWS>(sp, in, out, tx, ty);
@@ -355,17 +373,18 @@ __global__ __launch_bounds__(256, 4) void frame_deramp_kernel(const FrameDev d, 
 // burst; CTAs past a smaller one return at once.  No tile search and no
 // persistent loop, so each instantiation keeps the single-burst register
 // budget and the hardware keeps every SM full of streaming CTAs.
-template <bool kVec, int ROWS>
+template <bool kVec, int ROWS, typename TIn>
 __global__ __launch_bounds__(256) void frame_deramp_grid_kernel(const FrameDev d, const FrameIO io,
                                                                 const __grid_constant__ FrameBurstList list) {
   const int b = list.idx[blockIdx.z];
   const s1b_burst_plan_t &sp = d.plans[b];
   if ((int)blockIdx.x * kFrameDerampCols >= sp.samples || (int)blockIdx.y * ROWS >= sp.lines) return;
   const FrameBurst &fb = d.bursts[b];
-  deramp_tile<kVec, ROWS>(sp, io.slc + fb.slc_off, io.work + fb.der_off, blockIdx.x, blockIdx.y);
+  deramp_tile<kVec, ROWS>(sp, static_cast<const TIn *>(io.slc) + fb.slc_off, io.work + fb.der_off, blockIdx.x,
+                          blockIdx.y);
 }
 
-template <bool kVec>
+template <bool kVec, typename TIn>
 void launch_deramp_grid(const FrameDev &d, const FrameIO &io, int rows, const int32_t *bursts, int n,
                         cudaStream_t st) {
   for (int k0 = 0; k0 < n; k0 += kFrameListMax) {
@@ -374,9 +393,9 @@ void launch_deramp_grid(const FrameDev &d, const FrameIO &io, int rows, const in
     for (int k = 0; k < list.n; ++k) list.idx[k] = bursts[k0 + k];
     const dim3 grid((unsigned)d.deramp_tiles_x, (unsigned)d.deramp_tiles_y, (unsigned)list.n);
     switch (rows) {
-      case 8: frame_deramp_grid_kernel<kVec, 8><<<grid, 256, 0, st>>>(d, io, list); break;
-      case 16: frame_deramp_grid_kernel<kVec, 16><<<grid, 256, 0, st>>>(d, io, list); break;
-      default: frame_deramp_grid_kernel<kVec, 32><<<grid, 256, 0, st>>>(d, io, list); break;
+      case 8: frame_deramp_grid_kernel<kVec, 8, TIn><<<grid, 256, 0, st>>>(d, io, list); break;
+      case 16: frame_deramp_grid_kernel<kVec, 16, TIn><<<grid, 256, 0, st>>>(d, io, list); break;
+      default: frame_deramp_grid_kernel<kVec, 32, TIn><<<grid, 256, 0, st>>>(d, io, list); break;
     }
   }
 }
@@ -481,20 +500,29 @@ __global__ void xyz2llh_kernel(const double *xyz, double *llh, int64_t n) {
   llh[3 * i + 2] = rp / cos(lat) - re;
 }
 
+template <typename TIn>
+int launch_deramp(const char *name, const s1b_burst_plan_t *plan, const void *in, void *out, void *stream) {
+  if (!plan || !in || !out) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, name);
+  const int S = plan->samples, L = plan->lines;
+  if (S < 1 || L < 1) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "deramp: empty burst");
+  cudaStream_t st = (cudaStream_t)stream;
+  dim3 grid((S + 511) / 512, (L + DERAMP_ROWS - 1) / DERAMP_ROWS);
+  const bool vec = (S % 2 == 0) && ((uintptr_t)in % (2 * sizeof(TIn)) == 0) && ((uintptr_t)out % 16 == 0);
+  if (vec)
+    deramp_kernel<true, TIn><<<grid, 256, 0, st>>>(*plan, (const TIn *)in, (float2 *)out);
+  else
+    deramp_kernel<false, TIn><<<grid, 256, 0, st>>>(*plan, (const TIn *)in, (float2 *)out);
+  return s1b_launch_status();
+}
+
 }  // namespace
 
 extern "C" int s1b_deramp(const s1b_burst_plan_t *plan, const void *in, void *out, void *stream) {
-  if (!plan || !in || !out) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_deramp: null argument");
-  const int S = plan->samples, L = plan->lines;
-  if (S < 1 || L < 1) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_deramp: empty burst");
-  cudaStream_t st = (cudaStream_t)stream;
-  dim3 grid((S + 511) / 512, (L + DERAMP_ROWS - 1) / DERAMP_ROWS);
-  const bool vec = (S % 2 == 0) && ((uintptr_t)in % 16 == 0) && ((uintptr_t)out % 16 == 0);
-  if (vec)
-    deramp_kernel<true><<<grid, 256, 0, st>>>(*plan, (const float2 *)in, (float2 *)out);
-  else
-    deramp_kernel<false><<<grid, 256, 0, st>>>(*plan, (const float2 *)in, (float2 *)out);
-  return s1b_launch_status();
+  return launch_deramp<float2>("s1b_deramp: null argument", plan, in, out, stream);
+}
+
+extern "C" int s1b_deramp_ci16(const s1b_burst_plan_t *plan, const void *in, void *out, void *stream) {
+  return launch_deramp<short2>("s1b_deramp_ci16: null argument", plan, in, out, stream);
 }
 
 extern "C" int s1b_geo2rdr(const s1b_burst_plan_t *plan, const int16_t *dem, int64_t dem_pitch,
@@ -548,9 +576,9 @@ int frame_launch_init(const FrameDev &d, const FrameIO &io, cudaStream_t st) {
 
 int frame_max_ctas_deramp(int rows) {
   switch (rows) {
-    case 8: return resident_ctas(frame_deramp_kernel<8>, 256);
-    case 16: return resident_ctas(frame_deramp_kernel<16>, 256);
-    case 32: return resident_ctas(frame_deramp_kernel<32>, 256);
+    case 8: return resident_ctas(frame_deramp_kernel<8, float2>, 256);
+    case 16: return resident_ctas(frame_deramp_kernel<16, float2>, 256);
+    case 32: return resident_ctas(frame_deramp_kernel<32, float2>, 256);
     default: return 0;
   }
 }
@@ -569,17 +597,31 @@ int frame_launch_deramp(const FrameDev &d, const FrameIO &io, int rows, int ctas
   const int full = frame_max_ctas_deramp(rows);
   if (full <= 0) return s1b_fail(S1B_ERR_UNSUPPORTED, "frame deramp: tile rows must be 8, 16 or 32");
   if (d.n_deramp_tiles == 0) return S1B_OK;
+  const bool ci16 = d.sample_format == S1B_SAMPLES_CI16;
   if (ctas == 0) {  // one CTA per tile, one launch per load width
-    launch_deramp_grid<true>(d, io, rows, split.vec.data(), (int)split.vec.size(), st);
-    launch_deramp_grid<false>(d, io, rows, split.scalar.data(), (int)split.scalar.size(), st);
+    if (ci16) {
+      launch_deramp_grid<true, short2>(d, io, rows, split.vec.data(), (int)split.vec.size(), st);
+      launch_deramp_grid<false, short2>(d, io, rows, split.scalar.data(), (int)split.scalar.size(), st);
+    } else {
+      launch_deramp_grid<true, float2>(d, io, rows, split.vec.data(), (int)split.vec.size(), st);
+      launch_deramp_grid<false, float2>(d, io, rows, split.scalar.data(), (int)split.scalar.size(), st);
+    }
     return s1b_launch_status();
   }
   long long g = ctas < full ? ctas : full;
   if (g > d.n_deramp_tiles) g = d.n_deramp_tiles;
-  switch (rows) {
-    case 8: frame_deramp_kernel<8><<<(unsigned)g, 256, 0, st>>>(d, io); break;
-    case 16: frame_deramp_kernel<16><<<(unsigned)g, 256, 0, st>>>(d, io); break;
-    default: frame_deramp_kernel<32><<<(unsigned)g, 256, 0, st>>>(d, io); break;
+  if (ci16) {
+    switch (rows) {
+      case 8: frame_deramp_kernel<8, short2><<<(unsigned)g, 256, 0, st>>>(d, io); break;
+      case 16: frame_deramp_kernel<16, short2><<<(unsigned)g, 256, 0, st>>>(d, io); break;
+      default: frame_deramp_kernel<32, short2><<<(unsigned)g, 256, 0, st>>>(d, io); break;
+    }
+  } else {
+    switch (rows) {
+      case 8: frame_deramp_kernel<8, float2><<<(unsigned)g, 256, 0, st>>>(d, io); break;
+      case 16: frame_deramp_kernel<16, float2><<<(unsigned)g, 256, 0, st>>>(d, io); break;
+      default: frame_deramp_kernel<32, float2><<<(unsigned)g, 256, 0, st>>>(d, io); break;
+    }
   }
   return s1b_launch_status();
 }

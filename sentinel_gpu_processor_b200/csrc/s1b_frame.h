@@ -44,11 +44,12 @@ struct FrameDev {
   int32_t deramp_rows, geo_cols;  // tile shapes the launches use
   int32_t deramp_tiles_x, deramp_tiles_y;  // deramp tiles of the largest burst, per axis
   int32_t geo_tiles_x, geo_tiles_y;        // geocoding tiles of the largest window, per axis
+  int32_t sample_format;                   // S1B_SAMPLES_C64 or S1B_SAMPLES_CI16
 };
 
 // Run-time buffers of one frame launch sequence.
 struct FrameIO {
-  const float2 *slc;
+  const void *slc;  // complex64 or complex int16 samples (FrameDev::sample_format)
   const int16_t *dem;
   int64_t dem_pitch;
   float2 *work;  // workspace viewed as complex64

@@ -26,7 +26,8 @@ def gslc_header(plan, first, last):
 
 def geocode_burst(plan, slc: torch.Tensor, dem: torch.Tensor, deramped: torch.Tensor | None = None,
                   out: torch.Tensor | None = None, sync: bool = True):
-    """Deramp + geocode one burst.
+    """Deramp + geocode one burst (``slc`` complex64, or complex int16 as
+    int16 [..., 2] straight from the measurement TIFF).
 
     Returns (header int32[64], data view [rows, ncol]) like the ``.gslc`` the
     reference writes, or None when it would skip the burst (empty window or no
@@ -35,7 +36,8 @@ def geocode_burst(plan, slc: torch.Tensor, dem: torch.Tensor, deramped: torch.Te
     """
     if plan.nrow <= 0 or plan.ncol <= 0:
         return None
-    deramped = kernels.deramp(plan, slc.reshape(-1), out=deramped)
+    flat = slc.reshape(-1, 2) if slc.dtype == torch.int16 else slc.reshape(-1)
+    deramped = kernels.deramp(plan, flat, out=deramped)
     full, rows = kernels.geo2rdr(plan, dem, deramped, out=out)
     if not sync:
         return full, rows
@@ -45,13 +47,17 @@ def geocode_burst(plan, slc: torch.Tensor, dem: torch.Tensor, deramped: torch.Te
     return gslc_header(plan, first, last), full[first:last]
 
 
-def geo2rdr_files(db_path, out_prefix, slc_path=None, stream=None):
+def geo2rdr_files(db_path, out_prefix, slc_path=None, stream=None, tiff=None):
     """File-level drop-in for ``geo2rdr dbname slcoutfile [slcinfile] [--stdin]``
     (geo2rdr.cu:704-734): reads the parameter DB and the files it names,
     writes ``<out>_burst_<i>.gslc``.  With ``stream`` (a binary file object,
     e.g. stdin) the bursts are read from it one after the other, every burst
     before its window is checked (geo2rdr.cu:551-557); a short read raises
-    EOFError.  Returns the list of written paths."""
+    EOFError.  With ``tiff`` (an ``ingest.MeasurementTiff``) the bursts come
+    straight from the measurement TIFF as complex int16 -- what the reference
+    pipes in after widening (s1proc/sentinel_scene.py:164-207, 419-437) --
+    read ahead into pinned buffers, only those with a DEM window.  Returns the
+    list of written paths."""
     from types import SimpleNamespace
     p = formats.read_db(db_path)
     radar = SimpleNamespace(samples_per_burst=int(p["samplesPerBurst"]), lines_per_burst=int(p["linesPerBurst"]),
@@ -75,6 +81,21 @@ def geo2rdr_files(db_path, out_prefix, slc_path=None, stream=None):
     src = slc_path or p.get("slc_file")
     L, S = radar.lines_per_burst, radar.samples_per_burst
     written = []
+    if tiff is not None:
+        from . import ingest
+        if tiff.width != S:
+            raise ValueError(f"TIFF width {tiff.width} != samplesPerBurst {S}")
+        plans = [_plan.burst_plan(radar, orbit, fm, dc, b, rsc) for b in bursts]
+        use = [i for i, pl in enumerate(plans) if pl.nrow > 0 and pl.ncol > 0]
+        for i, slc in ingest.BurstStream(tiff, L, nb, indices=use):
+            res = geocode_burst(plans[i], slc, dem)
+            if res is None:
+                continue
+            hdr, data = res
+            path = f"{out_prefix}_burst_{i}.gslc"
+            formats.write_raster(path, hdr, data.cpu().numpy())
+            written.append(path)
+        return written
     for i, b in enumerate(bursts):
         if stream is not None:
             buf = stream.read(L * S * 8)

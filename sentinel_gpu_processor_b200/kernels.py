@@ -36,16 +36,28 @@ def _c64(t, name):
 
 
 def deramp(plan: _lib.BurstPlan, slc: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
-    """TOPS deramp (reference deramp_burst, geo2rdr.cu:138-158)."""
+    """TOPS deramp (reference deramp_burst, geo2rdr.cu:138-158).
+
+    ``slc`` is complex64 [lines * samples] or the measurement TIFF's complex
+    int16 samples as int16 [..., 2] (re, im; ``s1b_deramp_ci16``, widened on
+    the device).  Returns complex64 of the input's shape (without the (re, im)
+    axis for int16 input)."""
     _need_cuda(slc, out)
-    _c64(slc, "slc")
-    if slc.numel() != plan.lines * plan.samples:
+    ci16 = slc.dtype == torch.int16
+    if ci16:
+        if not slc.is_contiguous() or slc.shape[-1] != 2:
+            raise ValueError("int16 slc must be a contiguous [..., 2] (re, im) tensor")
+        n = slc.numel() // 2
+    else:
+        _c64(slc, "slc")
+        n = slc.numel()
+    if n != plan.lines * plan.samples:
         raise ValueError("slc size does not match the plan")
     if out is None:
-        out = torch.empty_like(slc)
+        out = torch.empty(slc.shape[:-1] if ci16 else slc.shape, dtype=torch.complex64, device=slc.device)
     lib = _lib.load()
-    _lib.check(_call("deramp", lib.s1b_deramp, ctypes.byref(plan), _lib.dptr(slc), _lib.dptr(out), _lib.stream_ptr()),
-               "s1b_deramp")
+    fn, name = (lib.s1b_deramp_ci16, "s1b_deramp_ci16") if ci16 else (lib.s1b_deramp, "s1b_deramp")
+    _lib.check(_call("deramp", fn, ctypes.byref(plan), _lib.dptr(slc), _lib.dptr(out), _lib.stream_ptr()), name)
     return out
 
 

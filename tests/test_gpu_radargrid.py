@@ -118,15 +118,20 @@ def test_resample_with_large_offsets_uses_direct_path(cuda, scene):
     assert rel_err(got, want) < 2e-5
 
 
-@pytest.mark.parametrize("shape,win", [((96, 320), 5), ((70, 257), 5), ((33, 130), 3), ((40, 128), 9)])
+@pytest.mark.parametrize("shape,win", [((96, 320), 5), ((70, 257), 5), ((33, 130), 3), ((40, 128), 9),
+                                       ((50, 200), 1), ((66, 136), 7), ((97, 390), 9)])
 def test_box_coherence_matches_oracle(cuda, shape, win):
     rng = np.random.default_rng(shape[0] + win)
     a = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
     n = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
     b = (0.8 * a * np.exp(1j * 0.3) + 0.6 * n).astype(np.complex64)
+    # a zero patch: windows inside it have zero power and coherence 0
+    a[10:30, 40:70] = 0
     got = kernels.box_coherence(torch.from_numpy(a).to(cuda), torch.from_numpy(b).to(cuda), win).cpu().numpy()
     want = orr.box_coherence(a, b, win)
     assert np.abs(got - want).max() < 1e-4
+    h = win // 2
+    assert (got[10 + h:30 - h, 40 + h:70 - h] == 0).all()
 
 
 def test_resampled_pair_is_coherent(cuda):
