@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--config", default="frame",
                     choices=["frame", "frame_pairs", "c1", "c1geo", "c0", "small", "adjoint"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--samples", default="ci16", choices=["ci16", "c64"],
+                    help="frame SLC sample type: complex int16 as in the measurement TIFF (widened on the GPU), "
+                         "or complex64 as the reference's geo2rdr pipe carries it")
     return ap.parse_args()
 
 
@@ -248,15 +251,22 @@ def _workload(args, rank, dev):
 
         from sentinel_gpu_processor_b200.chain import BatchedFrameChain
         sc = synth.make_frame(seed=20261203 + 2000 + rank, device=dev)
-        chain = BatchedFrameChain(sc.ref, sc.sec, sc.rsc, sc.rowlook, sc.collook, sc.alpha, device=dev)
-        chain.load(sc.ref_slc, sc.sec_slc)
+        chain = BatchedFrameChain(sc.ref, sc.sec, sc.rsc, sc.rowlook, sc.collook, sc.alpha, device=dev,
+                                  sample_format=args.samples)
+        if args.samples == "ci16":
+            for v, s in zip(chain.ref_views + chain.sec_views, sc.ref_slc + sc.sec_slc):
+                v.copy_(synth.cint16(s))
+        else:
+            chain.load(sc.ref_slc, sc.sec_slc)
         torch.cuda.synchronize()
         sc.ref_slc = sc.sec_slc = None  # the frame's SLC buffer holds them now
         chain.tuned = chain.autotune(sc.dem, reps=2)
         chain.capture(sc.dem)
         desc = (f"full IW frame: {chain.n_pairs} burst pairs (3 subswaths x 9) of uneven size, lines 1480-1530, "
                 f"samples 20000-25500, 100-line overlap; batched: one launch per stage over the descriptor table "
-                f"of all {2 * chain.n_pairs} bursts, one CUDA graph per step, tile shapes from the autotuner")
+                f"of all {2 * chain.n_pairs} bursts, one CUDA graph per step, tile shapes from the autotuner; "
+                + ("SLC samples complex int16 (the measurement TIFF's type, widened on the GPU in the deramp)"
+                   if args.samples == "ci16" else "SLC samples complex64 (as the reference's geo2rdr pipe)"))
         return sc, chain, chain.replay, desc
     if args.config == "frame_pairs":
         sc = synth.make_frame(seed=20261203 + 2000 + rank, device=dev)
@@ -466,7 +476,10 @@ def _kernel_table(chain, sc, args, times, peak):
         res = [r for r in chain.last if r is not None]
         box_px = sum((r.box[2] - r.box[0]) * (r.box[3] - r.box[1]) for r in res)
         ml = sum(r.ifg.numel() for r in res)
-        bytes_per = {"deramp": 16 * burst, "geo2rdr": GEO_BYTES_PER_GEO_PX * geo + GEO_BYTES_PER_BURST_PX * burst,
+        # deramp: read one input sample (8 bytes complex64, 4 complex int16), write 8
+        din = 4 if getattr(chain, "sample_format", "c64") == "ci16" else 8
+        bytes_per = {"deramp": (din + 8) * burst,
+                     "geo2rdr": GEO_BYTES_PER_GEO_PX * geo + GEO_BYTES_PER_BURST_PX * burst,
                      "crossmul_looks": 16 * box_px + 20 * ml, "goldstein": 16 * ml}
     else:
         pls = [p for pl in chain.pairs for p in pl] if args.config == "frame_pairs" else chain.plans
@@ -548,7 +561,8 @@ def run_s1b(args):
         extra = {"burst_pairs": chain.n_pairs, "burst_px_per_step": chain.burst_pixels,
                  "geo_px_total": sum(chain.geo_pixels()),
                  "ifg_ml_shapes_first3": [list(r.ifg.shape) for r in res[:3]],
-                 "batched": True, "cuda_graph": True, "tuning": chain.tuned}
+                 "batched": True, "cuda_graph": True, "tuning": chain.tuned,
+                 "slc_samples": "complex int16" if args.samples == "ci16" else "complex64"}
         launches = chain.launches_per_step()
     elif args.config == "frame_pairs":
         extra = {"burst_pairs": len(chain.pairs), "burst_px_per_step": chain.burst_pixels,

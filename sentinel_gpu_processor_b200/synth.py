@@ -472,6 +472,15 @@ def make_frame(seed=20261203, device="cpu", n_swaths=3, n_bursts=9, baseline=150
                      extra={"coherence": cohs, "hmax": hmax})
 
 
+def cint16(slc, scale: float = 2000.0):
+    """Complex int16 samples (int16 [..., 2], re and im) of a synthetic SLC
+    tensor, as a Sentinel-1 measurement TIFF holds them: ``round(scale *
+    slc)``, clipped to the int16 range."""
+    import torch
+    q = torch.stack([slc.real, slc.imag], -1).mul(scale).round().clamp(-32768, 32767)
+    return q.to(torch.int16).contiguous()
+
+
 def frame_pair(frame: PairScene, k: int, margin: int = 64) -> PairScene:
     """Burst pair ``k`` of a frame as its own PairScene, on the part of the
     frame's DEM grid that covers both bursts' footprints (plus a margin)."""
