@@ -358,6 +358,21 @@ int s1b_coherence_cc(const void *ifg, const float *amp1, const float *amp2, int3
 /* ECEF -> geodetic (deg, deg, m), one-step Bowring (s1proc/geometry.py:166-193). */
 int s1b_xyz2llh(const double *xyz, double *llh, int64_t n, void *stream);
 
+/* Line-of-sight unit vectors and look angles of every pixel of an RSC grid,
+ * replacing s1proc/utils.py:240-292 (_los, via orbitrangetime_vec,
+ * s1proc/orbit.py:168-188).  Pixel (row, col) is at latitude lat0 + row *
+ * lat_step and longitude lon0 + col * lon_step (degrees; a separate multiply
+ * and add, as numpy.mgrid forms rsc.grid()) and height dem[row * dem_pitch +
+ * col] (int16, metres).  Its zero-Doppler time is solved by Newton from t0
+ * (the middle state vector's time); los: float32 [nrow * ncol * 3], the unit
+ * vector satellite -> point; theta: float32 [nrow * ncol], the look angle
+ * acos(clip(los . -(cos lat cos lon, cos lat sin lon, sin lat), -1, 1)) in
+ * degrees, formed from the float32 vector as the reference does.  Device
+ * pointers; ncol <= 65535 * 128. */
+int s1b_los_grid(const s1b_orbit_poly_t *orbit, double t0, double lat0, double lat_step, double lon0,
+                 double lon_step, const int16_t *dem, int64_t dem_pitch, int32_t nrow, int32_t ncol, float *los,
+                 float *theta, void *stream);
+
 /* ------------------------------------------------------------ burst stitching */
 
 /* One burst interferogram of a frame: `offset` = first element in the data

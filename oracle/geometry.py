@@ -11,6 +11,8 @@ Follows, operation for operation where it matters for rounding:
   * ``csrc/src/orbit.cu:224-245``    intp_orbit (truncating window rule)
   * ``csrc/src/orbit.cu:247-280``    orbitrangetime (51 iterations, 5e-9 s)
   * ``csrc/src/bounds.cu:7-317``     bounds / rah2ll / geodesic heading
+  * ``s1proc/orbit.py:84-166``       Python interpolant (closest window) and Newton
+  * ``s1proc/utils.py:240-292``      _los: LOS vectors and look angles of a grid
 
 All functions are vectorised over leading axes with NumPy float64.
 """
@@ -180,6 +182,76 @@ def orbitrangetime(tt, xx, vv, xyz, tline0, satx0, satv0, max_iter=51, tol=5.0e-
         flat_active[ia[done]] = False
     dr = xyz - satx
     return tline, dr, iters
+
+
+def interp_orbit_closest(tt, xx, vv, t):
+    """The Python orbit interpolant: the 4-point Hermite window around the
+    state vector closest to t (argmin |t - tt|, clamped to [1, n-3]).
+    s1proc/orbit.py:84-115.  tt [n], xx/vv [n, 3], t [...]."""
+    tt = np.asarray(tt, dtype=np.float64)
+    xx = np.asarray(xx, dtype=np.float64).reshape(-1, 3)
+    vv = np.asarray(vv, dtype=np.float64).reshape(-1, 3)
+    t = np.asarray(t, dtype=np.float64)
+    il = np.abs(t[..., None] - tt).argmin(axis=-1)
+    il = np.minimum(np.maximum(il, 1), tt.shape[0] - 3)
+    idx = il[..., None] - 1 + np.arange(4)
+    return orbithermite(tt[idx], xx[idx], vv[idx], t)
+
+
+def orbitrangetime_py(tt, xx, vv, xyz, tline0, satx0, satv0):
+    """s1proc/orbit.py:118-166 (the numba loop), vectorised over points: the
+    same fixed-point step and 5e-9 s stop on the closest-sample interpolant.
+    Returns (dr [..., 3], tline [...])."""
+    xyz = np.asarray(xyz, dtype=np.float64)
+    shape = xyz.shape[:-1]
+    tline = np.full(shape, float(tline0))
+    satx = np.broadcast_to(np.asarray(satx0, dtype=np.float64), shape + (3,)).copy()
+    satv = np.broadcast_to(np.asarray(satv0, dtype=np.float64), shape + (3,)).copy()
+    active = np.ones(shape, dtype=bool)
+    for _ in range(51):
+        if not active.any():
+            break
+        ia = np.nonzero(active.ravel())[0]
+        tl = tline.reshape(-1)[ia]
+        sx = satx.reshape(-1, 3)[ia]
+        sv = satv.reshape(-1, 3)[ia]
+        dr = xyz.reshape(-1, 3)[ia] - sx
+        fn = dr[:, 0] * sv[:, 0] + dr[:, 1] * sv[:, 1] + dr[:, 2] * sv[:, 2]
+        fnprime = -sv[:, 0] * sv[:, 0] - sv[:, 1] * sv[:, 1] - sv[:, 2] * sv[:, 2]
+        tprev = tl
+        tl = tl - fn / fnprime
+        nx, nv = interp_orbit_closest(tt, xx, vv, tl)
+        tline.reshape(-1)[ia] = tl
+        satx.reshape(-1, 3)[ia] = nx
+        satv.reshape(-1, 3)[ia] = nv
+        active.reshape(-1)[ia[np.abs(tl - tprev) < 5.0e-9]] = False
+    return xyz - satx, tline
+
+
+def los_grid(orb, dem, latmax, lonmin, dlat, dlon, nlat, nlon):
+    """LOS unit vectors (float32 [n, 3]) and look angles (float32 [nlat, nlon],
+    degrees) of an RSC grid.  s1proc/utils.py:240-292 (_los): the grid of
+    geocoordinates.py:114-118 (numpy.mgrid from latmax to latmin, lonmin to
+    lonmax, with latmin/lonmax from geocoordinates.py:70-71), llh2xyz_vec and
+    orbitrangetime from the middle state vector (orbit.py:168-188), the float32
+    cast, then the look angle from the float32 vectors."""
+    orb = np.asarray(orb, dtype=np.float64)
+    tt, xx, vv = orb[:, 0], orb[:, 1:4], orb[:, 4:7]
+    latmin = latmax + dlat * (nlat - 1)
+    lonmax = lonmin + dlon * (nlon - 1)
+    lat, lon = np.mgrid[latmax:latmin:(nlat * 1j), lonmin:lonmax:(nlon * 1j)]
+    llh = np.column_stack((lat.flatten(), lon.flatten(), np.asarray(dem).flatten()))
+    xyz = llh2xyz(llh)
+    nmid = len(tt) // 2
+    dr, _ = orbitrangetime_py(tt, xx, vv, xyz, tt[nmid], xx[nmid], vv[nmid])
+    losvec = (dr / np.sqrt(dr[:, 0] * dr[:, 0] + dr[:, 1] * dr[:, 1] + dr[:, 2] * dr[:, 2])[:, None])
+    losvec = losvec.astype(np.float32)
+    r_lat = np.radians(lat.flatten())
+    r_lon = np.radians(lon.flatten())
+    r_n = -np.column_stack([np.cos(r_lat) * np.cos(r_lon), np.cos(r_lat) * np.sin(r_lon), np.sin(r_lat)])
+    costheta = np.clip(np.sum(losvec * r_n, axis=1).reshape(nlat, nlon), -1, 1)
+    theta = np.rad2deg(np.arccos(costheta)).astype(np.float32)
+    return losvec, theta
 
 
 # --------------------------------------------------------------------------

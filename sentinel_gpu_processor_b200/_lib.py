@@ -151,6 +151,8 @@ _SIGNATURES = {
                               c_int32, c_void_p, c_void_p]),
     "s1b_coherence_cc": (c_int, [c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_uint64, c_void_p, c_void_p]),
     "s1b_xyz2llh": (c_int, [c_void_p, c_void_p, c_int64, c_void_p]),
+    "s1b_los_grid": (c_int, [POINTER(OrbitPoly), c_double, c_double, c_double, c_double, c_double, c_void_p, c_int64,
+                             c_int32, c_int32, c_void_p, c_void_p, c_void_p]),
     "s1b_stitch_workspace_bytes": (c_size_t, [POINTER(StitchBurst), c_int32, c_int32]),
     "s1b_stitch": (c_int, [POINTER(StitchBurst), c_int32, c_void_p, c_int32, c_int32, c_int32, c_void_p,
                            POINTER(c_double), c_void_p, c_size_t, c_void_p]),

@@ -479,6 +479,44 @@ __global__ void llh2xyz_kernel(const double *llh, double *xyz, int64_t n) {
   xyz[3 * i + 2] = (re * (1 - kRe2D) + h) * sl;
 }
 
+// Line of sight and look angle of every pixel of an RSC grid
+// (s1proc/utils.py:240-292, _los): the pixel's geodetic point (row lat, column
+// lon, DEM height) to ECEF, its zero-Doppler time by Newton from t0 (the
+// middle state vector's time, s1proc/orbit.py:168-188), the unit vector
+// satellite -> point, stored as float32, and the look angle
+// acos(clip(los32 . n, -1, 1)) in degrees with n = -(cos lat cos lon,
+// cos lat sin lon, sin lat) formed from the float32 vector, as the reference
+// casts before its dot product.  Grid coordinates are start + index * step
+// with a separate multiply and add, as numpy.mgrid forms them.
+__global__ void los_grid_kernel(const __grid_constant__ s1b_orbit_poly_t P, double t0, double lat0, double lat_step,
+                                double lon0, double lon_step, const int16_t *__restrict__ dem, int64_t pitch,
+                                int nrow, int ncol, float *__restrict__ los, float *__restrict__ theta) {
+  const int col = blockIdx.y * blockDim.x + threadIdx.x, row = blockIdx.x;
+  if (col >= ncol || row >= nrow) return;
+  const double latd = __dadd_rn(__dmul_rn((double)row, lat_step), lat0);
+  const double lond = __dadd_rn(__dmul_rn((double)col, lon_step), lon0);
+  const double lat = latd * kPiD / 180, lon = lond * kPiD / 180, h = (double)__ldg(dem + (int64_t)row * pitch + col);
+  double sl, cl, so, co;
+  sincos(lat, &sl, &cl);
+  sincos(lon, &so, &co);
+  const double re = kRaD / sqrt(1. - kRe2D * sl * sl);
+  const double p[3] = {(re + h) * cl * co, (re + h) * cl * so, (re * (1 - kRe2D) + h) * sl};
+  OrbitState st;
+  orbit_eval(P, t0, st);
+  double t = t0, dr[3];
+  zero_doppler(P, p, t, st, dr);
+  const double inv = 1.0 / sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+  const float l0 = (float)(dr[0] * inv), l1 = (float)(dr[1] * inv), l2 = (float)(dr[2] * inv);
+  const int64_t o = (int64_t)row * ncol + col;
+  los[3 * o] = l0;
+  los[3 * o + 1] = l1;
+  los[3 * o + 2] = l2;
+  const double n0 = -(cl * co), n1 = -(cl * so), n2 = -sl;
+  double c = __dadd_rn(__dadd_rn(__dmul_rn((double)l0, n0), __dmul_rn((double)l1, n1)), __dmul_rn((double)l2, n2));
+  c = fmin(fmax(c, -1.0), 1.0);
+  theta[o] = (float)(acos(c) * (180.0 / kPiD));
+}
+
 // ECEF -> geodetic with the one-step Bowring formula of s1proc/geometry.py:166-193
 // (the form bounds.cu uses), degrees and metres.
 __global__ void xyz2llh_kernel(const double *xyz, double *llh, int64_t n) {
@@ -558,6 +596,20 @@ extern "C" int s1b_llh2xyz(const double *llh, double *xyz, int64_t n, void *stre
   if (n > 0 && (!llh || !xyz)) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_llh2xyz: null argument");
   if (n <= 0) return S1B_OK;
   llh2xyz_kernel<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(llh, xyz, n);
+  return s1b_launch_status();
+}
+
+extern "C" int s1b_los_grid(const s1b_orbit_poly_t *orbit, double t0, double lat0, double lat_step, double lon0,
+                            double lon_step, const int16_t *dem, int64_t dem_pitch, int32_t nrow, int32_t ncol,
+                            float *los, float *theta, void *stream) {
+  if (!orbit || !dem || !los || !theta) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_los_grid: null argument");
+  if (nrow < 0 || ncol < 0 || (ncol > 0 && dem_pitch < ncol))
+    return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_los_grid: bad grid size or pitch");
+  if (nrow == 0 || ncol == 0) return S1B_OK;
+  if ((ncol + 127) / 128 > 65535) return s1b_fail(S1B_ERR_TOO_LARGE, "s1b_los_grid: grid too wide");
+  const dim3 grid((unsigned)nrow, (unsigned)((ncol + 127) / 128));
+  los_grid_kernel<<<grid, 128, 0, (cudaStream_t)stream>>>(*orbit, t0, lat0, lat_step, lon0, lon_step, dem, dem_pitch,
+                                                          nrow, ncol, los, theta);
   return s1b_launch_status();
 }
 

@@ -1,7 +1,8 @@
 """s1proc's geometry call surface on the GPU, with its names, arguments and
 return layouts (s1proc/geometry.py:150-241, s1proc/orbit.py:84-188):
 ``llh2xyz``, ``xyz2llh`` and their ``_vec`` forms, ``interp_orbit``,
-``orbitrangetime``, ``orbitrangetime_vec``.
+``orbitrangetime``, ``orbitrangetime_vec``, and ``los`` (s1proc/utils.py:240-292,
+``_los``: line-of-sight vectors and look angles of a DEM grid).
 
 Arrays are numpy in and out like the numba originals; the arithmetic runs
 in libs1b (float64).  The orbit is the reference interpolant as window
@@ -73,3 +74,28 @@ def orbitrangetime_vec(llh, tt, xx, vv):
     xyz = kernels.llh2xyz(torch.as_tensor(np.asarray(llh, dtype=np.float64).reshape(-1, 3), device=_dev()))
     _, dr = kernels.zero_doppler(poly, xyz, float(tt[len(tt) // 2]))
     return (dr / dr.norm(dim=1, keepdim=True)).cpu().numpy()
+
+
+def los(orb, dem, rsc):
+    """LOS unit vectors and look angles of every pixel of an RSC grid, as
+    s1proc/utils.py:240-292 (``_los``) computes them, in one kernel.
+
+    ``orb``: [n, 7] rows (time, x, y, z, vx, vy, vz); ``dem``: int16 heights,
+    nlat * nlon values; ``rsc``: an object with latmax, lonmin, dlat, dlon,
+    nlat, nlon (``formats.read_rsc`` or the reference's GeoCoordinates).
+    Returns (losvec float32 [nlat * nlon, 3], theta float32 [nlat, nlon]
+    degrees).  The grid is numpy.mgrid's (geocoordinates.py:70-71, 114-118);
+    each point's zero-Doppler time is solved from the middle state vector's
+    time (orbit.py:168-188)."""
+    orb = np.asarray(orb, dtype=np.float64)
+    tt, xx, vv = orb[:, 0], orb[:, 1:4], orb[:, 4:7]
+    poly = _plan.orbit_poly(tt, xx, vv)
+    nlat, nlon = int(rsc.nlat), int(rsc.nlon)
+    latmin = rsc.latmax + rsc.dlat * (nlat - 1)
+    lonmax = rsc.lonmin + rsc.dlon * (nlon - 1)
+    # numpy.mgrid with a complex step: start + index * ((stop - start) / (num - 1))
+    lat_step = (latmin - rsc.latmax) / float(nlat - 1) if nlat > 1 else 0.0
+    lon_step = (lonmax - rsc.lonmin) / float(nlon - 1) if nlon > 1 else 0.0
+    d = torch.as_tensor(np.ascontiguousarray(np.asarray(dem, dtype=np.int16).reshape(nlat, nlon)), device=_dev())
+    losvec, theta = kernels.los_grid(poly, tt[len(tt) // 2], rsc.latmax, lat_step, rsc.lonmin, lon_step, d)
+    return losvec.cpu().numpy(), theta.cpu().numpy()

@@ -160,6 +160,23 @@ def zero_doppler(poly: _lib.OrbitPoly, xyz: torch.Tensor, tline0: float):
     return t, dr
 
 
+def los_grid(poly: _lib.OrbitPoly, t0: float, lat0: float, lat_step: float, lon0: float, lon_step: float,
+             dem: torch.Tensor):
+    """Line-of-sight unit vectors (float32 [nrow * ncol, 3]) and look angles
+    (float32 [nrow, ncol], degrees) of a lat/lon grid with int16 heights
+    ``dem`` [nrow, ncol] (unit column stride); ``s1b_los_grid``."""
+    _need_cuda(dem)
+    if dem.dtype != torch.int16 or dem.dim() != 2 or dem.stride(1) != 1:
+        raise ValueError("dem must be an int16 [nrow, ncol] tensor with unit column stride")
+    nrow, ncol = dem.shape
+    los = torch.empty((nrow * ncol, 3), dtype=torch.float32, device=dem.device)
+    theta = torch.empty((nrow, ncol), dtype=torch.float32, device=dem.device)
+    _lib.check(_call("los_grid", _lib.load().s1b_los_grid, ctypes.byref(poly), float(t0), float(lat0),
+                     float(lat_step), float(lon0), float(lon_step), _lib.dptr(dem), dem.stride(0), nrow, ncol,
+                     _lib.dptr(los), _lib.dptr(theta), _lib.stream_ptr()), "s1b_los_grid")
+    return los, theta
+
+
 def llh2xyz(llh: torch.Tensor) -> torch.Tensor:
     _need_cuda(llh)
     llh = llh.contiguous().to(torch.float64)

@@ -90,3 +90,24 @@ def test_geometry_mirror_matches_oracle(cuda):
     x, v = G.interp_orbit(tt, xx, vv, float(tt[mid]) + 1.3)
     xo, vo = og.intp_orbit(tt, xx, vv, np.float64(tt[mid] + 1.3))
     assert np.abs(x - xo).max() < 1e-6 and np.abs(v - vo).max() < 1e-8
+
+
+@pytest.mark.parametrize("shape", [(70, 300), (1, 129)])
+def test_los_grid_matches_oracle(cuda, shape):
+    """s1proc/utils.py:240-292 (_los) on a DEM grid: float32 LOS vectors within
+    a few ulps and look angles within 2e-5 degrees of the float64 oracle."""
+    from types import SimpleNamespace
+    sc = synth.make_pair("tiny", seed=7)
+    tt, xx, vv = sc.ref[0].orbit
+    orb = np.column_stack([tt, xx, vv])
+    nlat, nlon = shape
+    r = sc.rsc
+    rsc = SimpleNamespace(latmax=r.latmax + 3 * r.dlat, lonmin=r.lonmin + 5 * r.dlon, dlat=r.dlat, dlon=r.dlon,
+                          nlat=nlat, nlon=nlon)
+    dem = np.random.default_rng(nlat * nlon).integers(-50, 3000, size=(nlat, nlon)).astype(np.int16)
+    losvec, theta = G.los(orb, dem, rsc)
+    want_los, want_theta = og.los_grid(orb, dem, rsc.latmax, rsc.lonmin, rsc.dlat, rsc.dlon, nlat, nlon)
+    assert losvec.dtype == np.float32 and losvec.shape == (nlat * nlon, 3)
+    assert theta.dtype == np.float32 and theta.shape == (nlat, nlon)
+    assert np.abs(losvec - want_los).max() < 3e-7
+    assert np.abs(theta - want_theta).max() < 2e-5
