@@ -147,6 +147,106 @@ __device__ __forceinline__ void crossmul_tile(const XmArgs &a, int i, int chunk,
   }
 }
 
+// Frame form of crossmul_tile: one CTA walks XM_ROWS multilooked rows of a
+// column chunk (frames give grids of hundreds of thousands of row chunks).
+// Per row every thread sums the `rowlook` rows of its columns into a float4
+// (conj product re, im, both powers) in one of two shared-memory buffers;
+// after a barrier one warp (a different one each row, so the others go on
+// loading the next row) or, for chunks of more than 32 outputs, the whole CTA
+// forms the `collook` sums and the epilogue, with the same operations in the
+// same order as crossmul_tile.  The buffer a row's epilogue reads is
+// rewritten only after the next row's barrier, which that warp reaches once
+// its epilogue is done.  (On single pairs, grids of a few thousand CTAs,
+// this form measured slower than crossmul_tile, so they keep that one.)
+constexpr int XM_ROWS = 4;
+
+__device__ __forceinline__ void crossmul_rows_tile(const XmArgs &a, int i0, int chunk, float4 *smem4) {
+  const int W = a.m_per_cta * a.collook;
+  const int j0 = chunk * a.m_per_cta;
+  const int mcta = min(a.m_per_cta, a.ncol_ml - j0);
+  const int wcta = mcta * a.collook;
+  const int64_t col0 = (int64_t)j0 * a.collook;
+  const int i1 = min(i0 + XM_ROWS, a.nrow_ml);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const float fcl = (float)a.collook, frl = (float)a.rowlook;
+  for (int i = i0; i < i1; ++i) {
+    float4 *buf = smem4 + ((i - i0) & 1) * W;
+    const int64_t row0 = (int64_t)i * a.rowlook;
+    for (int c = threadIdx.x; c < wcta; c += 2 * XM_THREADS) {
+      const bool two = c + XM_THREADS < wcta;
+      const int cc = two ? c + XM_THREADS : c;
+      float ir[2] = {0.f, 0.f}, ii[2] = {0.f, 0.f}, p1[2] = {0.f, 0.f}, p2[2] = {0.f, 0.f};
+      const float2 *pr = a.ref + a.ref_off + row0 * a.ref_width + col0;
+      const float2 *ps = a.sec + a.sec_off + row0 * a.sec_width + col0;
+      int k = 0;
+      for (; k + 4 <= a.rowlook; k += 4) {
+        float2 r[4][2], s[4][2];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          r[u][0] = __ldg(pr + (int64_t)(k + u) * a.ref_width + c);
+          r[u][1] = __ldg(pr + (int64_t)(k + u) * a.ref_width + cc);
+          s[u][0] = __ldg(ps + (int64_t)(k + u) * a.sec_width + c);
+          s[u][1] = __ldg(ps + (int64_t)(k + u) * a.sec_width + cc);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            ir[q] += r[u][q].x * s[u][q].x + r[u][q].y * s[u][q].y;
+            ii[q] += -r[u][q].y * s[u][q].x + r[u][q].x * s[u][q].y;
+            p1[q] += r[u][q].x * r[u][q].x + r[u][q].y * r[u][q].y;
+            p2[q] += s[u][q].x * s[u][q].x + s[u][q].y * s[u][q].y;
+          }
+        }
+      }
+      for (; k < a.rowlook; ++k) {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int col = q ? cc : c;
+          const float2 r = __ldg(pr + (int64_t)k * a.ref_width + col);
+          const float2 s = __ldg(ps + (int64_t)k * a.sec_width + col);
+          ir[q] += r.x * s.x + r.y * s.y;
+          ii[q] += -r.y * s.x + r.x * s.y;
+          p1[q] += r.x * r.x + r.y * r.y;
+          p2[q] += s.x * s.x + s.y * s.y;
+        }
+      }
+      buf[c] = make_float4(ir[0], ii[0], p1[0], p2[0]);
+      if (two) buf[cc] = make_float4(ir[1], ii[1], p1[1], p2[1]);
+    }
+    __syncthreads();
+    const bool one = mcta <= 32;
+    if (one && warp != (i - i0) % (XM_THREADS / 32)) continue;
+    for (int m = one ? lane : threadIdx.x; m < mcta; m += one ? 32 : XM_THREADS) {
+      float ir = 0.f, ii = 0.f, p1 = 0.f, p2 = 0.f;
+      const float4 *b = buf + m * a.collook;
+#pragma unroll 4
+      for (int u = 0; u < a.collook; ++u) {
+        const float4 v = b[u];
+        ir += v.x;
+        ii += v.y;
+        p1 += v.z;
+        p2 += v.w;
+      }
+      ir = ir / fcl / frl;
+      ii = ii / fcl / frl;
+      const bool unit = (a.rowlook == 1 && a.collook == 1);
+      const float am1 = unit ? sqrtf(sqrtf(p1)) : sqrtf(p1 / fcl / frl);
+      const float am2 = unit ? sqrtf(sqrtf(p2)) : sqrtf(p2 / fcl / frl);
+      const int64_t o = (int64_t)i * a.ncol_ml + j0 + m;
+      if (a.ifg) a.ifg[o] = make_float2(ir, ii);
+      if (a.amp1) a.amp1[o] = am1;
+      if (a.amp2) a.amp2[o] = am2;
+      if (a.coh) {
+        float c = hypotf(ir, ii) / (am1 + 1e-12f) / (am2 + 1e-12f);
+        if (c > 1.f) c = fill_uniform(a.seed, (uint64_t)o);
+        a.coh[o] = c;
+      }
+      if (a.phase) a.phase[o] = atan2f(ii, ir);
+    }
+  }
+}
+
 __global__ __launch_bounds__(XM_THREADS) void crossmul_looks_kernel(const XmArgs a) {
   extern __shared__ float4 smem4[];
   crossmul_tile(a, blockIdx.x, blockIdx.y, smem4);
@@ -243,14 +343,14 @@ __global__ void frame_box_kernel(const FrameDev d, s1b_frame_pair_t *pout) {
   pout[k] = r;
 }
 
-// Crossmul + looks of every pair: blockIdx.z = pair, x = multilooked row,
-// y = column chunk; CTAs outside a pair's box return at once.
+// Crossmul + looks of every pair: blockIdx.z = pair, x = group of XM_ROWS
+// multilooked rows, y = column chunk; CTAs outside a pair's box return at once.
 __global__ __launch_bounds__(XM_THREADS) void frame_crossmul_kernel(const FrameDev d, const FrameIO io,
                                                                    int m_per_cta) {
   extern __shared__ float4 smem4[];
   const int k = blockIdx.z;
   const s1b_frame_pair_t &r = io.pout[k];
-  if (!r.ok || (int)blockIdx.x >= r.nrow_ml || (int)blockIdx.y * m_per_cta >= r.ncol_ml) return;
+  if (!r.ok || (int)blockIdx.x * XM_ROWS >= r.nrow_ml || (int)blockIdx.y * m_per_cta >= r.ncol_ml) return;
   const FramePair pr = d.pairs[k];
   const s1b_burst_plan_t &p1 = d.plans[pr.ref], &p2 = d.plans[pr.sec];
   const FrameBurst &b1 = d.bursts[pr.ref], &b2 = d.bursts[pr.sec];
@@ -272,7 +372,7 @@ __global__ __launch_bounds__(XM_THREADS) void frame_crossmul_kernel(const FrameD
   a.coh = io.coh ? io.coh + pr.ml_off : nullptr;
   a.phase = nullptr;
   a.seed = d.fill_seed;
-  crossmul_tile(a, blockIdx.x, blockIdx.y, smem4);
+  crossmul_rows_tile(a, blockIdx.x * XM_ROWS, blockIdx.y, smem4);
 }
 
 }  // namespace
@@ -370,14 +470,14 @@ int frame_launch_crossmul(const FrameDev &d, const FrameIO &io, cudaStream_t st)
   if (d.collook > XM_MAX_COLLOOK) return s1b_fail(S1B_ERR_TOO_LARGE, "frame crossmul: collook above 4096");
   if (d.max_nrow_ml <= 0 || d.max_ncol_ml <= 0) return S1B_OK;
   const int m_per_cta = d.collook >= 512 ? 1 : 512 / d.collook;
-  const size_t smem = (size_t)m_per_cta * d.collook * 2 * sizeof(float2);
+  const size_t smem = (size_t)m_per_cta * d.collook * 2 * sizeof(float4);  // two buffers of float4
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(frame_crossmul_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return s1b_fail(S1B_ERR_CUDA, cudaGetErrorString(e));
   }
   const int nchunk = (d.max_ncol_ml + m_per_cta - 1) / m_per_cta;
   if (nchunk > 65535 || d.n_pairs > 65535) return s1b_fail(S1B_ERR_TOO_LARGE, "frame crossmul: grid too large");
-  dim3 grid(d.max_nrow_ml, nchunk, d.n_pairs);
+  dim3 grid((d.max_nrow_ml + XM_ROWS - 1) / XM_ROWS, nchunk, d.n_pairs);
   frame_crossmul_kernel<<<grid, XM_THREADS, smem, st>>>(d, io, m_per_cta);
   return s1b_launch_status();
 }
