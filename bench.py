@@ -81,13 +81,23 @@ def dist_setup(n):
 
 
 def max_over_ranks(x, world):
+    """The slowest rank's value (elapsed times are max-reduced across ranks);
+    the tensor lives where the process group's backend reduces (NCCL: the
+    GPU, gloo: the host)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_rate(world, steps, units_per_step, elapsed_ms):
+    """Whole-job throughput of weakly scaled replicas: every rank processes
+    ``units_per_step`` per step, the job takes the slowest rank's time."""
+    return world * steps * units_per_step / (elapsed_ms / 1e3)
 
 
 def barrier(world):
@@ -346,7 +356,7 @@ def _e2e(chain, sc, args, world):
     t2.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(s2.elapsed_time(t2), world)
-    return world * k_e2e * chain.burst_pixels / (e2e_ms / 1e3), h2d, d2h
+    return job_rate(world, k_e2e, chain.burst_pixels, e2e_ms), h2d, d2h
 
 
 def _e2e_frame(chain, sc, args, world):
@@ -383,7 +393,7 @@ def _e2e_frame(chain, sc, args, world):
     t2.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(s2.elapsed_time(t2), world)
-    return world * k_e2e * chain.burst_pixels / (e2e_ms / 1e3), h2d, d2h
+    return job_rate(world, k_e2e, chain.burst_pixels, e2e_ms), h2d, d2h
 
 
 def _e2e_radar(chain, sc, args, world):
@@ -420,7 +430,7 @@ def _e2e_radar(chain, sc, args, world):
     t2.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(s2.elapsed_time(t2), world)
-    return world * k_e2e * chain.burst_pixels / (e2e_ms / 1e3), h2d, d2h
+    return job_rate(world, k_e2e, chain.burst_pixels, e2e_ms), h2d, d2h
 
 
 KERNELS = ("deramp", "geo2rdr", "crossmul_looks", "goldstein", "geo2rdr_offsets", "resample", "box_coherence")
@@ -539,7 +549,7 @@ def run_s1b(args):
     chain.geo_events = None
     barrier(world)
     elapsed_ms = max_over_ranks(start.elapsed_time(stop), world)
-    value = world * args.steps * chain.burst_pixels / (elapsed_ms / 1e3)
+    value = job_rate(world, args.steps, chain.burst_pixels, elapsed_ms)
     e2e, h2d, d2h = _e2e(chain, sc, args, world)
 
     if isinstance(res, list):
