@@ -407,12 +407,15 @@ class BatchedFrameChain:
                 pass
             self._handle = None
 
-    def _args(self, dem):
+    def _args(self, dem, slc=None):
         if dem.dtype != torch.int16 or dem.dim() != 2 or dem.stride(1) != 1 or dem.device != self.dev:
             raise ValueError("dem must be an int16 [nlat, nlon] device raster with unit column stride")
         if dem.shape[0] < max(p.win_bottom for p in self.plans) or dem.shape[1] < max(p.win_right for p in self.plans):
             raise ValueError("dem does not cover every burst's DEM window")
-        return (self._handle, _lib.dptr(self.slc), _lib.dptr(dem), dem.stride(0), _lib.dptr(self.workspace),
+        slc = self.slc if slc is None else slc
+        if slc.dtype != self.slc.dtype or slc.shape != self.slc.shape or not slc.is_contiguous() or slc.device != self.dev:
+            raise ValueError("slc must be a contiguous buffer like chain.slc")
+        return (self._handle, _lib.dptr(slc), _lib.dptr(dem), dem.stride(0), _lib.dptr(self.workspace),
                 _lib.dptr(self.ifg), _lib.dptr(self.amp1), _lib.dptr(self.amp2), _lib.dptr(self.coh),
                 _lib.dptr(self.filt), _lib.dptr(self.pairs_dev))
 
@@ -421,9 +424,11 @@ class BatchedFrameChain:
         for v, s in zip(self.ref_views + self.sec_views, list(ref_slcs) + list(sec_slcs)):
             v.copy_(s.reshape(v.shape), non_blocking=True)
 
-    def run(self, dem):
-        """One frame run on the current stream (inputs already in ``slc``)."""
-        _lib.check(_call_frame("frame_run", _lib.load().s1b_frame_run, *self._args(dem), _lib.stream_ptr()),
+    def run(self, dem, slc=None):
+        """One frame run on the current stream (inputs already in ``slc``,
+        default the chain's own buffer; another buffer must have its layout,
+        e.g. ``torch.empty_like(chain.slc)``)."""
+        _lib.check(_call_frame("frame_run", _lib.load().s1b_frame_run, *self._args(dem, slc), _lib.stream_ptr()),
                    "s1b_frame_run")
 
     def autotune(self, dem, reps=3):
@@ -451,18 +456,23 @@ class BatchedFrameChain:
         t = (ctypes.c_int32 * 4)(deramp_rows, deramp_ctas, geo_cols, geo_ctas)
         _lib.check(_lib.load().s1b_frame_set_tuning(self._handle, t), "s1b_frame_set_tuning")
 
-    def capture(self, dem):
-        """Record one frame run into a CUDA graph; ``replay()`` reruns it."""
-        self.run(dem)
+    def capture(self, dem, slc=None):
+        """Record one frame run into a CUDA graph; ``replay()`` reruns it.
+        With ``slc`` (another buffer like ``chain.slc``) the graph is returned
+        instead of kept as the chain's."""
+        self.run(dem, slc)
         torch.cuda.synchronize()
         g = torch.cuda.CUDAGraph()
         s = torch.cuda.Stream()
         s.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(s):
             with torch.cuda.graph(g, stream=s):
-                self.run(dem)
+                self.run(dem, slc)
         torch.cuda.current_stream().wait_stream(s)
+        if slc is not None:
+            return g
         self.graph = g
+        return g
 
     def replay(self):
         self.graph.replay()
@@ -522,6 +532,66 @@ class BatchedFrameChain:
 
     def burst_pixels_all(self):
         return [p.lines * p.samples for p in self.plans]
+
+
+class FramePipeline:
+    """Frames streamed through one ``BatchedFrameChain`` with host buffers.
+
+    Two input slots (SLC buffer and DEM) alternate, each with its own CUDA
+    graph of the frame run: ``submit`` enqueues the host-to-device copy of a
+    frame's bursts (and DEM) on a copy stream, into the slot the frame before
+    last used once that frame's run is done, and, on the current stream, the
+    run and the device-to-host copy of the products.  So the copy of frame k + 1 crosses PCIe while frame k runs;
+    the frames' runs and product reads stay in order on one stream.  Nothing
+    synchronises the host: ``host_out`` holds frame k's products once the
+    current stream has passed its ``submit``.
+    """
+
+    def __init__(self, chain: BatchedFrameChain, dem):
+        self.chain = chain
+        self.slcs = [chain.slc, torch.empty_like(chain.slc)]
+        self.dems = [dem, dem.clone()]
+        self.views = []
+        for buf in self.slcs:
+            vs = []
+            for p, off in zip(chain.plans, chain.burst_offsets):
+                v = buf[off:off + p.lines * p.samples]
+                vs.append(v.view(p.lines, p.samples, 2) if chain.sample_format == "ci16" else v.view(p.lines, p.samples))
+            self.views.append(vs[0::2] + vs[1::2])  # the order of chain.ref_views + chain.sec_views
+        if chain.graph is None:
+            chain.capture(dem)
+        self.slcs[1].copy_(self.slcs[0])
+        self.graphs = [chain.graph, chain.capture(self.dems[1], self.slcs[1])]
+        self.copy = torch.cuda.Stream(chain.dev)
+        self.loaded = [torch.cuda.Event() for _ in range(2)]
+        self.done = [torch.cuda.Event() for _ in range(2)]
+        self.k = 0
+
+    def outputs(self):
+        return (self.chain.ifg, self.chain.amp1, self.chain.amp2, self.chain.coh, self.chain.filt)
+
+    def submit(self, host_bursts, host_dem=None, host_out=None):
+        """One frame: ``host_bursts`` are its bursts (reference then secondary
+        order of ``chain.ref_views + chain.sec_views``), ideally pinned;
+        ``host_dem`` its DEM (None: the slot keeps the one it has);
+        ``host_out`` optional pinned tensors like ``outputs()``."""
+        b = self.k & 1
+        cur = torch.cuda.current_stream(self.chain.dev)
+        if self.k >= 2:
+            self.copy.wait_event(self.done[b])  # the run that read this slot is over
+        with torch.cuda.stream(self.copy):
+            if host_dem is not None:
+                self.dems[b].copy_(host_dem, non_blocking=True)
+            for v, h in zip(self.views[b], host_bursts):
+                v.copy_(h.reshape(v.shape), non_blocking=True)
+            self.loaded[b].record(self.copy)
+        cur.wait_event(self.loaded[b])
+        self.graphs[b].replay()
+        if host_out is not None:
+            for h, o in zip(host_out, self.outputs()):
+                h.copy_(o, non_blocking=True)
+        self.done[b].record(cur)
+        self.k += 1
 
 
 def _call_frame(name, fn, *args):

@@ -13,6 +13,7 @@
 //   * FP64 phases are reduced mod 2 pi in FP64, then rotated in FP32;
 //   * the non-zero-row search is folded into the geocoding epilogue.
 #include <climits>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 #include "s1b.h"
@@ -73,6 +74,52 @@ __device__ __forceinline__ void deramp_tile(const s1b_burst_plan_t &P, const TIn
   }
   const bool two = (c0 + 1) < S;
   const double eta0 = -L * P.ati / 2.;
+  if constexpr (std::is_same<TIn, float2>::value) {
+    // complex64: rows in batches of 8 whose loads are all issued before any
+    // of their arithmetic (predicated, no early exit between them).  Measured
+    // 0.088 ms against 0.095 ms per 1500 x 21000 burst; the complex int16
+    // path, with half the bytes per load, measured slower this way (the
+    // batch halves the resident CTAs) and keeps the row loop below.
+    constexpr int B = 8;
+    static_assert(ROWS % B == 0, "deramp rows per tile");
+#pragma unroll 1
+    for (int rb = 0; rb < ROWS; rb += B) {
+      float2 a[B][2];
+#pragma unroll
+      for (int k = 0; k < B; ++k) {
+        const int r = r0 + rb + k;
+        const size_t base = (size_t)r * S + c0;
+        a[k][0] = a[k][1] = make_float2(0.f, 0.f);
+        if (r < L) {
+          if (kVec) {
+            load_pair(in + base, a[k][0], a[k][1]);
+          } else {
+            a[k][0] = load_one(in + base);
+            if (two) a[k][1] = load_one(in + base + 1);
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < B; ++k) {
+        const int r = r0 + rb + k;
+        if (r < L) {
+          const double eta = eta0 + r * P.ati;  // geo2rdr.cu:530-531
+          const size_t base = (size_t)r * S + c0;
+          const double d0 = eta - etaref[0];
+          const double d1 = eta - etaref[1];
+          const float2 b0 = cmul(a[k][0], phasor(mkt[0] * d0 * d0));
+          const float2 b1 = cmul(a[k][1], phasor(mkt[1] * d1 * d1));
+          if (kVec) {
+            __stcs(reinterpret_cast<float4 *>(out + base), make_float4(b0.x, b0.y, b1.x, b1.y));
+          } else {
+            __stcs(out + base, b0);
+            if (two) __stcs(out + base + 1, b1);
+          }
+        }
+      }
+    }
+    return;
+  }
 #pragma unroll 4
   for (int rr = 0; rr < ROWS; ++rr) {
     const int r = r0 + rr;
