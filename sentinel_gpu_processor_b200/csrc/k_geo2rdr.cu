@@ -167,7 +167,10 @@ __global__ __launch_bounds__(256) void deramp_kernel(const __grid_constant__ s1b
 // longitude terms depend only on the column and stay in registers.  Warps
 // cover 32 consecutive columns of a row, so DEM reads and output writes
 // coalesce; the next row's DEM sample is loaded one row ahead.
-constexpr int G_TX = 128, G_RY = 16;  // single-burst launch; the frame launch tunes the width
+// 32 rows per tile: the per-warp set-up (the centre pixel's exact Newton on
+// the orbit polynomial, FP64 row trigonometry) is amortised over twice the
+// rows of a 16-row tile (measured 11.15 -> 9.88 ms per 27-pair frame)
+constexpr int G_TX = 128, G_RY = 32;  // single-burst launch; the frame launch tunes the width
 
 __global__ void rows_init_kernel(int32_t *rows, int nrow) {
   rows[0] = nrow;
@@ -195,8 +198,8 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
   const double inv_dmrg = 1.0 / P.dmrg, prf = 1.0 / P.dtaz, two_over_c = 2.0 / kSolD;
   // One cubic orbit expansion per warp, at the zero-Doppler time of the
   // warp's centre pixel, solved on the window polynomial from the burst
-  // centre (geo2rdr.cu:588-600).  The warp's 32 x 16 pixels lie within
-  // ~0.1 s of it, where the dropped fourth-order term is < 1e-9 m.  Lanes 1
+  // centre (geo2rdr.cu:588-600).  The warp's 32 x 32 pixels lie within
+  // ~0.2 s of it, where the dropped fourth-order term is < 1e-9 m.  Lanes 1
   // and 2 solve two opposite corners at the same time; the three solutions
   // bound the warp's footprint in the burst, whose lines are prefetched into
   // L2 before the per-pixel solves, so the bilinear gathers hit L2.
@@ -249,7 +252,7 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
     const int l0 = max(0, (int)fmax(a0 - 2.0, -1.0)), l1 = min(P.lines - 1, (int)fmin(a1 + 3.0, 1e9));
     const int s0 = max(0, (int)fmax(g0 - 2.0, -1.0)), s1 = min(P.samples - 1, (int)fmin(g1 + 3.0, 1e9));
     const int nl = l1 - l0 + 1;
-    if (nl > 0 && nl <= 48 && s1 >= s0 && s1 - s0 < 256) {
+    if (nl > 0 && nl <= 96 && s1 >= s0 && s1 - s0 < 256) {
       const int nch = (((s1 - s0 + 1) * 8) + 127) / 128 + 1;  // 128-byte lines per burst line segment
       for (int k = lane; k < nl * nch; k += 32) {
         const int li = k / nch, ch = k - li * nch;
@@ -283,7 +286,7 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
       const ZeroDopplerPoint q = zero_doppler_point(zd, p);
       if (r == 0) {
         // the column's first point starts at the warp centre; its slope
-        // serves the whole column (f' changes by < 1e-4 over 16 rows)
+        // serves the whole column (f' changes by < 1e-3 over 32 rows)
         inv_c1 = rcp_newton(q.c1);
         hprev = -P.dtaz;
       } else {
@@ -337,7 +340,7 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
     }
   }
   // first / last non-zero output row (geo2rdr.cu:86-128): the warp's extent
-  // over its 16 rows, one reduction pair per warp and tile (per-row
+  // over its rows, one reduction pair per warp and tile (per-row
   // reductions on one address serialise in its L2 slice)
   rlo = __reduce_min_sync(0xffffffffu, rlo);
   rhi = __reduce_max_sync(0xffffffffu, rhi);

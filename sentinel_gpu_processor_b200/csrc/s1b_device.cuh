@@ -199,8 +199,8 @@ __device__ __forceinline__ void zero_doppler_cubic(const OrbitCubic &o, const do
 //   c3 = -(|a|^2/2 + (2/3) v.j)  (the same for every point),
 // and, since d|p - x|^2/dh = -2 f,
 //   |p - x(t0 + h)|^2 = |d|^2 - h (2 c0 + h (c1 + h ((2/3) c2 + h c3 / 2))).
-// The dropped h^4 term of f is (5/12)(a.j) h^4 < 1e-6 for |h| < 0.1 s
-// (a time error below 1e-14 s).  A point costs four dot products of d; each
+// The dropped h^4 term of f is (5/12)(a.j) h^4 < 5e-5 for |h| < 0.2 s
+// (a time error below 1e-12 s).  A point costs four dot products of d; each
 // Newton step three FMA.
 struct ZeroDopplerPatch {
   double t0, x[3], v[3], a[3], jh[3];  // jh = j / 2
