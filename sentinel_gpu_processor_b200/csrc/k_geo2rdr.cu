@@ -167,9 +167,11 @@ __global__ __launch_bounds__(256) void deramp_kernel(const __grid_constant__ s1b
 // longitude terms depend only on the column and stay in registers.  Warps
 // cover 32 consecutive columns of a row, so DEM reads and output writes
 // coalesce; the next row's DEM sample is loaded one row ahead.
-// 32 rows per tile: the per-warp set-up (the centre pixel's exact Newton on
-// the orbit polynomial, FP64 row trigonometry) is amortised over twice the
-// rows of a 16-row tile (measured 11.15 -> 9.88 ms per 27-pair frame)
+// Rows per tile (a multiple of 32): the per-warp set-up (the centre pixel's
+// exact Newton on the orbit polynomial, FP64 row trigonometry) is amortised
+// over the tile's rows.  Measured per 27-pair frame: 16 rows 11.15 ms, 32
+// rows 9.88 ms, 64 rows 9.41 ms (kFrameGeoRows); a single burst's grid is
+// too small for 64-row tiles (0.195 ms at 32 rows, 0.221 ms at 64).
 constexpr int G_TX = 128, G_RY = 32;  // single-burst launch; the frame launch tunes the width
 
 __global__ void rows_init_kernel(int32_t *rows, int nrow) {
@@ -177,21 +179,24 @@ __global__ void rows_init_kernel(int32_t *rows, int nrow) {
   rows[1] = -1;
 }
 
-template <int TX>
+template <int TX, int RY>
 __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const int16_t *__restrict__ dem,
                                              int64_t pitch, const float2 *__restrict__ burst,
                                              float2 *__restrict__ out, int32_t *__restrict__ rows, int nrow,
                                              int ncol, int tile_x, int tile_y) {
   const int tx = threadIdx.x, lane = tx & 31;
   const int col = tile_x * TX + tx;
-  const int row0 = tile_y * G_RY;
-  // llh->ECEF trigonometry (orbit.cu:20-27): row terms on lanes 0..15
+  static_assert(RY % 32 == 0, "tile rows");
+  const int row0 = tile_y * RY;
+  // llh->ECEF trigonometry (orbit.cu:20-27): lane l holds the row terms of
+  // row r + l for the current 32 rows r .. r + 31 of the tile
   double r_sin = 0.0, r_cos = 0.0, r_re = 0.0;
-  if (lane < G_RY) {
-    const double lat = (P.lat0 + (row0 + lane) * P.dlat) * kPiD / 180;
+  auto row_terms = [&](int r) {
+    const double lat = (P.lat0 + (row0 + r + lane) * P.dlat) * kPiD / 180;
     sincos(lat, &r_sin, &r_cos);
     r_re = kRaD / sqrt(1. - kRe2D * r_sin * r_sin);
-  }
+  };
+  row_terms(0);
   double sinlon, coslon;
   sincos((P.lon0 + col * P.dlon) * kPiD / 180, &sinlon, &coslon);
   const bool colok = col < ncol;
@@ -208,7 +213,7 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
   double faz = 0.0, frg = 0.0;
   if (lane < 3) {
     const int c0 = tile_x * TX + wid * 32;
-    const int cr = lane == 0 ? min(row0 + G_RY / 2, nrow - 1) : (lane == 1 ? row0 : min(row0 + G_RY - 1, nrow - 1));
+    const int cr = lane == 0 ? min(row0 + RY / 2, nrow - 1) : (lane == 1 ? row0 : min(row0 + RY - 1, nrow - 1));
     const int cc = lane == 0 ? min(c0 + 16, ncol - 1) : (lane == 1 ? min(c0, ncol - 1) : min(c0 + 31, ncol - 1));
     double sla, cla, slo, clo;
     sincos((P.lat0 + cr * P.dlat) * kPiD / 180, &sla, &cla);
@@ -252,7 +257,7 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
     const int l0 = max(0, (int)fmax(a0 - 2.0, -1.0)), l1 = min(P.lines - 1, (int)fmin(a1 + 3.0, 1e9));
     const int s0 = max(0, (int)fmax(g0 - 2.0, -1.0)), s1 = min(P.samples - 1, (int)fmin(g1 + 3.0, 1e9));
     const int nl = l1 - l0 + 1;
-    if (nl > 0 && nl <= 96 && s1 >= s0 && s1 - s0 < 256) {
+    if (nl > 0 && nl <= 3 * RY && s1 >= s0 && s1 - s0 < 256) {
       const int nch = (((s1 - s0 + 1) * 8) + 127) / 128 + 1;  // 128-byte lines per burst line segment
       for (int k = lane; k < nl * nch; k += 32) {
         const int li = k / nch, ch = k - li * nch;
@@ -267,14 +272,15 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
   const ZeroDopplerPatch &zd = s_zd[wid];
   const double k4_wvl = 4.0 / P.wvl;  // two-way range phase, half-cycles per metre
   double h = 0.0, hprev = 0.0, inv_c1 = 0.0;
-  const int rmax = min(G_RY, nrow - row0);
+  const int rmax = min(RY, nrow - row0);
   int16_t hn = colok && rmax > 0 ? __ldg(dem + (int64_t)row0 * pitch + col) : 0;
   int rlo = INT_MAX, rhi = -1;
   for (int r = 0; r < rmax; ++r) {
     const int row = row0 + r;
-    const double sinlat = __shfl_sync(0xffffffffu, r_sin, r);
-    const double coslat = __shfl_sync(0xffffffffu, r_cos, r);
-    const double re = __shfl_sync(0xffffffffu, r_re, r);
+    if (r > 0 && (r & 31) == 0) row_terms(r);  // the next 32 rows (warp-uniform)
+    const double sinlat = __shfl_sync(0xffffffffu, r_sin, r & 31);
+    const double coslat = __shfl_sync(0xffffffffu, r_cos, r & 31);
+    const double re = __shfl_sync(0xffffffffu, r_re, r & 31);
     const double hgt = (double)hn;
     if (colok && r + 1 < rmax) hn = __ldg(dem + (int64_t)(row + 1) * pitch + col);
     float2 res = make_float2(0.f, 0.f);
@@ -354,7 +360,7 @@ __global__ __launch_bounds__(G_TX) void geo2rdr_kernel(
     const __grid_constant__ s1b_burst_plan_t P, const int16_t *__restrict__ dem, int64_t pitch,
     const float2 *__restrict__ burst, float2 *__restrict__ out, int32_t *__restrict__ rows,
     int nrow, int ncol) {
-  geo2rdr_tile<G_TX>(P, dem, pitch, burst, out, rows, nrow, ncol, blockIdx.x, blockIdx.y);
+  geo2rdr_tile<G_TX, G_RY>(P, dem, pitch, burst, out, rows, nrow, ncol, blockIdx.x, blockIdx.y);
 }
 
 // ------------------------------------------------------------ frame stages
@@ -362,7 +368,6 @@ __global__ __launch_bounds__(G_TX) void geo2rdr_kernel(
 // Tiles are taken round-robin; the geocoding CTA copies the plan of the burst
 // it works on (orbit polynomials included) into shared memory when the burst
 // changes (consecutive tiles of a CTA usually stay in one burst).
-static_assert(G_RY == kFrameGeoRows, "geocoding tile rows");
 
 __global__ void frame_init_kernel(const FrameDev d, s1b_frame_pair_t *pout) {
   for (int b = threadIdx.x; b < d.n_bursts; b += blockDim.x) {
@@ -465,7 +470,7 @@ __global__ __launch_bounds__(TX) void frame_geo2rdr_kernel(const FrameDev d, con
     const int64_t local = idx - fb.geo_tile0;
     const int ty = (int)(local / tiles_x), tx = (int)(local - (int64_t)ty * tiles_x);
     const int16_t *dem = io.dem + (int64_t)sp.win_top * io.dem_pitch + sp.win_left;
-    geo2rdr_tile<TX>(sp, dem, io.dem_pitch, io.work + fb.der_off, io.work + fb.geo_off, d.rows + 2 * b,
+    geo2rdr_tile<TX, kFrameGeoRows>(sp, dem, io.dem_pitch, io.work + fb.der_off, io.work + fb.geo_off, d.rows + 2 * b,
                      fb.nrow, fb.ncol, tx, ty);
   }
 }
@@ -479,9 +484,9 @@ __global__ __launch_bounds__(TX) void frame_geo2rdr_grid_kernel(const FrameDev d
   const int b = blockIdx.z;
   const s1b_burst_plan_t &sp = d.plans[b];
   const FrameBurst &fb = d.bursts[b];
-  if ((int)blockIdx.x * TX >= fb.ncol || (int)blockIdx.y * G_RY >= fb.nrow) return;
+  if ((int)blockIdx.x * TX >= fb.ncol || (int)blockIdx.y * kFrameGeoRows >= fb.nrow) return;
   const int16_t *dem = io.dem + (int64_t)sp.win_top * io.dem_pitch + sp.win_left;
-  geo2rdr_tile<TX>(sp, dem, io.dem_pitch, io.work + fb.der_off, io.work + fb.geo_off, d.rows + 2 * b,
+  geo2rdr_tile<TX, kFrameGeoRows>(sp, dem, io.dem_pitch, io.work + fb.der_off, io.work + fb.geo_off, d.rows + 2 * b,
                    fb.nrow, fb.ncol, blockIdx.x, blockIdx.y);
 }
 

@@ -31,7 +31,23 @@ def _batched(cuda, frame):
     return bc
 
 
-def _check(res, want):
+@pytest.fixture(scope="module")
+def batched(cuda, frame):
+    """Products of one batched run at the default tuning (cloned)."""
+    from types import SimpleNamespace
+    bc = _batched(cuda, frame)
+    bc.run(frame.dem)
+    assert any(r["filtered"] for r in bc.pair_table())  # Goldstein ran on some pair
+    keys = ("ifg", "amp1", "amp2", "coh", "filt")
+    return [None if r is None else SimpleNamespace(header=list(r.header), box=tuple(r.box),
+                                                   gslc_headers=[list(h) for h in r.gslc_headers],
+                                                   **{k: getattr(r, k).clone() for k in keys})
+            for r in bc.results()]
+
+
+def _check(res, want, exact=True):
+    """Same pairs, headers, boxes and crops; products bit-identical (exact) or
+    within float rounding (1e-5 of each product's largest magnitude)."""
     assert len(res) == len(want)
     assert any(r is not None for r in res)
     for r, w in zip(res, want):
@@ -43,17 +59,30 @@ def _check(res, want):
         for a, b in zip(r.gslc_headers, w.gslc_headers):
             assert list(a) == list(b)
         for k in ("ifg", "amp1", "amp2", "coh", "filt"):
-            assert torch.equal(getattr(r, k), getattr(w, k)), k
+            x, y = getattr(r, k), getattr(w, k)
+            if exact:
+                assert torch.equal(x, y), k
+            else:
+                assert x.shape == y.shape, k
+                if k == "coh":
+                    # values of 1 up to rounding (windows with one non-zero
+                    # sample) land either side of the > 1 fill rule
+                    # (s1proc/coherence.py:143-144): compare away from it
+                    m = (x < 0.999) & (y < 0.999)
+                    assert float(m.float().mean()) > 0.9
+                    x, y = x[m], y[m]
+                assert float((x - y).abs().max()) <= 1e-5 * float(y.abs().max()), k
 
 
-def test_batched_frame_matches_per_pair_chain(cuda, frame, per_pair):
-    bc = _batched(cuda, frame)
-    bc.run(frame.dem)
-    _check(bc.results(), per_pair)
-    assert any(r["filtered"] for r in bc.pair_table())
+def test_batched_frame_matches_per_pair_chain(cuda, frame, per_pair, batched):
+    """The batched frame against the per-pair chain (single-burst entry
+    points).  The two geocode with different tile heights (64 rows in the
+    frame, 32 for a single burst), so each warp expands the orbit about a
+    different centre pixel: the products agree to float rounding."""
+    _check(batched, per_pair, exact=False)
 
 
-def test_graph_replay_after_autotune(cuda, frame, per_pair):
+def test_graph_replay_after_autotune(cuda, frame, batched):
     bc = _batched(cuda, frame)
     t = bc.autotune(frame.dem, reps=1)
     assert t["deramp_rows"] in (8, 16, 32) and t["geo_cols"] in (64, 128, 256)
@@ -63,18 +92,18 @@ def test_graph_replay_after_autotune(cuda, frame, per_pair):
         x.zero_()
     bc.replay()
     torch.cuda.synchronize()
-    _check(bc.results(), per_pair)
+    _check(bc.results(), batched)
     prof = bc.profile(frame.dem)
     assert set(prof) == {"deramp", "geo2rdr", "box", "crossmul_looks", "goldstein"}
     assert all(v >= 0.0 for v in prof.values())
 
 
 @pytest.mark.parametrize("tuning", [(8, 148, 64, 148), (32, 0, 256, 0), (16, 296, 128, 0)])
-def test_every_tile_shape_gives_the_same_products(cuda, frame, per_pair, tuning):
+def test_every_tile_shape_gives_the_same_products(cuda, frame, batched, tuning):
     bc = _batched(cuda, frame)
     bc.set_tuning(*tuning)
     bc.run(frame.dem)
-    _check(bc.results(), per_pair)
+    _check(bc.results(), batched)
 
 
 def test_frame_pipeline_matches_plain_runs(cuda, frame):
