@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--config", default="frame",
                     choices=["frame", "frame_pairs", "c1", "c1geo", "c0", "small", "adjoint"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--deramp", default="fused", choices=["fused", "kernel"],
+                    help="frame deramp: inside the geocoding's gathers, or a separate kernel writing deramped bursts")
     ap.add_argument("--samples", default="ci16", choices=["ci16", "c64"],
                     help="frame SLC sample type: complex int16 as in the measurement TIFF (widened on the GPU), "
                          "or complex64 as the reference's geo2rdr pipe carries it")
@@ -262,7 +264,7 @@ def _workload(args, rank, dev):
         from sentinel_gpu_processor_b200.chain import BatchedFrameChain
         sc = synth.make_frame(seed=20261203 + 2000 + rank, device=dev)
         chain = BatchedFrameChain(sc.ref, sc.sec, sc.rsc, sc.rowlook, sc.collook, sc.alpha, device=dev,
-                                  sample_format=args.samples)
+                                  sample_format=args.samples, deramp_fused=args.deramp == "fused")
         if args.samples == "ci16":
             for v, s in zip(chain.ref_views + chain.sec_views, sc.ref_slc + sc.sec_slc):
                 v.copy_(synth.cint16(s))
@@ -487,11 +489,19 @@ def _kernel_table(chain, sc, args, times, peak):
         res = [r for r in chain.last if r is not None]
         box_px = sum((r.box[2] - r.box[0]) * (r.box[3] - r.box[1]) for r in res)
         ml = sum(r.ifg.numel() for r in res)
-        # deramp: read one input sample (8 bytes complex64, 4 complex int16), write 8
+        # deramp: read one input sample (8 bytes complex64, 4 complex int16), write 8;
+        # fused, the stage only writes the column tables (16 bytes per column) and
+        # the geocoding reads the raw samples instead of the deramped copy
         din = 4 if getattr(chain, "sample_format", "c64") == "ci16" else 8
-        bytes_per = {"deramp": (din + 8) * burst,
-                     "geo2rdr": GEO_BYTES_PER_GEO_PX * geo + GEO_BYTES_PER_BURST_PX * burst,
-                     "crossmul_looks": 16 * box_px + 20 * ml, "goldstein": 16 * ml}
+        if getattr(chain, "deramp_fused", False):
+            cols = sum(p.samples for p in pls)
+            if "deramp" in times:
+                times["tops_table"] = times.pop("deramp")
+            bytes_per = {"tops_table": 16 * cols, "geo2rdr": GEO_BYTES_PER_GEO_PX * geo + din * burst + 16 * cols}
+        else:
+            bytes_per = {"deramp": (din + 8) * burst,
+                         "geo2rdr": GEO_BYTES_PER_GEO_PX * geo + GEO_BYTES_PER_BURST_PX * burst}
+        bytes_per.update({"crossmul_looks": 16 * box_px + 20 * ml, "goldstein": 16 * ml})
     else:
         pls = [p for pl in chain.pairs for p in pl] if args.config == "frame_pairs" else chain.plans
         n = len(pls)
@@ -573,7 +583,8 @@ def run_s1b(args):
                  "geo_px_total": sum(chain.geo_pixels()),
                  "ifg_ml_shapes_first3": [list(r.ifg.shape) for r in res[:3]],
                  "batched": True, "cuda_graph": True, "tuning": chain.tuned,
-                 "slc_samples": "complex int16" if args.samples == "ci16" else "complex64"}
+                 "slc_samples": "complex int16" if args.samples == "ci16" else "complex64",
+                 "deramp": "fused into the geocoding gathers" if chain.deramp_fused else "separate kernel"}
         launches = chain.launches_per_step()
     elif args.config == "frame_pairs":
         extra = {"burst_pairs": len(chain.pairs), "burst_px_per_step": chain.burst_pixels,
@@ -591,7 +602,9 @@ def run_s1b(args):
     traffic = None
     if top == "geo2rdr":
         if args.config == "frame":  # one launch geocodes every burst
-            traffic = GEO_DRAM_BYTES_PER_GEO_PX * sum(p.nrow * p.ncol for p in chain.plans)
+            # ncu traffic per geo pixel was measured on the unfused kernel
+            traffic = (None if chain.deramp_fused
+                       else GEO_DRAM_BYTES_PER_GEO_PX * sum(p.nrow * p.ncol for p in chain.plans))
         else:
             pls = [p for pl in chain.pairs for p in pl] if args.config == "frame_pairs" else chain.plans
             traffic = GEO_DRAM_BYTES_PER_GEO_PX * sum(p.nrow * p.ncol for p in pls) / len(pls)

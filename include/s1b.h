@@ -449,6 +449,14 @@ int s1b_frame_burst_offset(const s1b_frame_t *frame, int32_t burst, int64_t *slc
  * widened in the deramp stage).  Offsets and slc_elems count samples either
  * way.  Products are identical for the same integer-valued samples. */
 int s1b_frame_set_sample_format(s1b_frame_t *frame, int32_t format);
+/* Deramp stage of later runs (no reference counterpart; the reference
+ * deramps a burst in its own kernel, csrc/src/geo2rdr.cu:138-158):
+ * 1 (the default): the geocoding deramps the four samples of each bilinear
+ * gather where it reads them, from the burst's raw samples and a per-column
+ * coefficient table (no deramped copy of any burst is written); 0: a deramp
+ * kernel writes every burst's deramped copy and the geocoding reads it.  The
+ * products are bit-identical either way. */
+int s1b_frame_set_deramp_fusion(s1b_frame_t *frame, int32_t fused);
 /* Slot of pair k in the product arrays: first element and capacity. */
 int s1b_frame_pair_slot(const s1b_frame_t *frame, int32_t pair, int64_t *ml_off, int32_t *max_nrow_ml,
                         int32_t *max_ncol_ml);

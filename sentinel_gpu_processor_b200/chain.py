@@ -326,14 +326,17 @@ class BatchedFrameChain:
     The SLCs live back to back in one device buffer; ``ref_views``/``sec_views``
     are the per-burst views to fill.  ``sample_format="ci16"`` keeps them as
     the measurement TIFF's complex int16 samples (int16 [lines, samples, 2],
-    half the bytes to move and to read), widened in the deramp stage; the
+    half the bytes to move and to read), widened where they are read; the
     products equal those of the complex64 buffer holding the same values.
+    ``deramp_fused`` (default): the geocoding deramps the samples of each
+    bilinear gather itself (no deramped copy of the bursts); False runs a
+    deramp kernel first.  The products are bit-identical either way.
     ``autotune`` picks the deramp and geocoding tile shapes and grid sizes on
     the actual frame.
     """
 
     def __init__(self, refs, secs, rsc, rowlook, collook, alpha, n_win=32, device="cuda", fill_seed=0,
-                 sample_format="c64"):
+                 sample_format="c64", deramp_fused=True):
         import ctypes
         if sample_format not in ("c64", "ci16"):
             raise ValueError("sample_format must be 'c64' (complex64) or 'ci16' (complex int16)")
@@ -362,6 +365,8 @@ class BatchedFrameChain:
         self._handle = handle
         if sample_format == "ci16":
             _lib.check(lib.s1b_frame_set_sample_format(handle, _lib.S1B_SAMPLES_CI16), "s1b_frame_set_sample_format")
+        self.deramp_fused = bool(deramp_fused)
+        _lib.check(lib.s1b_frame_set_deramp_fusion(handle, int(self.deramp_fused)), "s1b_frame_set_deramp_fusion")
         sz = _lib.FrameSizes()
         _lib.check(lib.s1b_frame_sizes(handle, ctypes.byref(sz)), "s1b_frame_sizes")
         self.sizes = sz
@@ -518,7 +523,7 @@ class BatchedFrameChain:
         CTA-per-tile launch per load width (16-byte rows or not) and per list
         of up to FRAME_LIST_MAX bursts."""
         t = self.tuning()
-        if t["deramp_ctas"]:
+        if self.deramp_fused or t["deramp_ctas"]:  # column tables, or one persistent deramp
             return 7
         base = self.slc.data_ptr()
         es = 4 if self.sample_format == "ci16" else 8

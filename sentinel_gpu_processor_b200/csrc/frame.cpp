@@ -152,6 +152,7 @@ extern "C" int s1b_frame_create(const s1b_burst_plan_t *plans, int32_t n_bursts,
   if (rowlook < 1 || collook < 1) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_frame_create: bad looks");
   if (n_win != 32) return s1b_fail(S1B_ERR_UNSUPPORTED, "s1b_frame_create: only n_win = 32 is implemented");
   s1b_frame *f = new s1b_frame();
+  f->dev.fused_deramp = 1;  // the geocoding deramps its gathers (s1b_frame_set_deramp_fusion)
   if (cudaGetDevice(&f->device) != cudaSuccess) {
     delete f;
     return s1b_fail(S1B_ERR_NO_DEVICE, "s1b_frame_create: no CUDA device");
@@ -292,6 +293,12 @@ extern "C" int s1b_frame_tuning(const s1b_frame_t *f, int32_t tuning[4]) {
   return S1B_OK;
 }
 
+extern "C" int s1b_frame_set_deramp_fusion(s1b_frame_t *f, int32_t fused) {
+  if (!f) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_frame_set_deramp_fusion: null frame");
+  f->dev.fused_deramp = fused ? 1 : 0;
+  return S1B_OK;
+}
+
 extern "C" int s1b_frame_set_sample_format(s1b_frame_t *f, int32_t format) {
   if (!f) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_frame_set_sample_format: null frame");
   if (format != S1B_SAMPLES_C64 && format != S1B_SAMPLES_CI16)
@@ -302,7 +309,7 @@ extern "C" int s1b_frame_set_sample_format(s1b_frame_t *f, int32_t format) {
 
 extern "C" int s1b_frame_set_tuning(s1b_frame_t *f, const int32_t tuning[4]) {
   if (!f || !tuning) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_frame_set_tuning: null argument");
-  if (frame_max_ctas_deramp(tuning[0]) <= 0 || frame_max_ctas_geo2rdr(tuning[2]) <= 0)
+  if (frame_max_ctas_deramp(tuning[0]) <= 0 || frame_max_ctas_geo2rdr(f->dev, tuning[2]) <= 0)
     return s1b_fail(S1B_ERR_UNSUPPORTED, "s1b_frame_set_tuning: deramp rows 8/16/32, geocoding columns 64/128/256");
   if (tuning[1] < 0 || tuning[3] < 0)
     return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_frame_set_tuning: negative CTA count");
@@ -351,10 +358,16 @@ extern "C" int s1b_frame_autotune(s1b_frame_t *f, const void *slc, const int16_t
   s = frame_launch_init(f->dev, io, st);
   const int shapes[2][3] = {{8, 16, 32}, {64, 128, 256}};
   for (int stage = 0; stage < 2 && !s; ++stage) {
+    if (stage == 0 && f->dev.fused_deramp) {
+      // nothing to tune: one launch writes the column tables the geocoding
+      // candidates read
+      s = frame_launch_deramp(f->dev, io, f->tuning[0], f->tuning[1], f->split, st);
+      continue;
+    }
     int best_shape = f->tuning[stage * 2], best_ctas = f->tuning[stage * 2 + 1];
     float best = 3.4e38f;
     for (int shape : shapes[stage]) {
-      const int full = stage == 0 ? frame_max_ctas_deramp(shape) : frame_max_ctas_geo2rdr(shape);
+      const int full = stage == 0 ? frame_max_ctas_deramp(shape) : frame_max_ctas_geo2rdr(f->dev, shape);
       const int per_sm = sms > 0 ? full / sms : 0;
       // one CTA per tile (0), then persistent grids of 1..per_sm CTAs per SM
       for (int j = 0; j <= per_sm && !s; ++j) {

@@ -51,6 +51,29 @@ __device__ __forceinline__ float2 load_one(const short2 *p) {
   return make_float2((float)v.x, (float)v.y);
 }
 
+// TOPS deramp coefficients of burst column c (geo2rdr.cu:533-541): -pi kt
+// and etaref.  One function for the deramp kernels and the frame's column
+// table, so the fused geocoding forms exactly the deramp kernel's phases.
+__device__ __forceinline__ void tops_column(const s1b_burst_plan_t &P, int c, double &mkt, double &etaref) {
+  const double tr = P.slant_range_time + c / P.range_sampling_rate;
+  double dt = tr - P.fm[0];
+  const double ka = P.fm[1] + dt * (P.fm[2] + P.fm[3] * dt);
+  dt = tr - P.dc[0];
+  const double fnc = P.dc[1] + dt * (P.dc[2] + P.dc[3] * dt);
+  const double kt = ka * P.ks / (ka - P.ks);
+  mkt = -kPiD * kt;
+  etaref = -fnc / ka - P.etac0;
+}
+
+// Deramped sample of line r: a * exp(i mkt (eta_r - etaref)^2), eta_r =
+// -L ati / 2 + r ati (geo2rdr.cu:530-531, 151-152).
+__device__ __forceinline__ float2 deramp_sample(const s1b_burst_plan_t &P, float2 a, int r, double mkt,
+                                                double etaref) {
+  const double eta = -P.lines * P.ati / 2. + r * P.ati;
+  const double d = eta - etaref;
+  return cmul(a, phasor(mkt * d * d));
+}
+
 template <bool kVec, int ROWS, typename TIn>
 __device__ __forceinline__ void deramp_tile(const s1b_burst_plan_t &P, const TIn *__restrict__ in,
                                             float2 *__restrict__ out, int tile_x, int tile_y) {
@@ -61,19 +84,8 @@ __device__ __forceinline__ void deramp_tile(const s1b_burst_plan_t &P, const TIn
   // geo2rdr.cu:533-541 for the thread's two columns: -pi*kt and etaref
   double mkt[2], etaref[2];
 #pragma unroll
-  for (int j = 0; j < 2; ++j) {
-    const int c = c0 + j < S ? c0 + j : c0;
-    const double tr = P.slant_range_time + c / P.range_sampling_rate;
-    double dt = tr - P.fm[0];
-    const double ka = P.fm[1] + dt * (P.fm[2] + P.fm[3] * dt);
-    dt = tr - P.dc[0];
-    const double fnc = P.dc[1] + dt * (P.dc[2] + P.dc[3] * dt);
-    const double kt = ka * P.ks / (ka - P.ks);
-    mkt[j] = -kPiD * kt;
-    etaref[j] = -fnc / ka - P.etac0;
-  }
+  for (int j = 0; j < 2; ++j) tops_column(P, c0 + j < S ? c0 + j : c0, mkt[j], etaref[j]);
   const bool two = (c0 + 1) < S;
-  const double eta0 = -L * P.ati / 2.;
   if constexpr (std::is_same<TIn, float2>::value) {
     // complex64: rows in batches of 8 whose loads are all issued before any
     // of their arithmetic (predicated, no early exit between them).  Measured
@@ -103,12 +115,9 @@ __device__ __forceinline__ void deramp_tile(const s1b_burst_plan_t &P, const TIn
       for (int k = 0; k < B; ++k) {
         const int r = r0 + rb + k;
         if (r < L) {
-          const double eta = eta0 + r * P.ati;  // geo2rdr.cu:530-531
           const size_t base = (size_t)r * S + c0;
-          const double d0 = eta - etaref[0];
-          const double d1 = eta - etaref[1];
-          const float2 b0 = cmul(a[k][0], phasor(mkt[0] * d0 * d0));
-          const float2 b1 = cmul(a[k][1], phasor(mkt[1] * d1 * d1));
+          const float2 b0 = deramp_sample(P, a[k][0], r, mkt[0], etaref[0]);
+          const float2 b1 = deramp_sample(P, a[k][1], r, mkt[1], etaref[1]);
           if (kVec) {
             __stcs(reinterpret_cast<float4 *>(out + base), make_float4(b0.x, b0.y, b1.x, b1.y));
           } else {
@@ -124,7 +133,6 @@ __device__ __forceinline__ void deramp_tile(const s1b_burst_plan_t &P, const TIn
   for (int rr = 0; rr < ROWS; ++rr) {
     const int r = r0 + rr;
     if (r >= L) break;
-    const double eta = eta0 + r * P.ati;  // geo2rdr.cu:530-531
     const size_t base = (size_t)r * S + c0;
     float2 a0, a1;
     if (kVec) {
@@ -133,10 +141,8 @@ __device__ __forceinline__ void deramp_tile(const s1b_burst_plan_t &P, const TIn
       a0 = load_one(in + base);
       a1 = two ? load_one(in + base + 1) : make_float2(0.f, 0.f);
     }
-    const double d0 = eta - etaref[0];
-    const double d1 = eta - etaref[1];
-    const float2 b0 = cmul(a0, phasor(mkt[0] * d0 * d0));
-    const float2 b1 = cmul(a1, phasor(mkt[1] * d1 * d1));
+    const float2 b0 = deramp_sample(P, a0, r, mkt[0], etaref[0]);
+    const float2 b1 = deramp_sample(P, a1, r, mkt[1], etaref[1]);
     if (kVec) {
       __stcs(reinterpret_cast<float4 *>(out + base), make_float4(b0.x, b0.y, b1.x, b1.y));
     } else {
@@ -179,11 +185,26 @@ __global__ void rows_init_kernel(int32_t *rows, int nrow) {
   rows[1] = -1;
 }
 
-template <int TX, int RY>
+// Read-only (L1-cached) sample loads for the bilinear gathers.
+__device__ __forceinline__ float2 load_ro(const float2 *p) { return __ldg(p); }
+__device__ __forceinline__ float2 load_ro(const short2 *p) {
+  const short2 v = __ldg(p);
+  return make_float2((float)v.x, (float)v.y);
+}
+
+// Geocoding of one tile.  Unfused (kFused false): `burst` is the deramped
+// burst (complex64).  Fused: `burst` holds the raw samples (complex64 or
+// complex int16) and `tops` the burst's per-column deramp coefficients
+// (-pi kt, etaref); each of the four bilinear samples is deramped where it is
+// gathered, with the deramp kernel's own expressions (deramp_sample), so the
+// result equals the unfused path's bit for bit and the deramped copy of the
+// burst is never written.
+template <int TX, int RY, typename TSrc = float2, bool kFused = false>
 __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const int16_t *__restrict__ dem,
-                                             int64_t pitch, const float2 *__restrict__ burst,
+                                             int64_t pitch, const TSrc *__restrict__ burst,
                                              float2 *__restrict__ out, int32_t *__restrict__ rows, int nrow,
-                                             int ncol, int tile_x, int tile_y) {
+                                             int ncol, int tile_x, int tile_y,
+                                             const double2 *__restrict__ tops = nullptr) {
   const int tx = threadIdx.x, lane = tx & 31;
   const int col = tile_x * TX + tx;
   static_assert(RY % 32 == 0, "tile rows");
@@ -258,10 +279,10 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
     const int s0 = max(0, (int)fmax(g0 - 2.0, -1.0)), s1 = min(P.samples - 1, (int)fmin(g1 + 3.0, 1e9));
     const int nl = l1 - l0 + 1;
     if (nl > 0 && nl <= 3 * RY && s1 >= s0 && s1 - s0 < 256) {
-      const int nch = (((s1 - s0 + 1) * 8) + 127) / 128 + 1;  // 128-byte lines per burst line segment
+      const int nch = (((s1 - s0 + 1) * (int)sizeof(TSrc)) + 127) / 128 + 1;  // 128-byte lines per line segment
       for (int k = lane; k < nl * nch; k += 32) {
         const int li = k / nch, ch = k - li * nch;
-        const float2 *ptr = burst + (size_t)(l0 + li) * P.samples + s0;
+        const TSrc *ptr = burst + (size_t)(l0 + li) * P.samples + s0;
         const char *line = reinterpret_cast<const char *>(ptr) + ch * 128;
         if (line <= reinterpret_cast<const char *>(burst + (size_t)(l0 + li) * P.samples + s1))
           asm volatile("prefetch.global.L2 [%0];" ::"l"(line));
@@ -329,8 +350,19 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
         // bilinear interpolation of the deramped burst (geo2rdr.cu:220-237)
         const float fr = (float)(rgoff - intr), fa = (float)(azoff - inta);
         const size_t i1 = (size_t)inta * P.samples + intr;
-        const float2 b1 = __ldg(burst + i1), b2 = __ldg(burst + i1 + 1);
-        const float2 b3 = __ldg(burst + i1 + P.samples), b4 = __ldg(burst + i1 + P.samples + 1);
+        float2 b1, b2, b3, b4;
+        if constexpr (kFused) {
+          const double2 t0 = __ldg(tops + intr), t1 = __ldg(tops + intr + 1);
+          b1 = deramp_sample(P, load_ro(burst + i1), inta, t0.x, t0.y);
+          b2 = deramp_sample(P, load_ro(burst + i1 + 1), inta, t1.x, t1.y);
+          b3 = deramp_sample(P, load_ro(burst + i1 + P.samples), inta + 1, t0.x, t0.y);
+          b4 = deramp_sample(P, load_ro(burst + i1 + P.samples + 1), inta + 1, t1.x, t1.y);
+        } else {
+          b1 = __ldg(burst + i1);
+          b2 = __ldg(burst + i1 + 1);
+          b3 = __ldg(burst + i1 + P.samples);
+          b4 = __ldg(burst + i1 + P.samples + 1);
+        }
         const float2 c1 = make_float2(fmaf(fr, b2.x - b1.x, b1.x), fmaf(fr, b2.y - b1.y, b1.y));
         const float2 c2 = make_float2(fmaf(fr, b4.x - b3.x, b3.x), fmaf(fr, b4.y - b3.y, b3.y));
         const float2 v = make_float2(fmaf(fa, c2.x - c1.x, c1.x), fmaf(fa, c2.y - c1.y, c1.y));
@@ -455,7 +487,36 @@ void launch_deramp_grid(const FrameDev &d, const FrameIO &io, int rows, const in
   }
 }
 
-template <int TX>
+// One tile of the frame's geocoding: unfused from the burst's deramped copy,
+// fused from its raw samples and its column table (both at der_off).
+template <int TX, typename TSrc, bool kFused>
+__device__ __forceinline__ void frame_geo_tile(const s1b_burst_plan_t &sp, const FrameBurst &fb, const FrameIO &io,
+                                               int32_t *rows, int tx, int ty) {
+  const int16_t *dem = io.dem + (int64_t)sp.win_top * io.dem_pitch + sp.win_left;
+  if constexpr (kFused)
+    geo2rdr_tile<TX, kFrameGeoRows, TSrc, true>(sp, dem, io.dem_pitch, static_cast<const TSrc *>(io.slc) + fb.slc_off,
+                                                io.work + fb.geo_off, rows, fb.nrow, fb.ncol, tx, ty,
+                                                reinterpret_cast<const double2 *>(io.work + fb.der_off));
+  else
+    geo2rdr_tile<TX, kFrameGeoRows>(sp, dem, io.dem_pitch, io.work + fb.der_off, io.work + fb.geo_off, rows, fb.nrow,
+                                    fb.ncol, tx, ty);
+}
+
+// Per-column deramp coefficients (-pi kt, etaref) of every burst for the
+// fused geocoding: blockIdx.y = burst, a thread per column, written as
+// double2 into the burst's deramped-copy slot of the workspace (unused when
+// fused).
+__global__ void frame_tops_table_kernel(const FrameDev d, const FrameIO io) {
+  const int b = blockIdx.y;
+  const s1b_burst_plan_t &sp = d.plans[b];
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= sp.samples) return;
+  double mkt, eref;
+  tops_column(sp, c, mkt, eref);
+  reinterpret_cast<double2 *>(io.work + d.bursts[b].der_off)[c] = make_double2(mkt, eref);
+}
+
+template <int TX, typename TSrc, bool kFused>
 __global__ __launch_bounds__(TX) void frame_geo2rdr_kernel(const FrameDev d, const FrameIO io) {
   __shared__ __align__(16) s1b_burst_plan_t sp;
   int cur = -1;
@@ -469,9 +530,7 @@ __global__ __launch_bounds__(TX) void frame_geo2rdr_kernel(const FrameDev d, con
     const int tiles_x = (fb.ncol + TX - 1) / TX;
     const int64_t local = idx - fb.geo_tile0;
     const int ty = (int)(local / tiles_x), tx = (int)(local - (int64_t)ty * tiles_x);
-    const int16_t *dem = io.dem + (int64_t)sp.win_top * io.dem_pitch + sp.win_left;
-    geo2rdr_tile<TX, kFrameGeoRows>(sp, dem, io.dem_pitch, io.work + fb.der_off, io.work + fb.geo_off, d.rows + 2 * b,
-                     fb.nrow, fb.ncol, tx, ty);
+    frame_geo_tile<TX, TSrc, kFused>(sp, fb, io, d.rows + 2 * b, tx, ty);
   }
 }
 
@@ -479,15 +538,13 @@ __global__ __launch_bounds__(TX) void frame_geo2rdr_kernel(const FrameDev d, con
 // window; the plan is read through the table (uniform, L1-resident loads)
 // instead of a shared-memory copy, which keeps the single-burst register
 // budget.  The grid spans the largest window; CTAs past a smaller one return.
-template <int TX>
+template <int TX, typename TSrc, bool kFused>
 __global__ __launch_bounds__(TX) void frame_geo2rdr_grid_kernel(const FrameDev d, const FrameIO io) {
   const int b = blockIdx.z;
   const s1b_burst_plan_t &sp = d.plans[b];
   const FrameBurst &fb = d.bursts[b];
   if ((int)blockIdx.x * TX >= fb.ncol || (int)blockIdx.y * kFrameGeoRows >= fb.nrow) return;
-  const int16_t *dem = io.dem + (int64_t)sp.win_top * io.dem_pitch + sp.win_left;
-  geo2rdr_tile<TX, kFrameGeoRows>(sp, dem, io.dem_pitch, io.work + fb.der_off, io.work + fb.geo_off, d.rows + 2 * b,
-                   fb.nrow, fb.ncol, blockIdx.x, blockIdx.y);
+  frame_geo_tile<TX, TSrc, kFused>(sp, fb, io, d.rows + 2 * b, blockIdx.x, blockIdx.y);
 }
 
 template <typename K>
@@ -690,13 +747,19 @@ int frame_max_ctas_deramp(int rows) {
   }
 }
 
-int frame_max_ctas_geo2rdr(int cols) {
+template <typename TSrc, bool kFused>
+int max_ctas_geo(int cols) {
   switch (cols) {
-    case 64: return resident_ctas(frame_geo2rdr_kernel<64>, 64);
-    case 128: return resident_ctas(frame_geo2rdr_kernel<128>, 128);
-    case 256: return resident_ctas(frame_geo2rdr_kernel<256>, 256);
+    case 64: return resident_ctas(frame_geo2rdr_kernel<64, TSrc, kFused>, 64);
+    case 128: return resident_ctas(frame_geo2rdr_kernel<128, TSrc, kFused>, 128);
+    case 256: return resident_ctas(frame_geo2rdr_kernel<256, TSrc, kFused>, 256);
     default: return 0;
   }
+}
+
+int frame_max_ctas_geo2rdr(const FrameDev &d, int cols) {
+  if (!d.fused_deramp) return max_ctas_geo<float2, false>(cols);
+  return d.sample_format == S1B_SAMPLES_CI16 ? max_ctas_geo<short2, true>(cols) : max_ctas_geo<float2, true>(cols);
 }
 
 int frame_launch_deramp(const FrameDev &d, const FrameIO &io, int rows, int ctas, const FrameDerampSplit &split,
@@ -704,6 +767,11 @@ int frame_launch_deramp(const FrameDev &d, const FrameIO &io, int rows, int ctas
   const int full = frame_max_ctas_deramp(rows);
   if (full <= 0) return s1b_fail(S1B_ERR_UNSUPPORTED, "frame deramp: tile rows must be 8, 16 or 32");
   if (d.n_deramp_tiles == 0) return S1B_OK;
+  if (d.fused_deramp) {  // the geocoding deramps its gathers: only the column tables
+    const int ncols = d.deramp_tiles_x * kFrameDerampCols;
+    frame_tops_table_kernel<<<dim3((unsigned)((ncols + 255) / 256), (unsigned)d.n_bursts), 256, 0, st>>>(d, io);
+    return s1b_launch_status();
+  }
   const bool ci16 = d.sample_format == S1B_SAMPLES_CI16;
   if (ctas == 0) {  // one CTA per tile, one launch per load width
     if (ci16) {
@@ -733,25 +801,32 @@ int frame_launch_deramp(const FrameDev &d, const FrameIO &io, int rows, int ctas
   return s1b_launch_status();
 }
 
-int frame_launch_geo2rdr(const FrameDev &d, const FrameIO &io, int cols, int ctas, cudaStream_t st) {
-  const int full = frame_max_ctas_geo2rdr(cols);
+template <typename TSrc, bool kFused>
+int launch_geo(const FrameDev &d, const FrameIO &io, int cols, int ctas, cudaStream_t st) {
+  const int full = max_ctas_geo<TSrc, kFused>(cols);
   if (full <= 0) return s1b_fail(S1B_ERR_UNSUPPORTED, "frame geo2rdr: tile columns must be 64, 128 or 256");
   if (d.n_geo_tiles == 0) return S1B_OK;
   if (ctas == 0) {  // one CTA per tile
     const dim3 grid((unsigned)d.geo_tiles_x, (unsigned)d.geo_tiles_y, (unsigned)d.n_bursts);
     switch (cols) {
-      case 64: frame_geo2rdr_grid_kernel<64><<<grid, 64, 0, st>>>(d, io); break;
-      case 128: frame_geo2rdr_grid_kernel<128><<<grid, 128, 0, st>>>(d, io); break;
-      default: frame_geo2rdr_grid_kernel<256><<<grid, 256, 0, st>>>(d, io); break;
+      case 64: frame_geo2rdr_grid_kernel<64, TSrc, kFused><<<grid, 64, 0, st>>>(d, io); break;
+      case 128: frame_geo2rdr_grid_kernel<128, TSrc, kFused><<<grid, 128, 0, st>>>(d, io); break;
+      default: frame_geo2rdr_grid_kernel<256, TSrc, kFused><<<grid, 256, 0, st>>>(d, io); break;
     }
     return s1b_launch_status();
   }
   long long g = ctas < full ? ctas : full;
   if (g > d.n_geo_tiles) g = d.n_geo_tiles;
   switch (cols) {
-    case 64: frame_geo2rdr_kernel<64><<<(unsigned)g, 64, 0, st>>>(d, io); break;
-    case 128: frame_geo2rdr_kernel<128><<<(unsigned)g, 128, 0, st>>>(d, io); break;
-    default: frame_geo2rdr_kernel<256><<<(unsigned)g, 256, 0, st>>>(d, io); break;
+    case 64: frame_geo2rdr_kernel<64, TSrc, kFused><<<(unsigned)g, 64, 0, st>>>(d, io); break;
+    case 128: frame_geo2rdr_kernel<128, TSrc, kFused><<<(unsigned)g, 128, 0, st>>>(d, io); break;
+    default: frame_geo2rdr_kernel<256, TSrc, kFused><<<(unsigned)g, 256, 0, st>>>(d, io); break;
   }
   return s1b_launch_status();
+}
+
+int frame_launch_geo2rdr(const FrameDev &d, const FrameIO &io, int cols, int ctas, cudaStream_t st) {
+  if (!d.fused_deramp) return launch_geo<float2, false>(d, io, cols, ctas, st);
+  return d.sample_format == S1B_SAMPLES_CI16 ? launch_geo<short2, true>(d, io, cols, ctas, st)
+                                             : launch_geo<float2, true>(d, io, cols, ctas, st);
 }

@@ -45,6 +45,7 @@ struct FrameDev {
   int32_t deramp_tiles_x, deramp_tiles_y;  // deramp tiles of the largest burst, per axis
   int32_t geo_tiles_x, geo_tiles_y;        // geocoding tiles of the largest window, per axis
   int32_t sample_format;                   // S1B_SAMPLES_C64 or S1B_SAMPLES_CI16
+  int32_t fused_deramp;                    // 1: geocoding deramps its gathers (column tables only)
 };
 
 // Run-time buffers of one frame launch sequence.
@@ -83,7 +84,7 @@ int frame_launch_deramp(const FrameDev &d, const FrameIO &io, int rows_per_tile,
                         const FrameDerampSplit &split, cudaStream_t st);
 int frame_launch_geo2rdr(const FrameDev &d, const FrameIO &io, int cols_per_tile, int ctas, cudaStream_t st);
 int frame_max_ctas_deramp(int rows_per_tile);
-int frame_max_ctas_geo2rdr(int cols_per_tile);
+int frame_max_ctas_geo2rdr(const FrameDev &d, int cols_per_tile);
 int frame_launch_box(const FrameDev &d, const FrameIO &io, cudaStream_t st);
 int frame_launch_crossmul(const FrameDev &d, const FrameIO &io, cudaStream_t st);
 int frame_launch_goldstein(const FrameDev &d, const FrameIO &io, cudaStream_t st);

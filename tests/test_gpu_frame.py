@@ -135,3 +135,29 @@ def test_frame_pipeline_matches_plain_runs(cuda, frame):
         for g, x in zip(got, w):
             assert torch.equal(torch.view_as_real(g) if g.is_complex() else g,
                                torch.view_as_real(x) if x.is_complex() else x)
+
+
+@pytest.mark.parametrize("fmt", ["c64", "ci16"])
+def test_fused_deramp_matches_deramp_kernel(cuda, frame, fmt):
+    """The geocoding that deramps its own gathers (from the raw samples and
+    the column tables) gives the products of the deramp kernel + geocoding
+    path bit for bit: both form each deramped sample with the same code."""
+    outs = []
+    for fused in (True, False):
+        bc = BatchedFrameChain(frame.ref, frame.sec, frame.rsc, frame.rowlook, frame.collook, frame.alpha,
+                               device=cuda, sample_format=fmt, deramp_fused=fused)
+        if fmt == "ci16":
+            for v, s in zip(bc.ref_views + bc.sec_views, frame.ref_slc + frame.sec_slc):
+                v.copy_(synth.cint16(s))
+        else:
+            bc.load(frame.ref_slc, frame.sec_slc)
+        bc.run(frame.dem)
+        outs.append([None if r is None else [getattr(r, k).clone() for k in ("ifg", "amp1", "amp2", "coh", "filt")]
+                     for r in bc.results()])
+        assert bc.launches_per_step() >= 7
+    assert any(r is not None for r in outs[0])
+    for a, b in zip(*outs):
+        assert (a is None) == (b is None)
+        if a is not None:
+            for x, y in zip(a, b):
+                assert torch.equal(x, y)
