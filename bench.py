@@ -48,6 +48,10 @@ GEO_BYTES_PER_BURST_PX = 8
 # the TMA resampler per output pixel (31.5 M px: 550.9 + 228.7 MB).  Both
 # kernels stream their inputs once, so traffic scales with the unit count.
 GEO_DRAM_BYTES_PER_GEO_PX = 22.81
+# fused frame geocoding (deramp in the gathers): ncu DRAM traffic over algorithmic
+# bytes on the small frame (487.1 MB / 496.2 MB, profiles/geo2rdr_frame_fused.md);
+# both terms (raw samples read, geocoded pixels written) scale with the frame
+GEO_FUSED_TRAFFIC_RATIO = 0.982
 RESAMPLE_DRAM_BYTES_PER_PX = 24.75
 
 
@@ -58,7 +62,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="s1b", choices=["s1b", "reference"])
     ap.add_argument("--config", default="frame",
-                    choices=["frame", "frame_pairs", "c1", "c1geo", "c0", "small", "adjoint"])
+                    choices=["frame", "frame_small", "frame_pairs", "c1", "c1geo", "c0", "small", "adjoint"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--deramp", default="fused", choices=["fused", "kernel"],
                     help="frame deramp: inside the geocoding's gathers, or a separate kernel writing deramped bursts")
@@ -207,6 +211,11 @@ def peaks():
         return 6650.0, "fallback"
 
 
+# the batched frame: the full IW frame, and a small one (1 subswath x 3 bursts
+# at half size, default tuning) for quick runs and profiler captures
+FRAME_CONFIGS = ("frame", "frame_small")
+
+
 def make_scene(config, seed, device):
     from sentinel_gpu_processor_b200 import synth
     return synth.make_pair(config, seed=seed, device=device)
@@ -258,11 +267,13 @@ def _workload(args, rank, dev):
     """(scene, chain, run(), host-buffer run maker, description) for the config."""
     from sentinel_gpu_processor_b200 import synth
     from sentinel_gpu_processor_b200.chain import FrameChain, PairChain
-    if args.config == "frame":
+    if args.config in FRAME_CONFIGS:
         import torch
 
         from sentinel_gpu_processor_b200.chain import BatchedFrameChain
-        sc = synth.make_frame(seed=20261203 + 2000 + rank, device=dev)
+        small = args.config == "frame_small"
+        sc = synth.make_frame(seed=20261203 + 2000 + rank, device=dev,
+                              **(dict(n_swaths=1, n_bursts=3, scale=0.5) if small else {}))
         chain = BatchedFrameChain(sc.ref, sc.sec, sc.rsc, sc.rowlook, sc.collook, sc.alpha, device=dev,
                                   sample_format=args.samples, deramp_fused=args.deramp == "fused")
         if args.samples == "ci16":
@@ -272,12 +283,17 @@ def _workload(args, rank, dev):
             chain.load(sc.ref_slc, sc.sec_slc)
         torch.cuda.synchronize()
         sc.ref_slc = sc.sec_slc = None  # the frame's SLC buffer holds them now
-        chain.tuned = chain.autotune(sc.dem, reps=2)
+        chain.tuned = chain.tuning() if small else chain.autotune(sc.dem, reps=2)
         chain.capture(sc.dem)
-        desc = (f"full IW frame: {chain.n_pairs} burst pairs (3 subswaths x 9) of uneven size, lines 1480-1530, "
-                f"samples 20000-25500, 100-line overlap; batched: one launch per stage over the descriptor table "
-                f"of all {2 * chain.n_pairs} bursts, one CUDA graph per step, tile shapes from the autotuner; "
-                + ("SLC samples complex int16 (the measurement TIFF's type, widened on the GPU in the deramp)"
+        if small:
+            head = (f"small frame: {chain.n_pairs} burst pairs (1 subswath x 3) of half-size bursts, default "
+                    f"tile shapes")
+        else:
+            head = (f"full IW frame: {chain.n_pairs} burst pairs (3 subswaths x 9) of uneven size, lines 1480-1530, "
+                    f"samples 20000-25500, 100-line overlap; tile shapes from the autotuner")
+        desc = (head + f"; batched: one launch per stage over the descriptor table of all {2 * chain.n_pairs} "
+                f"bursts, one CUDA graph per step; "
+                + ("SLC samples complex int16 (the measurement TIFF's type, widened on the GPU)"
                    if args.samples == "ci16" else "SLC samples complex64 (as the reference's geo2rdr pipe)"))
         return sc, chain, chain.replay, desc
     if args.config == "frame_pairs":
@@ -312,7 +328,7 @@ def _e2e(chain, sc, args, world):
     import torch
     if args.config == "c1":
         return _e2e_radar(chain, sc, args, world)
-    if args.config == "frame":
+    if args.config in FRAME_CONFIGS:
         return _e2e_frame(chain, sc, args, world)
     frame = args.config == "frame_pairs"
     refs = sc.ref_slc if frame else sc.ref_slc[:1]
@@ -481,7 +497,7 @@ def _kernel_table(chain, sc, args, times, peak):
         box_px = chain.box[2] * chain.box[3]
         bytes_per = {"geo2rdr_offsets": 32 * px, "resample": 24 * px, "crossmul_looks": 16 * box_px + 20 * ml,
                      "box_coherence": 20 * px, "goldstein": 16 * ml}
-    elif args.config == "frame":
+    elif args.config in FRAME_CONFIGS:
         # one launch per stage covers every burst / pair of the frame
         pls = chain.plans
         burst = sum(p.lines * p.samples for p in pls)
@@ -537,7 +553,7 @@ def run_s1b(args):
     for _ in range(warm):
         res = run()
     torch.cuda.synchronize()
-    if args.config == "frame":
+    if args.config in FRAME_CONFIGS:
         res = chain.results()
     if res is None or (isinstance(res, list) and any(r is None for r in res)):
         raise SystemExit("empty interferogram for the synthetic input")
@@ -568,7 +584,7 @@ def run_s1b(args):
     else:
         chain.last = res
     peak, peak_kind = peaks()
-    if args.config == "frame":
+    if args.config in FRAME_CONFIGS:
         times = {}
         for _ in range(max(2, min(args.steps, 10))):
             for name, ms in chain.profile(sc.dem).items():
@@ -578,7 +594,7 @@ def run_s1b(args):
                               max(2, min(args.steps, 10)))
     table = _kernel_table(chain, sc, args, times, peak)
     top = max(table, key=lambda n: table[n]["total_ms"])
-    if args.config == "frame":
+    if args.config in FRAME_CONFIGS:
         extra = {"burst_pairs": chain.n_pairs, "burst_px_per_step": chain.burst_pixels,
                  "geo_px_total": sum(chain.geo_pixels()),
                  "ifg_ml_shapes_first3": [list(r.ifg.shape) for r in res[:3]],
@@ -601,9 +617,8 @@ def run_s1b(args):
         launches = chain.launches_per_step()
     traffic = None
     if top == "geo2rdr":
-        if args.config == "frame":  # one launch geocodes every burst
-            # ncu traffic per geo pixel was measured on the unfused kernel
-            traffic = (None if chain.deramp_fused
+        if args.config in FRAME_CONFIGS:  # one launch geocodes every burst
+            traffic = (GEO_FUSED_TRAFFIC_RATIO * table["geo2rdr"]["bytes_per_launch"] if chain.deramp_fused
                        else GEO_DRAM_BYTES_PER_GEO_PX * sum(p.nrow * p.ncol for p in chain.plans))
         else:
             pls = [p for pl in chain.pairs for p in pl] if args.config == "frame_pairs" else chain.plans
@@ -625,7 +640,7 @@ def run_s1b(args):
         "roofline": {"bound": "hbm", "kernel": top, "achieved": t["achieved_gbs"], "peak": peak, "unit": "GB/s",
                      "frac": t["frac"], "traffic": traffic, "peak_kind": peak_kind,
                      "bytes_per_launch": t["bytes_per_launch"], "launch_ms": t["avg_ms"],
-                     "timed": ("CUDA events between the stages of profiled frame runs" if args.config == "frame"
+                     "timed": ("CUDA events between the stages of profiled frame runs" if args.config in FRAME_CONFIGS
                                else "CUDA events around every launch of the entry point over instrumented eager steps"),
                      "note": ("FP64-compute bound (zero-Doppler Newton): low HBM fraction by design"
                               if top in ("geo2rdr", "geo2rdr_offsets") else "HBM-bound")},
@@ -661,10 +676,11 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "reference executables not built in oracle/_ref "
                                                               "(python oracle/build_ref.py)"}))
         return
-    if args.config in ("frame", "frame_pairs"):
+    if args.config in ("frame", "frame_small", "frame_pairs"):
         # a bounded sample of the frame: its first burst pair (the reference
         # runs geo2rdr once per burst for uneven burst sizes)
-        frame = synth.make_frame(seed=20261203 + 2000, device="cuda")
+        frame = synth.make_frame(seed=20261203 + 2000, device="cuda",
+                                 **(dict(n_swaths=1, n_bursts=3, scale=0.5) if args.config == "frame_small" else {}))
         base_sc = synth.frame_pair(frame, 0)
         del frame
         base_sc.dem = base_sc.dem.cpu()
