@@ -44,10 +44,10 @@ GEO_BYTES_PER_GEO_PX = 2 + 8
 GEO_BYTES_PER_BURST_PX = 8
 # Measured DRAM traffic (ncu dram__bytes_read.sum + dram__bytes_write.sum of
 # one launch on the 1500 x 21000 burst pair, divided by the units it
-# processed): geocoding per geo pixel (16.06 M geo px: 274.0 + 92.2 MB) and
+# processed): geocoding per geo pixel (16.06 M geo px: 285.6 + 93.9 MB) and
 # the TMA resampler per output pixel (31.5 M px: 550.9 + 228.7 MB).  Both
 # kernels stream their inputs once, so traffic scales with the unit count.
-GEO_DRAM_BYTES_PER_GEO_PX = 22.81
+GEO_DRAM_BYTES_PER_GEO_PX = 23.63
 # fused frame geocoding (deramp in the gathers): ncu DRAM traffic over algorithmic
 # bytes on the small frame (487.1 MB / 496.2 MB, profiles/geo2rdr_frame_fused.md);
 # both terms (raw samples read, geocoded pixels written) scale with the frame
