@@ -33,6 +33,16 @@ constexpr double kRe2D = 0.00669437999015;
 // (short2: re, im), widened exactly to float in registers.
 constexpr int DERAMP_ROWS = 16;
 
+// int16 -> float without the conversion unit: 1.5 * 2^23 has a unit ulp, so
+// adding a small integer to its bit pattern adds it to the value (exact for
+// |x| < 2^22) and subtracting 1.5 * 2^23 leaves x exactly.  The same value as
+// (float)x, from an integer add and an FP32 add.
+__device__ __forceinline__ float i16_to_f32(int x) { return __int_as_float(0x4B400000 + x) - 12582912.0f; }
+// The same for int -> double with 1.5 * 2^52 (exact for |x| < 2^51).
+__device__ __forceinline__ double i32_to_f64(int x) {
+  return __longlong_as_double(0x4338000000000000LL + (long long)x) - 6755399441055744.0;
+}
+
 // Two adjacent samples from an address aligned to their size (16 bytes for
 // complex64, 8 for complex int16), streamed.
 __device__ __forceinline__ void load_pair(const float2 *p, float2 &a0, float2 &a1) {
@@ -42,13 +52,13 @@ __device__ __forceinline__ void load_pair(const float2 *p, float2 &a0, float2 &a
 }
 __device__ __forceinline__ void load_pair(const short2 *p, float2 &a0, float2 &a1) {
   const short4 v = __ldcs(reinterpret_cast<const short4 *>(p));
-  a0 = make_float2((float)v.x, (float)v.y);
-  a1 = make_float2((float)v.z, (float)v.w);
+  a0 = make_float2(i16_to_f32(v.x), i16_to_f32(v.y));
+  a1 = make_float2(i16_to_f32(v.z), i16_to_f32(v.w));
 }
 __device__ __forceinline__ float2 load_one(const float2 *p) { return __ldcs(p); }
 __device__ __forceinline__ float2 load_one(const short2 *p) {
   const short2 v = __ldcs(p);
-  return make_float2((float)v.x, (float)v.y);
+  return make_float2(i16_to_f32(v.x), i16_to_f32(v.y));
 }
 
 // TOPS deramp coefficients of burst column c (geo2rdr.cu:533-541): -pi kt
@@ -65,13 +75,21 @@ __device__ __forceinline__ void tops_column(const s1b_burst_plan_t &P, int c, do
   etaref = -fnc / ka - P.etac0;
 }
 
-// Deramped sample of line r: a * exp(i mkt (eta_r - etaref)^2), eta_r =
-// -L ati / 2 + r ati (geo2rdr.cu:530-531, 151-152).
-__device__ __forceinline__ float2 deramp_sample(const s1b_burst_plan_t &P, float2 a, int r, double mkt,
-                                                double etaref) {
-  const double eta = -P.lines * P.ati / 2. + r * P.ati;
+// Azimuth time of line r relative to the burst centre: eta_r = -L ati / 2 +
+// r ati (geo2rdr.cu:530-531).
+__device__ __forceinline__ double deramp_eta(const s1b_burst_plan_t &P, int r) {
+  return -P.lines * P.ati / 2. + i32_to_f64(r) * P.ati;
+}
+
+// Deramped sample: a * exp(i mkt (eta - etaref)^2) (geo2rdr.cu:151-152).
+__device__ __forceinline__ float2 deramp_at(float2 a, double eta, double mkt, double etaref) {
   const double d = eta - etaref;
   return cmul(a, phasor(mkt * d * d));
+}
+
+__device__ __forceinline__ float2 deramp_sample(const s1b_burst_plan_t &P, float2 a, int r, double mkt,
+                                                double etaref) {
+  return deramp_at(a, deramp_eta(P, r), mkt, etaref);
 }
 
 template <bool kVec, int ROWS, typename TIn>
@@ -189,7 +207,7 @@ __global__ void rows_init_kernel(int32_t *rows, int nrow) {
 __device__ __forceinline__ float2 load_ro(const float2 *p) { return __ldg(p); }
 __device__ __forceinline__ float2 load_ro(const short2 *p) {
   const short2 v = __ldg(p);
-  return make_float2((float)v.x, (float)v.y);
+  return make_float2(i16_to_f32(v.x), i16_to_f32(v.y));
 }
 
 // Geocoding of one tile.  Unfused (kFused false): `burst` is the deramped
@@ -302,7 +320,7 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
     const double sinlat = __shfl_sync(0xffffffffu, r_sin, r & 31);
     const double coslat = __shfl_sync(0xffffffffu, r_cos, r & 31);
     const double re = __shfl_sync(0xffffffffu, r_re, r & 31);
-    const double hgt = (double)hn;
+    const double hgt = i32_to_f64(hn);
     if (colok && r + 1 < rmax) hn = __ldg(dem + (int64_t)(row + 1) * pitch + col);
     float2 res = make_float2(0.f, 0.f);
     if (colok) {
@@ -353,10 +371,11 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
         float2 b1, b2, b3, b4;
         if constexpr (kFused) {
           const double2 t0 = __ldg(tops + intr), t1 = __ldg(tops + intr + 1);
-          b1 = deramp_sample(P, load_ro(burst + i1), inta, t0.x, t0.y);
-          b2 = deramp_sample(P, load_ro(burst + i1 + 1), inta, t1.x, t1.y);
-          b3 = deramp_sample(P, load_ro(burst + i1 + P.samples), inta + 1, t0.x, t0.y);
-          b4 = deramp_sample(P, load_ro(burst + i1 + P.samples + 1), inta + 1, t1.x, t1.y);
+          const double ea = deramp_eta(P, inta), eb = deramp_eta(P, inta + 1);  // once per gathered line
+          b1 = deramp_at(load_ro(burst + i1), ea, t0.x, t0.y);
+          b2 = deramp_at(load_ro(burst + i1 + 1), ea, t1.x, t1.y);
+          b3 = deramp_at(load_ro(burst + i1 + P.samples), eb, t0.x, t0.y);
+          b4 = deramp_at(load_ro(burst + i1 + P.samples + 1), eb, t1.x, t1.y);
         } else {
           b1 = __ldg(burst + i1);
           b2 = __ldg(burst + i1 + 1);
