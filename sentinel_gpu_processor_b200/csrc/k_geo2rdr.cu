@@ -554,15 +554,18 @@ __global__ __launch_bounds__(TX) void frame_geo2rdr_kernel(const FrameDev d, con
 }
 
 // One CTA per tile: blockIdx.z is the burst, (x, y) the tile in its DEM
-// window; the plan is read through the table (uniform, L1-resident loads)
-// instead of a shared-memory copy, which keeps the single-burst register
-// budget.  The grid spans the largest window; CTAs past a smaller one return.
+// window.  The CTA copies its burst's plan (12.5 KB) to shared memory first:
+// the pixel loop's plan scalars then come from shared memory rather than
+// uniform global loads (measured 13.67 -> 13.28 ms per 27-pair frame).  The
+// grid spans the largest window; CTAs past a smaller one return before the
+// copy's barriers (a uniform test of the block index).
 template <int TX, typename TSrc, bool kFused>
 __global__ __launch_bounds__(TX) void frame_geo2rdr_grid_kernel(const FrameDev d, const FrameIO io) {
+  __shared__ __align__(16) s1b_burst_plan_t sp;
   const int b = blockIdx.z;
-  const s1b_burst_plan_t &sp = d.plans[b];
   const FrameBurst &fb = d.bursts[b];
   if ((int)blockIdx.x * TX >= fb.ncol || (int)blockIdx.y * kFrameGeoRows >= fb.nrow) return;
+  frame_load_plan(sp, d.plans + b);
   frame_geo_tile<TX, TSrc, kFused>(sp, fb, io, d.rows + 2 * b, blockIdx.x, blockIdx.y);
 }
 
