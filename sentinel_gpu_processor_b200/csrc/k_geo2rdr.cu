@@ -194,7 +194,8 @@ __global__ __launch_bounds__(256) void deramp_kernel(const __grid_constant__ s1b
 // Rows per tile (a multiple of 32): the per-warp set-up (the centre pixel's
 // exact Newton on the orbit polynomial, FP64 row trigonometry) is amortised
 // over the tile's rows.  Measured per 27-pair frame: 16 rows 11.15 ms, 32
-// rows 9.88 ms, 64 rows 9.41 ms (kFrameGeoRows); a single burst's grid is
+// rows 9.88 ms, 64 rows 9.41 ms (unfused), and for the fused frame kernel 64
+// rows 13.30 ms, 128 rows 13.08 ms (kFrameGeoRows); a single burst's grid is
 // too small for 64-row tiles (0.195 ms at 32 rows, 0.221 ms at 64).
 constexpr int G_TX = 128, G_RY = 32;  // single-burst launch; the frame launch tunes the width
 

@@ -75,7 +75,7 @@ struct FrameBurstList {
 
 // Tile-space helpers shared by host and device.
 constexpr int kFrameDerampCols = 512;  // columns of a deramp tile (256 threads x 2)
-constexpr int kFrameGeoRows = 64;      // rows of a geocoding tile (column walk length)
+constexpr int kFrameGeoRows = 128;     // rows of a geocoding tile (column walk length)
 
 // Launchers (k_geo2rdr.cu, k_crossmul.cu, k_goldstein.cu).  `ctas` is the
 // persistent grid; 0 launches one CTA per tile over (tile x, tile y, burst).
