@@ -200,6 +200,15 @@ int s1b_deramp_ci16(const s1b_burst_plan_t *plan, const void *in, void *out, voi
 int s1b_geo2rdr(const s1b_burst_plan_t *plan, const int16_t *dem, int64_t dem_pitch,
                 const void *deramped, void *out, int32_t *rows, void *stream);
 
+/* Culling of geocoding work outside the burst's valid lines, on by default,
+ * for every later s1b_geo2rdr and frame launch in the process (a frame's
+ * captured graph keeps the setting it was captured with).  Blocks of 32
+ * window rows whose azimuth lines lie outside [first_valid_line + 5,
+ * last_valid_line - 5) at every int16 height are written as zeros without
+ * their zero-Doppler solves; the products are identical either way.  No
+ * reference counterpart (an execution choice).  Returns the previous setting. */
+int s1b_set_geocode_culling(int32_t on);
+
 /* Zero-Doppler solve for arbitrary ECEF points (device arrays, n points):
  * replaces orbitrangetime / orbitrangetime_vec (csrc/src/orbit.cu:247-280,
  * s1proc/orbit.py:118-188).  Seeds every point with (tline0, orbit(tline0)).

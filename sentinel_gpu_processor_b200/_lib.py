@@ -129,6 +129,7 @@ _SIGNATURES = {
     "s1b_deramp": (c_int, [POINTER(BurstPlan), c_void_p, c_void_p, c_void_p]),
     "s1b_deramp_ci16": (c_int, [POINTER(BurstPlan), c_void_p, c_void_p, c_void_p]),
     "s1b_geo2rdr": (c_int, [POINTER(BurstPlan), c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "s1b_set_geocode_culling": (c_int, [c_int32]),
     "s1b_zero_doppler": (c_int, [POINTER(OrbitPoly), c_void_p, c_int64, c_double, c_void_p, c_void_p, c_void_p]),
     "s1b_llh2xyz": (c_int, [c_void_p, c_void_p, c_int64, c_void_p]),
     "s1b_crossmul_looks": (c_int, [c_void_p, c_int32, c_int32, c_int32, c_int32, c_void_p, c_int32, c_int32,

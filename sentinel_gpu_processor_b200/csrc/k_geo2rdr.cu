@@ -204,6 +204,10 @@ __global__ void rows_init_kernel(int32_t *rows, int nrow) {
   rows[1] = -1;
 }
 
+// Culling of the geocoding blocks outside the burst's valid lines (on by
+// default; off only to compare the two, which give identical products).
+static int g_cull_geo = 1;
+
 // Read-only (L1-cached) sample loads for the bilinear gathers.
 __device__ __forceinline__ float2 load_ro(const float2 *p) { return __ldg(p); }
 __device__ __forceinline__ float2 load_ro(const short2 *p) {
@@ -218,11 +222,21 @@ __device__ __forceinline__ float2 load_ro(const short2 *p) {
 // gathered, with the deramp kernel's own expressions (deramp_sample), so the
 // result equals the unfused path's bit for bit and the deramped copy of the
 // burst is never written.
+//
+// Culling (cull true): a DEM window is the bounding box of a burst footprint
+// turned by the orbit heading, and about 40% of an IW burst's window lies
+// before its first valid line or after its last.  Each warp fits a
+// zero-height line model, affine in (row, column), to its corner solutions,
+// with the line shift per metre of height; a block of 32 rows whose lines
+// stay outside [first_valid_line + 5, last_valid_line - 5) at every int16
+// height is written as zeros without solving its pixels.  Every block seeds
+// its Newton iteration from the line model, so a pixel's result does not
+// depend on whether the blocks before it were culled.
 template <int TX, int RY, typename TSrc = float2, bool kFused = false>
 __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const int16_t *__restrict__ dem,
                                              int64_t pitch, const TSrc *__restrict__ burst,
                                              float2 *__restrict__ out, int32_t *__restrict__ rows, int nrow,
-                                             int ncol, int tile_x, int tile_y,
+                                             int ncol, int tile_x, int tile_y, bool cull,
                                              const double2 *__restrict__ tops = nullptr) {
   const int tx = threadIdx.x, lane = tx & 31;
   const int col = tile_x * TX + tx;
@@ -243,18 +257,24 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
   const double inv_dmrg = 1.0 / P.dmrg, prf = 1.0 / P.dtaz, two_over_c = 2.0 / kSolD;
   // One cubic orbit expansion per warp, at the zero-Doppler time of the
   // warp's centre pixel, solved on the window polynomial from the burst
-  // centre (geo2rdr.cu:588-600).  The warp's 32 x 32 pixels lie within
+  // centre (geo2rdr.cu:588-600).  The warp's 32 x RY pixels lie within
   // ~0.2 s of it, where the dropped fourth-order term is < 1e-9 m.  Lanes 1
-  // and 2 solve two opposite corners at the same time; the three solutions
-  // bound the warp's footprint in the burst, whose lines are prefetched into
-  // L2 before the per-pixel solves, so the bilinear gathers hit L2.
+  // to 3 solve three corners at the same time; the four solutions bound the
+  // warp's footprint in the burst, whose lines are prefetched into L2 before
+  // the per-pixel solves, so the bilinear gathers hit L2, and give the line
+  // model that seeds and culls the pixel solves.
   __shared__ ZeroDopplerPatch s_zd[TX / 32];
   const int wid = tx >> 5;
-  double faz = 0.0, frg = 0.0;
-  if (lane < 3) {
-    const int c0 = tile_x * TX + wid * 32;
-    const int cr = lane == 0 ? min(row0 + RY / 2, nrow - 1) : (lane == 1 ? row0 : min(row0 + RY - 1, nrow - 1));
-    const int cc = lane == 0 ? min(c0 + 16, ncol - 1) : (lane == 1 ? min(c0, ncol - 1) : min(c0 + 31, ncol - 1));
+  // the warp's pixels span rows rT .. rB and columns cL .. cR of the window
+  const int c0 = tile_x * TX + wid * 32;
+  const int rT = row0, rB = min(row0 + RY - 1, nrow - 1), cL = min(c0, ncol - 1), cR = min(c0 + 31, ncol - 1);
+  const int rC = min(row0 + RY / 2, nrow - 1), cC = min(c0 + 16, ncol - 1);
+  double faz = 0.0, frg = 0.0, zl = 0.0, kl = 0.0;
+  bool conv = true;
+  if (lane < 4) {
+    // lane 0: centre; 1: top left; 2: bottom right; 3: top right
+    const int cr = lane == 0 ? rC : (lane == 2 ? rB : rT);
+    const int cc = lane == 0 ? cC : (lane == 1 ? cL : cR);
     double sla, cla, slo, clo;
     sincos((P.lat0 + cr * P.dlat) * kPiD / 180, &sla, &cla);
     sincos((P.lon0 + cc * P.dlon) * kPiD / 180, &slo, &clo);
@@ -269,19 +289,32 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
       st.a[i] = P.amid[i];
     }
     double tc = P.tmid, drc[3];
-    zero_doppler(P.orbit, pc, tc, st, drc);
+    conv = zero_doppler(P.orbit, pc, tc, st, drc) < 51;
+    faz = (tc - P.tstart) * prf;
+    frg = (sqrt(drc[0] * drc[0] + drc[1] * drc[1] + drc[2] * drc[2]) - P.rngstart) * inv_dmrg;
+    // lines per metre of height: the zero-Doppler condition (p - X).V = 0
+    // moved along the ellipsoid normal n = dp/dh gives
+    // dt/dh = -(V.n) / ((p - X).A - V.V)
+    const double nrm[3] = {cla * clo, cla * slo, sla};
+    double vn = 0.0, fp = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      vn = fma(st.v[i], nrm[i], vn);
+      fp = fma(drc[i], st.a[i], fp);
+      fp = fma(-st.v[i], st.v[i], fp);
+    }
+    kl = -vn * rcp_newton(fp) * prf;
+    zl = faz - kl * hc;  // the point's line at zero height
     if (lane == 0) {
       OrbitCubic oc;
       orbit_cubic(P.orbit, tc, oc);
       zero_doppler_patch(oc, s_zd[wid]);
     }
-    faz = (tc - P.tstart) * prf;
-    frg = (sqrt(drc[0] * drc[0] + drc[1] * drc[1] + drc[2] * drc[2]) - P.rngstart) * inv_dmrg;
   }
   {
     double a0 = faz, a1 = faz, g0 = frg, g1 = frg;
 #pragma unroll
-    for (int k = 1; k < 3; ++k) {
+    for (int k = 1; k < 4; ++k) {
       const double a = __shfl_sync(0xffffffffu, faz, k), g = __shfl_sync(0xffffffffu, frg, k);
       a0 = fmin(a0, a);
       a1 = fmax(a1, a);
@@ -308,93 +341,141 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
       }
     }
   }
-  __syncwarp();  // lane 0's patch model is visible to the warp
+  // Line model of the warp (identical in every lane): zero-height line
+  // zTL + zr (row - rT) + zc (col - cL) from the top corners and the bottom
+  // right one, plus kC lines per metre of height.  The centre's distance
+  // from the model measures its curvature; the cull margin covers four times
+  // that, the heights (-32768 .. 32767 m, the slope with a quarter to spare
+  // for its change over the warp and with height) and 2 lines.
+  // The seed model goes to shared memory as times from the centre's:
+  // h = s.x + s.y col + s.z r + s.w hgt; bit j of cullmask marks block j culled.
+  __shared__ double4 s_seed[TX / 32];
+  const int rmax = min(RY, nrow - row0);
+  unsigned cullmask = 0;
+  {
+    const double zTL = __shfl_sync(0xffffffffu, zl, 1), zBR = __shfl_sync(0xffffffffu, zl, 2);
+    const double zTR = __shfl_sync(0xffffffffu, zl, 3), zC = __shfl_sync(0xffffffffu, zl, 0);
+    const double kC = __shfl_sync(0xffffffffu, kl, 0), fazC = __shfl_sync(0xffffffffu, faz, 0);
+    const double zr = rB > rT ? (zBR - zTR) * rcp_newton(rB - rT) : 0.0;
+    const double zc = cR > cL ? (zTR - zTL) * rcp_newton(cR - cL) : 0.0;
+    const double kmax = fmax(fmax(fabs(kC), fabs(__shfl_sync(0xffffffffu, kl, 1))),
+                             fmax(fabs(__shfl_sync(0xffffffffu, kl, 2)), fabs(__shfl_sync(0xffffffffu, kl, 3))));
+    const double resid = fabs(zC - (zTL + zr * (rC - rT) + zc * (cC - cL)));
+    const double slack = 2.0 + 4.0 * resid + 1.25 * 32768.0 * kmax;
+    // every corner converged and the model is sound (NaN fails each test)
+    if (__all_sync(0xffffffffu, conv) && cull && resid < 1.0 && slack < 1.0e4) {
+      const double zcs = zc * (cR - cL);  // the model's change across the warp's columns
+#pragma unroll
+      for (int j = 0; j < RY / 32; ++j) {
+        const int rb = 32 * j, rend = min(rb + 32, rmax);
+        const double za = zTL + zr * rb, zb = zTL + zr * (rend - 1);
+        const double lo = fmin(za, zb) + fmin(zcs, 0.0) - slack, hi = fmax(za, zb) + fmax(zcs, 0.0) + slack;
+        if (rb < rmax && (hi < P.first_valid_line + 5 || lo >= P.last_valid_line - 5)) cullmask |= 1u << j;
+      }
+    }
+    if (lane == 0)
+      s_seed[wid] = make_double4((zTL - zc * cL - fazC) * P.dtaz, zc * P.dtaz, zr * P.dtaz, kC * P.dtaz);
+  }
+  __syncwarp();  // lane 0's patch and seed models are visible to the warp
   const ZeroDopplerPatch &zd = s_zd[wid];
   const double k4_wvl = 4.0 / P.wvl;  // two-way range phase, half-cycles per metre
   double h = 0.0, hprev = 0.0, inv_c1 = 0.0;
-  const int rmax = min(RY, nrow - row0);
-  int16_t hn = colok && rmax > 0 ? __ldg(dem + (int64_t)row0 * pitch + col) : 0;
+  int16_t hn = colok && rmax > 0 && !(cullmask & 1u) ? __ldg(dem + (int64_t)row0 * pitch + col) : 0;
   int rlo = INT_MAX, rhi = -1;
   for (int r = 0; r < rmax; ++r) {
-    const int row = row0 + r;
-    if (r > 0 && (r & 31) == 0) row_terms(r);  // the next 32 rows (warp-uniform)
-    const double sinlat = __shfl_sync(0xffffffffu, r_sin, r & 31);
-    const double coslat = __shfl_sync(0xffffffffu, r_cos, r & 31);
-    const double re = __shfl_sync(0xffffffffu, r_re, r & 31);
-    const double hgt = i32_to_f64(hn);
-    if (colok && r + 1 < rmax) hn = __ldg(dem + (int64_t)(row + 1) * pitch + col);
-    float2 res = make_float2(0.f, 0.f);
-    if (colok) {
-      double p[3];
-      p[0] = (re + hgt) * coslat * coslon;
-      p[1] = (re + hgt) * coslat * sinlon;
-      p[2] = (re * (1 - kRe2D) + hgt) * sinlat;
-      const ZeroDopplerPoint q = zero_doppler_point(zd, p);
-      if (r == 0) {
-        // the column's first point starts at the warp centre; its slope
-        // serves the whole column (f' changes by < 1e-3 over 32 rows)
-        inv_c1 = rcp_newton(q.c1);
-        hprev = -P.dtaz;
-      } else {
-        const double hn2 = 2.0 * h - hprev;  // linear extrapolation from the two rows above
-        hprev = h;
-        h = hn2;
+    if ((r & 31) == 0) {  // a new block of 32 rows (warp-uniform)
+      if ((cullmask >> (r >> 5)) & 1u) {
+        const int rend = min(r + 32, rmax);
+        if (colok)
+          for (; r < rend; ++r) __stcs(out + (size_t)(row0 + r) * ncol + col, make_float2(0.f, 0.f));
+        // the next block's first height (none was loaded ahead)
+        if (colok && r < rmax) hn = __ldg(dem + (int64_t)(row0 + r) * pitch + col);
+        r = rend - 1;
+        continue;
       }
-      const double rng = sqrt_heron(zero_doppler_solve(q, zd.c3, inv_c1, h));
-      if (r == 0) hprev = h - P.dtaz;
-      const double t = zd.t0 + h;
-      const double rgoff = (rng - P.rngstart) * inv_dmrg;
-      const double azoff = (t - P.tstart) * prf;
-      // validity window, geo2rdr.cu:208-209
-      bool valid = rgoff > P.first_valid_sample && rgoff < P.last_valid_sample - 1 &&
-                   azoff >= P.first_valid_line + 5 && azoff < P.last_valid_line - 5;
-      const int intr = (int)rgoff, inta = (int)azoff;
-      // the 2x2 neighbourhood must lie inside the burst even if the validity
-      // limits passed in exceed the raster
-      valid = valid && intr >= 0 && intr + 1 < P.samples && inta >= 0 && inta + 1 < P.lines;
-      if (valid) {
-        // per-pixel TOPS reramp (geo2rdr.cu:210-219); kt = ka ks / (ka - ks)
-        // and etac = -fnc / ka share one reciprocal of ka (ka - ks)
-        const double tr = rng * two_over_c;
-        double dt = tr - P.fm[0];
-        const double ka = P.fm[1] + dt * (P.fm[2] + P.fm[3] * dt);
-        dt = tr - P.dc[0];
-        const double fnc = P.dc[1] + dt * (P.dc[2] + P.dc[3] * dt);
-        const double kmk = ka - P.ks;
-        const double inv = rcp_newton(ka * kmk);
-        const double kt = ka * P.ks * (ka * inv);
-        const double etaref = -fnc * (kmk * inv) - P.etac0;
-        const double eta = -P.lines * P.dtaz / 2. + t - P.tstart;
-        const double ed = eta - etaref;
-        // bilinear interpolation of the deramped burst (geo2rdr.cu:220-237)
-        const float fr = (float)(rgoff - intr), fa = (float)(azoff - inta);
-        const size_t i1 = (size_t)inta * P.samples + intr;
-        float2 b1, b2, b3, b4;
-        if constexpr (kFused) {
-          const double2 t0 = __ldg(tops + intr), t1 = __ldg(tops + intr + 1);
-          const double ea = deramp_eta(P, inta), eb = deramp_eta(P, inta + 1);  // once per gathered line
-          b1 = deramp_at(load_ro(burst + i1), ea, t0.x, t0.y);
-          b2 = deramp_at(load_ro(burst + i1 + 1), ea, t1.x, t1.y);
-          b3 = deramp_at(load_ro(burst + i1 + P.samples), eb, t0.x, t0.y);
-          b4 = deramp_at(load_ro(burst + i1 + P.samples + 1), eb, t1.x, t1.y);
-        } else {
-          b1 = __ldg(burst + i1);
-          b2 = __ldg(burst + i1 + 1);
-          b3 = __ldg(burst + i1 + P.samples);
-          b4 = __ldg(burst + i1 + P.samples + 1);
-        }
-        const float2 c1 = make_float2(fmaf(fr, b2.x - b1.x, b1.x), fmaf(fr, b2.y - b1.y, b1.y));
-        const float2 c2 = make_float2(fmaf(fr, b4.x - b3.x, b3.x), fmaf(fr, b4.y - b3.y, b3.y));
-        const float2 v = make_float2(fmaf(fa, c2.x - c1.x, c1.x), fmaf(fa, c2.y - c1.y, c1.y));
-        // range phase and reramp (geo2rdr.cu:238-243): 4 pi rng / wvl + pi kt ed^2
-        // rad, formed in half-cycles
-        res = cmul(v, phasor_pi(fma(kt, ed * ed, k4_wvl * rng)));
-      }
-      __stcs(out + (size_t)row * ncol + col, res);
+      if (r > 0) row_terms(r);
     }
-    if (res.x != 0.f || res.y != 0.f) {
-      rlo = min(rlo, row);
-      rhi = row + 1;
+    {
+      const int row = row0 + r;
+      const double sinlat = __shfl_sync(0xffffffffu, r_sin, r & 31);
+      const double coslat = __shfl_sync(0xffffffffu, r_cos, r & 31);
+      const double re = __shfl_sync(0xffffffffu, r_re, r & 31);
+      const double hgt = i32_to_f64(hn);
+      if (colok && r + 1 < rmax) hn = __ldg(dem + (int64_t)(row + 1) * pitch + col);
+      float2 res = make_float2(0.f, 0.f);
+      if (colok) {
+        double p[3];
+        p[0] = (re + hgt) * coslat * coslon;
+        p[1] = (re + hgt) * coslat * sinlon;
+        p[2] = (re * (1 - kRe2D) + hgt) * sinlat;
+        const ZeroDopplerPoint q = zero_doppler_point(zd, p);
+        if ((r & 31) == 0) {
+          // the block's first point starts from the line model; its slope
+          // serves the block (f' changes by < 1e-3 over 32 rows)
+          inv_c1 = rcp_newton(q.c1);
+          const double4 m = s_seed[wid];
+          h = fma(m.w, hgt, fma(m.z, (double)r, fma(m.y, (double)col, m.x)));
+        } else {
+          const double hn2 = 2.0 * h - hprev;  // linear extrapolation from the two rows above
+          hprev = h;
+          h = hn2;
+        }
+        const double rng = sqrt_heron(zero_doppler_solve(q, zd.c3, inv_c1, h));
+        if ((r & 31) == 0) hprev = h - s_seed[wid].z;
+        const double t = zd.t0 + h;
+        const double rgoff = (rng - P.rngstart) * inv_dmrg;
+        const double azoff = (t - P.tstart) * prf;
+        // validity window, geo2rdr.cu:208-209
+        bool valid = rgoff > P.first_valid_sample && rgoff < P.last_valid_sample - 1 &&
+                     azoff >= P.first_valid_line + 5 && azoff < P.last_valid_line - 5;
+        const int intr = (int)rgoff, inta = (int)azoff;
+        // the 2x2 neighbourhood must lie inside the burst even if the validity
+        // limits passed in exceed the raster
+        valid = valid && intr >= 0 && intr + 1 < P.samples && inta >= 0 && inta + 1 < P.lines;
+        if (valid) {
+          // per-pixel TOPS reramp (geo2rdr.cu:210-219); kt = ka ks / (ka - ks)
+          // and etac = -fnc / ka share one reciprocal of ka (ka - ks)
+          const double tr = rng * two_over_c;
+          double dt = tr - P.fm[0];
+          const double ka = P.fm[1] + dt * (P.fm[2] + P.fm[3] * dt);
+          dt = tr - P.dc[0];
+          const double fnc = P.dc[1] + dt * (P.dc[2] + P.dc[3] * dt);
+          const double kmk = ka - P.ks;
+          const double inv = rcp_newton(ka * kmk);
+          const double kt = ka * P.ks * (ka * inv);
+          const double etaref = -fnc * (kmk * inv) - P.etac0;
+          const double eta = -P.lines * P.dtaz / 2. + t - P.tstart;
+          const double ed = eta - etaref;
+          // bilinear interpolation of the deramped burst (geo2rdr.cu:220-237)
+          const float fr = (float)(rgoff - intr), fa = (float)(azoff - inta);
+          const size_t i1 = (size_t)inta * P.samples + intr;
+          float2 b1, b2, b3, b4;
+          if constexpr (kFused) {
+            const double2 t0 = __ldg(tops + intr), t1 = __ldg(tops + intr + 1);
+            const double ea = deramp_eta(P, inta), eb = deramp_eta(P, inta + 1);  // once per gathered line
+            b1 = deramp_at(load_ro(burst + i1), ea, t0.x, t0.y);
+            b2 = deramp_at(load_ro(burst + i1 + 1), ea, t1.x, t1.y);
+            b3 = deramp_at(load_ro(burst + i1 + P.samples), eb, t0.x, t0.y);
+            b4 = deramp_at(load_ro(burst + i1 + P.samples + 1), eb, t1.x, t1.y);
+          } else {
+            b1 = __ldg(burst + i1);
+            b2 = __ldg(burst + i1 + 1);
+            b3 = __ldg(burst + i1 + P.samples);
+            b4 = __ldg(burst + i1 + P.samples + 1);
+          }
+          const float2 c1 = make_float2(fmaf(fr, b2.x - b1.x, b1.x), fmaf(fr, b2.y - b1.y, b1.y));
+          const float2 c2 = make_float2(fmaf(fr, b4.x - b3.x, b3.x), fmaf(fr, b4.y - b3.y, b3.y));
+          const float2 v = make_float2(fmaf(fa, c2.x - c1.x, c1.x), fmaf(fa, c2.y - c1.y, c1.y));
+          // range phase and reramp (geo2rdr.cu:238-243): 4 pi rng / wvl + pi kt ed^2
+          // rad, formed in half-cycles
+          res = cmul(v, phasor_pi(fma(kt, ed * ed, k4_wvl * rng)));
+        }
+        __stcs(out + (size_t)row * ncol + col, res);
+      }
+      if (res.x != 0.f || res.y != 0.f) {
+        rlo = min(rlo, row);
+        rhi = row + 1;
+      }
     }
   }
   // first / last non-zero output row (geo2rdr.cu:86-128): the warp's extent
@@ -411,8 +492,8 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
 __global__ __launch_bounds__(G_TX) void geo2rdr_kernel(
     const __grid_constant__ s1b_burst_plan_t P, const int16_t *__restrict__ dem, int64_t pitch,
     const float2 *__restrict__ burst, float2 *__restrict__ out, int32_t *__restrict__ rows,
-    int nrow, int ncol) {
-  geo2rdr_tile<G_TX, G_RY>(P, dem, pitch, burst, out, rows, nrow, ncol, blockIdx.x, blockIdx.y);
+    int nrow, int ncol, bool cull) {
+  geo2rdr_tile<G_TX, G_RY>(P, dem, pitch, burst, out, rows, nrow, ncol, blockIdx.x, blockIdx.y, cull);
 }
 
 // ------------------------------------------------------------ frame stages
@@ -511,15 +592,15 @@ void launch_deramp_grid(const FrameDev &d, const FrameIO &io, int rows, const in
 // fused from its raw samples and its column table (both at der_off).
 template <int TX, typename TSrc, bool kFused>
 __device__ __forceinline__ void frame_geo_tile(const s1b_burst_plan_t &sp, const FrameBurst &fb, const FrameIO &io,
-                                               int32_t *rows, int tx, int ty) {
+                                               int32_t *rows, int tx, int ty, bool cull) {
   const int16_t *dem = io.dem + (int64_t)sp.win_top * io.dem_pitch + sp.win_left;
   if constexpr (kFused)
     geo2rdr_tile<TX, kFrameGeoRows, TSrc, true>(sp, dem, io.dem_pitch, static_cast<const TSrc *>(io.slc) + fb.slc_off,
-                                                io.work + fb.geo_off, rows, fb.nrow, fb.ncol, tx, ty,
+                                                io.work + fb.geo_off, rows, fb.nrow, fb.ncol, tx, ty, cull,
                                                 reinterpret_cast<const double2 *>(io.work + fb.der_off));
   else
     geo2rdr_tile<TX, kFrameGeoRows>(sp, dem, io.dem_pitch, io.work + fb.der_off, io.work + fb.geo_off, rows, fb.nrow,
-                                    fb.ncol, tx, ty);
+                                    fb.ncol, tx, ty, cull);
 }
 
 // Per-column deramp coefficients (-pi kt, etaref) of every burst for the
@@ -550,7 +631,7 @@ __global__ __launch_bounds__(TX) void frame_geo2rdr_kernel(const FrameDev d, con
     const int tiles_x = (fb.ncol + TX - 1) / TX;
     const int64_t local = idx - fb.geo_tile0;
     const int ty = (int)(local / tiles_x), tx = (int)(local - (int64_t)ty * tiles_x);
-    frame_geo_tile<TX, TSrc, kFused>(sp, fb, io, d.rows + 2 * b, tx, ty);
+    frame_geo_tile<TX, TSrc, kFused>(sp, fb, io, d.rows + 2 * b, tx, ty, d.cull_geo != 0);
   }
 }
 
@@ -559,15 +640,17 @@ __global__ __launch_bounds__(TX) void frame_geo2rdr_kernel(const FrameDev d, con
 // the pixel loop's plan scalars then come from shared memory rather than
 // uniform global loads (measured 13.67 -> 13.28 ms per 27-pair frame).  The
 // grid spans the largest window; CTAs past a smaller one return before the
-// copy's barriers (a uniform test of the block index).
+// copy's barriers (a uniform test of the block index).  Registers are held
+// to 80 (768 threads per SM): at TX 128 that beats the 96 the compiler picks
+// (11.85 -> 11.62 ms per frame).
 template <int TX, typename TSrc, bool kFused>
-__global__ __launch_bounds__(TX) void frame_geo2rdr_grid_kernel(const FrameDev d, const FrameIO io) {
+__global__ __launch_bounds__(TX, 768 / TX) void frame_geo2rdr_grid_kernel(const FrameDev d, const FrameIO io) {
   __shared__ __align__(16) s1b_burst_plan_t sp;
   const int b = blockIdx.z;
   const FrameBurst &fb = d.bursts[b];
   if ((int)blockIdx.x * TX >= fb.ncol || (int)blockIdx.y * kFrameGeoRows >= fb.nrow) return;
   frame_load_plan(sp, d.plans + b);
-  frame_geo_tile<TX, TSrc, kFused>(sp, fb, io, d.rows + 2 * b, blockIdx.x, blockIdx.y);
+  frame_geo_tile<TX, TSrc, kFused>(sp, fb, io, d.rows + 2 * b, blockIdx.x, blockIdx.y, d.cull_geo != 0);
 }
 
 template <typename K>
@@ -715,8 +798,14 @@ extern "C" int s1b_geo2rdr(const s1b_burst_plan_t *plan, const int16_t *dem, int
   dim3 grid((ncol + G_TX - 1) / G_TX, (nrow + G_RY - 1) / G_RY);
   if (grid.y > 65535) return s1b_fail(S1B_ERR_TOO_LARGE, "s1b_geo2rdr: DEM window too tall");
   geo2rdr_kernel<<<grid, G_TX, 0, st>>>(*plan, dem, dem_pitch, (const float2 *)deramped,
-                                         (float2 *)out, rows, nrow, ncol);
+                                         (float2 *)out, rows, nrow, ncol, g_cull_geo != 0);
   return s1b_launch_status();
+}
+
+extern "C" int s1b_set_geocode_culling(int32_t on) {
+  const int prev = g_cull_geo;
+  g_cull_geo = on ? 1 : 0;
+  return prev;
 }
 
 extern "C" int s1b_zero_doppler(const s1b_orbit_poly_t *orbit, const double *xyz, int64_t n,
@@ -848,7 +937,9 @@ int launch_geo(const FrameDev &d, const FrameIO &io, int cols, int ctas, cudaStr
   return s1b_launch_status();
 }
 
-int frame_launch_geo2rdr(const FrameDev &d, const FrameIO &io, int cols, int ctas, cudaStream_t st) {
+int frame_launch_geo2rdr(const FrameDev &dev, const FrameIO &io, int cols, int ctas, cudaStream_t st) {
+  FrameDev d = dev;
+  d.cull_geo = g_cull_geo;
   if (!d.fused_deramp) return launch_geo<float2, false>(d, io, cols, ctas, st);
   return d.sample_format == S1B_SAMPLES_CI16 ? launch_geo<short2, true>(d, io, cols, ctas, st)
                                              : launch_geo<float2, true>(d, io, cols, ctas, st);

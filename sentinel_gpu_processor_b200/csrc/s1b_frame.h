@@ -46,6 +46,7 @@ struct FrameDev {
   int32_t geo_tiles_x, geo_tiles_y;        // geocoding tiles of the largest window, per axis
   int32_t sample_format;                   // S1B_SAMPLES_C64 or S1B_SAMPLES_CI16
   int32_t fused_deramp;                    // 1: geocoding deramps its gathers (column tables only)
+  int32_t cull_geo;                        // 1: geocoding culls blocks outside the valid lines (set per launch)
 };
 
 // Run-time buffers of one frame launch sequence.

@@ -93,6 +93,13 @@ def geo2rdr(plan: _lib.BurstPlan, dem: torch.Tensor, deramped: torch.Tensor, out
     return out, rows
 
 
+def set_geocode_culling(on: bool) -> bool:
+    """Switch the geocoding's culling of blocks outside the burst's valid
+    lines for later geo2rdr and frame launches of the process (on by default;
+    the products are identical either way).  Returns the previous setting."""
+    return bool(_lib.load().s1b_set_geocode_culling(1 if on else 0))
+
+
 def crossmul_looks(ref, ref_box, sec, sec_box, box, rowlook, collook, want=("ifg", "amp1", "amp2", "coh"),
                    fill_seed=0):
     """Fused crossmul + looks + power looks + coherence.
