@@ -462,9 +462,10 @@ int s1b_frame_set_sample_format(s1b_frame_t *frame, int32_t format);
  * deramps a burst in its own kernel, csrc/src/geo2rdr.cu:138-158):
  * 1 (the default): the geocoding deramps the four samples of each bilinear
  * gather where it reads them, from the burst's raw samples and a per-column
- * coefficient table (no deramped copy of any burst is written); 0: a deramp
- * kernel writes every burst's deramped copy and the geocoding reads it.  The
- * products are bit-identical either way. */
+ * table of (-kt, etaref) (no deramped copy of any burst is written; one
+ * phasor per gathered line carries its deramp and the pixel's reramp); 0: a
+ * deramp kernel writes every burst's deramped copy and the geocoding reads
+ * it.  The products agree to float rounding (below 1e-6 rad of phase). */
 int s1b_frame_set_deramp_fusion(s1b_frame_t *frame, int32_t fused);
 /* Slot of pair k in the product arrays: first element and capacity. */
 int s1b_frame_pair_slot(const s1b_frame_t *frame, int32_t pair, int64_t *ml_off, int32_t *max_nrow_ml,

@@ -330,7 +330,7 @@ class BatchedFrameChain:
     products equal those of the complex64 buffer holding the same values.
     ``deramp_fused`` (default): the geocoding deramps the samples of each
     bilinear gather itself (no deramped copy of the bursts); False runs a
-    deramp kernel first.  The products are bit-identical either way.
+    deramp kernel first.  The products agree to float rounding.
     ``autotune`` picks the deramp and geocoding tile shapes and grid sizes on
     the actual frame.
     """

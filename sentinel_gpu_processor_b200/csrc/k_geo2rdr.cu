@@ -64,15 +64,20 @@ __device__ __forceinline__ float2 load_one(const short2 *p) {
 // TOPS deramp coefficients of burst column c (geo2rdr.cu:533-541): -pi kt
 // and etaref.  One function for the deramp kernels and the frame's column
 // table, so the fused geocoding forms exactly the deramp kernel's phases.
-__device__ __forceinline__ void tops_column(const s1b_burst_plan_t &P, int c, double &mkt, double &etaref) {
+__device__ __forceinline__ void tops_kt(const s1b_burst_plan_t &P, int c, double &kt, double &etaref) {
   const double tr = P.slant_range_time + c / P.range_sampling_rate;
   double dt = tr - P.fm[0];
   const double ka = P.fm[1] + dt * (P.fm[2] + P.fm[3] * dt);
   dt = tr - P.dc[0];
   const double fnc = P.dc[1] + dt * (P.dc[2] + P.dc[3] * dt);
-  const double kt = ka * P.ks / (ka - P.ks);
-  mkt = -kPiD * kt;
+  kt = ka * P.ks / (ka - P.ks);
   etaref = -fnc / ka - P.etac0;
+}
+
+__device__ __forceinline__ void tops_column(const s1b_burst_plan_t &P, int c, double &mkt, double &etaref) {
+  double kt;
+  tops_kt(P, c, kt, etaref);
+  mkt = -kPiD * kt;
 }
 
 // Azimuth time of line r relative to the burst centre: eta_r = -L ati / 2 +
@@ -208,6 +213,20 @@ __global__ void rows_init_kernel(int32_t *rows, int nrow) {
 // default; off only to compare the two, which give identical products).
 static int g_cull_geo = 1;
 
+// exp(i pi q) for the small phase differences between neighbouring burst
+// columns (|pi q| <= 0.1 rad): Taylor series of cos and sin to the fourth
+// and fifth order (truncation error < 1e-7); larger angles through phasor_pi.
+__device__ __forceinline__ float2 rotation_pi(double q) {
+  const float x = (float)q * 3.14159265f;
+  if (fabsf(x) > 0.1f) return phasor_pi(q);
+  const float x2 = x * x;
+  return make_float2(fmaf(x2, fmaf(x2, 1.f / 24.f, -0.5f), 1.f), x * fmaf(x2, -1.f / 6.f, 1.f));
+}
+
+__device__ __forceinline__ float2 lerp2(float2 a, float2 b, float f) {
+  return make_float2(fmaf(f, b.x - a.x, a.x), fmaf(f, b.y - a.y, a.y));
+}
+
 // Read-only (L1-cached) sample loads for the bilinear gathers.
 __device__ __forceinline__ float2 load_ro(const float2 *p) { return __ldg(p); }
 __device__ __forceinline__ float2 load_ro(const short2 *p) {
@@ -217,11 +236,15 @@ __device__ __forceinline__ float2 load_ro(const short2 *p) {
 
 // Geocoding of one tile.  Unfused (kFused false): `burst` is the deramped
 // burst (complex64).  Fused: `burst` holds the raw samples (complex64 or
-// complex int16) and `tops` the burst's per-column deramp coefficients
-// (-pi kt, etaref); each of the four bilinear samples is deramped where it is
-// gathered, with the deramp kernel's own expressions (deramp_sample), so the
-// result equals the unfused path's bit for bit and the deramped copy of the
-// burst is never written.
+// complex int16) and `tops` the burst's per-column TOPS coefficients
+// (-kt, etaref); the four bilinear samples are deramped where they are
+// gathered and the deramped copy of the burst is never written.  Bilinear
+// interpolation is linear, so each gathered line's deramp phasor (at its
+// first column) merges with the pixel's reramp into one phasor, and the
+// second column's sample turns by the small difference of the two columns'
+// deramp phases; the pixel's kt and etaref come from the two table entries
+// interpolated at its range.  The products differ from the unfused path's by
+// float rounding.
 //
 // Culling (cull true): a DEM window is the bounding box of a burst footprint
 // turned by the orbit heading, and about 40% of an IW burst's window lies
@@ -433,42 +456,46 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
         // limits passed in exceed the raster
         valid = valid && intr >= 0 && intr + 1 < P.samples && inta >= 0 && inta + 1 < P.lines;
         if (valid) {
-          // per-pixel TOPS reramp (geo2rdr.cu:210-219); kt = ka ks / (ka - ks)
-          // and etac = -fnc / ka share one reciprocal of ka (ka - ks)
-          const double tr = rng * two_over_c;
-          double dt = tr - P.fm[0];
-          const double ka = P.fm[1] + dt * (P.fm[2] + P.fm[3] * dt);
-          dt = tr - P.dc[0];
-          const double fnc = P.dc[1] + dt * (P.dc[2] + P.dc[3] * dt);
-          const double kmk = ka - P.ks;
-          const double inv = rcp_newton(ka * kmk);
-          const double kt = ka * P.ks * (ka * inv);
-          const double etaref = -fnc * (kmk * inv) - P.etac0;
           const double eta = -P.lines * P.dtaz / 2. + t - P.tstart;
-          const double ed = eta - etaref;
+          const double frd = rgoff - i32_to_f64(intr);
           // bilinear interpolation of the deramped burst (geo2rdr.cu:220-237)
-          const float fr = (float)(rgoff - intr), fa = (float)(azoff - inta);
+          const float fr = (float)frd, fa = (float)(azoff - i32_to_f64(inta));
           const size_t i1 = (size_t)inta * P.samples + intr;
-          float2 b1, b2, b3, b4;
           if constexpr (kFused) {
+            // the samples' deramp phases -kt (eta_line - etaref)^2 and the
+            // reramp + range phase (geo2rdr.cu:210-219, 238-243) in half-cycles
             const double2 t0 = __ldg(tops + intr), t1 = __ldg(tops + intr + 1);
-            const double ea = deramp_eta(P, inta), eb = deramp_eta(P, inta + 1);  // once per gathered line
-            b1 = deramp_at(load_ro(burst + i1), ea, t0.x, t0.y);
-            b2 = deramp_at(load_ro(burst + i1 + 1), ea, t1.x, t1.y);
-            b3 = deramp_at(load_ro(burst + i1 + P.samples), eb, t0.x, t0.y);
-            b4 = deramp_at(load_ro(burst + i1 + P.samples + 1), eb, t1.x, t1.y);
+            const double ed = eta - fma(frd, t1.y - t0.y, t0.y);
+            const double hr = fma(-fma(frd, t1.x - t0.x, t0.x), ed * ed, k4_wvl * rng);
+            const double ea = deramp_eta(P, inta), eb = deramp_eta(P, inta + 1);
+            double d0 = ea - t0.y, d1 = ea - t1.y;
+            const double qa0 = t0.x * d0 * d0, qa1 = t1.x * d1 * d1;
+            d0 = eb - t0.y;
+            d1 = eb - t1.y;
+            const double qb0 = t0.x * d0 * d0, qb1 = t1.x * d1 * d1;
+            const float2 s2 = cmul(load_ro(burst + i1 + 1), rotation_pi(qa1 - qa0));
+            const float2 s4 = cmul(load_ro(burst + i1 + P.samples + 1), rotation_pi(qb1 - qb0));
+            const float2 ca = cmul(lerp2(load_ro(burst + i1), s2, fr), phasor_pi(hr + qa0));
+            const float2 cb = cmul(lerp2(load_ro(burst + i1 + P.samples), s4, fr), phasor_pi(hr + qb0));
+            res = lerp2(ca, cb, fa);
           } else {
-            b1 = __ldg(burst + i1);
-            b2 = __ldg(burst + i1 + 1);
-            b3 = __ldg(burst + i1 + P.samples);
-            b4 = __ldg(burst + i1 + P.samples + 1);
+            // per-pixel TOPS reramp (geo2rdr.cu:210-219); kt = ka ks / (ka - ks)
+            // and etac = -fnc / ka share one reciprocal of ka (ka - ks)
+            const double tr = rng * two_over_c;
+            double dt = tr - P.fm[0];
+            const double ka = P.fm[1] + dt * (P.fm[2] + P.fm[3] * dt);
+            dt = tr - P.dc[0];
+            const double fnc = P.dc[1] + dt * (P.dc[2] + P.dc[3] * dt);
+            const double kmk = ka - P.ks;
+            const double inv = rcp_newton(ka * kmk);
+            const double kt = ka * P.ks * (ka * inv);
+            const double ed = eta - (-fnc * (kmk * inv) - P.etac0);
+            const float2 c1 = lerp2(__ldg(burst + i1), __ldg(burst + i1 + 1), fr);
+            const float2 c2 = lerp2(__ldg(burst + i1 + P.samples), __ldg(burst + i1 + P.samples + 1), fr);
+            // range phase and reramp (geo2rdr.cu:238-243): 4 pi rng / wvl + pi kt ed^2
+            // rad, formed in half-cycles
+            res = cmul(lerp2(c1, c2, fa), phasor_pi(fma(kt, ed * ed, k4_wvl * rng)));
           }
-          const float2 c1 = make_float2(fmaf(fr, b2.x - b1.x, b1.x), fmaf(fr, b2.y - b1.y, b1.y));
-          const float2 c2 = make_float2(fmaf(fr, b4.x - b3.x, b3.x), fmaf(fr, b4.y - b3.y, b3.y));
-          const float2 v = make_float2(fmaf(fa, c2.x - c1.x, c1.x), fmaf(fa, c2.y - c1.y, c1.y));
-          // range phase and reramp (geo2rdr.cu:238-243): 4 pi rng / wvl + pi kt ed^2
-          // rad, formed in half-cycles
-          res = cmul(v, phasor_pi(fma(kt, ed * ed, k4_wvl * rng)));
         }
         __stcs(out + (size_t)row * ncol + col, res);
       }
@@ -603,18 +630,17 @@ __device__ __forceinline__ void frame_geo_tile(const s1b_burst_plan_t &sp, const
                                     fb.ncol, tx, ty, cull);
 }
 
-// Per-column deramp coefficients (-pi kt, etaref) of every burst for the
-// fused geocoding: blockIdx.y = burst, a thread per column, written as
-// double2 into the burst's deramped-copy slot of the workspace (unused when
-// fused).
+// Per-column TOPS coefficients (-kt, etaref) of every burst for the fused
+// geocoding: blockIdx.y = burst, a thread per column, written as double2
+// into the burst's deramped-copy slot of the workspace (unused when fused).
 __global__ void frame_tops_table_kernel(const FrameDev d, const FrameIO io) {
   const int b = blockIdx.y;
   const s1b_burst_plan_t &sp = d.plans[b];
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= sp.samples) return;
-  double mkt, eref;
-  tops_column(sp, c, mkt, eref);
-  reinterpret_cast<double2 *>(io.work + d.bursts[b].der_off)[c] = make_double2(mkt, eref);
+  double kt, eref;
+  tops_kt(sp, c, kt, eref);
+  reinterpret_cast<double2 *>(io.work + d.bursts[b].der_off)[c] = make_double2(-kt, eref);
 }
 
 template <int TX, typename TSrc, bool kFused>
