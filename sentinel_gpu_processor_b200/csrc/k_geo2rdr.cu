@@ -252,9 +252,9 @@ __device__ __forceinline__ float2 load_ro(const short2 *p) {
 // zero-height line model, affine in (row, column), to its corner solutions,
 // with the line shift per metre of height; a block of 32 rows whose lines
 // stay outside [first_valid_line + 5, last_valid_line - 5) at every int16
-// height is written as zeros without solving its pixels.  Every block seeds
-// its Newton iteration from the line model, so a pixel's result does not
-// depend on whether the blocks before it were culled.
+// height is written as zeros without solving its pixels.  Every pixel seeds
+// its Newton iteration from the line model, so its result does not depend on
+// whether the blocks before it were culled.
 template <int TX, int RY, typename TSrc = float2, bool kFused = false>
 __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const int16_t *__restrict__ dem,
                                              int64_t pitch, const TSrc *__restrict__ burst,
@@ -402,7 +402,7 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
   __syncwarp();  // lane 0's patch and seed models are visible to the warp
   const ZeroDopplerPatch &zd = s_zd[wid];
   const double k4_wvl = 4.0 / P.wvl;  // two-way range phase, half-cycles per metre
-  double h = 0.0, hprev = 0.0, inv_c1 = 0.0;
+  double h = 0.0, inv_c1 = 0.0;
   int16_t hn = colok && rmax > 0 && !(cullmask & 1u) ? __ldg(dem + (int64_t)row0 * pitch + col) : 0;
   int rlo = INT_MAX, rhi = -1;
   for (int r = 0; r < rmax; ++r) {
@@ -432,19 +432,15 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
         p[1] = (re + hgt) * coslat * sinlon;
         p[2] = (re * (1 - kRe2D) + hgt) * sinlat;
         const ZeroDopplerPoint q = zero_doppler_point(zd, p);
-        if ((r & 31) == 0) {
-          // the block's first point starts from the line model; its slope
-          // serves the block (f' changes by < 1e-3 over 32 rows)
-          inv_c1 = rcp_newton(q.c1);
+        // the chord slope of the block's first point serves the block (f'
+        // changes by < 1e-3 over 32 rows); every point starts from the line
+        // model, within ~1e-6 s of its root
+        if ((r & 31) == 0) inv_c1 = rcp_newton(q.c1);
+        {
           const double4 m = s_seed[wid];
-          h = fma(m.w, hgt, fma(m.z, (double)r, fma(m.y, (double)col, m.x)));
-        } else {
-          const double hn2 = 2.0 * h - hprev;  // linear extrapolation from the two rows above
-          hprev = h;
-          h = hn2;
+          h = fma(m.w, hgt, fma(m.z, i32_to_f64(r), fma(m.y, i32_to_f64(col), m.x)));
         }
         const double rng = sqrt_heron(zero_doppler_solve(q, zd.c3, inv_c1, h));
-        if ((r & 31) == 0) hprev = h - s_seed[wid].z;
         const double t = zd.t0 + h;
         const double rgoff = (rng - P.rngstart) * inv_dmrg;
         const double azoff = (t - P.tstart) * prf;
@@ -667,10 +663,14 @@ __global__ __launch_bounds__(TX) void frame_geo2rdr_kernel(const FrameDev d, con
 // uniform global loads (measured 13.67 -> 13.28 ms per 27-pair frame).  The
 // grid spans the largest window; CTAs past a smaller one return before the
 // copy's barriers (a uniform test of the block index).  Registers are held
-// to 80 (768 threads per SM): at TX 128 that beats the 96 the compiler picks
-// (11.85 -> 11.62 ms per frame).
+// to 72 (896 threads per SM) at TX 64 and 128 and to 64 at TX 256, with a
+// few spills: geocoding of the 27-pair frame 9.16 -> 8.78 ms at TX 128 and
+// 9.32 -> 8.91 ms at TX 256 against 80 registers.
+template <int TX>
+constexpr int kGeoGridMinBlocks = TX == 256 ? 4 : 896 / TX;
+
 template <int TX, typename TSrc, bool kFused>
-__global__ __launch_bounds__(TX, 768 / TX) void frame_geo2rdr_grid_kernel(const FrameDev d, const FrameIO io) {
+__global__ __launch_bounds__(TX, kGeoGridMinBlocks<TX>) void frame_geo2rdr_grid_kernel(const FrameDev d, const FrameIO io) {
   __shared__ __align__(16) s1b_burst_plan_t sp;
   const int b = blockIdx.z;
   const FrameBurst &fb = d.bursts[b];

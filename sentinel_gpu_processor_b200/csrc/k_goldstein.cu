@@ -153,20 +153,37 @@ __device__ __forceinline__ void goldstein_patch(const float2 *__restrict__ in, f
 #pragma unroll
   for (int r = 0; r < GN; ++r) M[r][lane] = hypotf(x[r].x, x[r].y);
   __syncwarp();
-  // 7x7 circular smoothing of |F| (goldstein.cu:105-119) and its patch sum
+  // 7x7 circular smoothing of |F| (goldstein.cu:105-119) and its patch sum.
+  // The table is even in both offsets, g[ky][kx] = g[|ky|][|kx|], so
+  //   S[y][x] = W0[y][x] + sum_{b=1..3} (Wb[y][x - b] + Wb[y][x + b]),
+  //   Wb[y][x] = sum_{a=0..3} g[a][b] (M[y - a][x] + M[y + a][x])  (a = 0 once):
+  // the four vertical filters Wb run down the lane's own column from a
+  // sliding window of seven rows, the horizontal offsets are lane shuffles
+  // (their wrap-around is the circular boundary).
   float S[GN];
   float psum = 0.f;
+  {
+    float win[7];  // M[y - 3 .. y + 3][lane]
 #pragma unroll
-  for (int y = 0; y < GN; ++y) {
-    float s = 0.f;
+    for (int k = 0; k < 6; ++k) win[k + 1] = M[(k - 3 + GN) & (GN - 1)][lane];
 #pragma unroll
-    for (int ky = -3; ky <= 3; ++ky) {
+    for (int y = 0; y < GN; ++y) {
 #pragma unroll
-      for (int kx = -3; kx <= 3; ++kx)
-        s += M[(y + ky + GN) & (GN - 1)][(lane + kx + GN) & (GN - 1)] * c_gauss[(ky + 3) * 7 + kx + 3];
+      for (int k = 0; k < 6; ++k) win[k] = win[k + 1];
+      win[6] = M[(y + 3) & (GN - 1)][lane];
+      const float p1 = win[2] + win[4], p2 = win[1] + win[5], p3 = win[0] + win[6];
+      float w[4];
+#pragma unroll
+      for (int b = 0; b < 4; ++b)  // g[a][b] = c_gauss[(3 - a) * 7 + 3 + b]
+        w[b] = fmaf(c_gauss[21 + 3 + b], win[3],
+                    fmaf(c_gauss[14 + 3 + b], p1, fmaf(c_gauss[7 + 3 + b], p2, c_gauss[3 + b] * p3)));
+      float s = w[0];
+#pragma unroll
+      for (int b = 1; b < 4; ++b)
+        s += __shfl_sync(0xffffffffu, w[b], (lane - b) & (GN - 1)) + __shfl_sync(0xffffffffu, w[b], (lane + b) & (GN - 1));
+      S[y] = s;
+      psum += s;
     }
-    S[y] = s;
-    psum += s;
   }
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) psum += __shfl_xor_sync(0xffffffffu, psum, off);
