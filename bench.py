@@ -49,9 +49,9 @@ GEO_BYTES_PER_BURST_PX = 8
 # kernels stream their inputs once, so traffic scales with the unit count.
 GEO_DRAM_BYTES_PER_GEO_PX = 23.63
 # fused frame geocoding (deramp in the gathers): ncu DRAM traffic over algorithmic
-# bytes on the small frame (487.1 MB / 496.2 MB, profiles/geo2rdr_frame_fused.md);
-# both terms (raw samples read, geocoded pixels written) scale with the frame
-GEO_FUSED_TRAFFIC_RATIO = 0.982
+# bytes of one launch on the small frame (586.5 MB / 496.1 MB); both terms (raw
+# samples read, geocoded pixels written) scale with the frame
+GEO_FUSED_TRAFFIC_RATIO = 1.182
 RESAMPLE_DRAM_BYTES_PER_PX = 24.75
 
 

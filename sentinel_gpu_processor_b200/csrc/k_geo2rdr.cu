@@ -512,6 +512,9 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
   }
 }
 
+// No register cap: on the 1500 x 21000 burst 32-row tiles at the compiler's
+// 96 registers beat 72 registers and 64- or 128-row tiles (0.219 against
+// 0.226-0.260 ms).
 __global__ __launch_bounds__(G_TX) void geo2rdr_kernel(
     const __grid_constant__ s1b_burst_plan_t P, const int16_t *__restrict__ dem, int64_t pitch,
     const float2 *__restrict__ burst, float2 *__restrict__ out, int32_t *__restrict__ rows,
@@ -639,8 +642,13 @@ __global__ void frame_tops_table_kernel(const FrameDev d, const FrameIO io) {
   reinterpret_cast<double2 *>(io.work + d.bursts[b].der_off)[c] = make_double2(-kt, eref);
 }
 
+// Minimum resident CTAs the frame's geocoding kernels are compiled for: 72
+// registers at TX 64 and 128, 64 at TX 256.
+template <int TX>
+constexpr int kGeoGridMinBlocks = TX == 256 ? 4 : 896 / TX;
+
 template <int TX, typename TSrc, bool kFused>
-__global__ __launch_bounds__(TX) void frame_geo2rdr_kernel(const FrameDev d, const FrameIO io) {
+__global__ __launch_bounds__(TX, kGeoGridMinBlocks<TX>) void frame_geo2rdr_kernel(const FrameDev d, const FrameIO io) {
   __shared__ __align__(16) s1b_burst_plan_t sp;
   int cur = -1;
   for (int64_t idx = blockIdx.x; idx < d.n_geo_tiles; idx += gridDim.x) {
@@ -666,9 +674,6 @@ __global__ __launch_bounds__(TX) void frame_geo2rdr_kernel(const FrameDev d, con
 // to 72 (896 threads per SM) at TX 64 and 128 and to 64 at TX 256, with a
 // few spills: geocoding of the 27-pair frame 9.16 -> 8.78 ms at TX 128 and
 // 9.32 -> 8.91 ms at TX 256 against 80 registers.
-template <int TX>
-constexpr int kGeoGridMinBlocks = TX == 256 ? 4 : 896 / TX;
-
 template <int TX, typename TSrc, bool kFused>
 __global__ __launch_bounds__(TX, kGeoGridMinBlocks<TX>) void frame_geo2rdr_grid_kernel(const FrameDev d, const FrameIO io) {
   __shared__ __align__(16) s1b_burst_plan_t sp;
