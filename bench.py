@@ -52,6 +52,8 @@ GEO_DRAM_BYTES_PER_GEO_PX = 23.63
 # bytes of one launch on the small frame (586.5 MB / 496.1 MB); both terms (raw
 # samples read, geocoded pixels written) scale with the frame
 GEO_FUSED_TRAFFIC_RATIO = 1.182
+# the same with the crossmul look sums formed in the geocoding (391.7 MB / 290.7 MB)
+GEO_XMUL_TRAFFIC_RATIO = 1.347
 RESAMPLE_DRAM_BYTES_PER_PX = 24.75
 
 
@@ -66,6 +68,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--deramp", default="fused", choices=["fused", "kernel"],
                     help="frame deramp: inside the geocoding's gathers, or a separate kernel writing deramped bursts")
+    ap.add_argument("--crossmul", default="fused", choices=["fused", "kernel"],
+                    help="frame: crossmul look sums formed in the geocoding (fused) or a crossmul kernel reading "
+                         "geocoded windows")
     ap.add_argument("--samples", default="ci16", choices=["ci16", "c64"],
                     help="frame SLC sample type: complex int16 as in the measurement TIFF (widened on the GPU), "
                          "or complex64 as the reference's geo2rdr pipe carries it")
@@ -275,7 +280,8 @@ def _workload(args, rank, dev):
         sc = synth.make_frame(seed=20261203 + 2000 + rank, device=dev,
                               **(dict(n_swaths=1, n_bursts=3, scale=0.5) if small else {}))
         chain = BatchedFrameChain(sc.ref, sc.sec, sc.rsc, sc.rowlook, sc.collook, sc.alpha, device=dev,
-                                  sample_format=args.samples, deramp_fused=args.deramp == "fused")
+                                  sample_format=args.samples, deramp_fused=args.deramp == "fused",
+                                  crossmul_fused=args.crossmul == "fused")
         if args.samples == "ci16":
             for v, s in zip(chain.ref_views + chain.sec_views, sc.ref_slc + sc.sec_slc):
                 v.copy_(synth.cint16(s))
@@ -518,6 +524,20 @@ def _kernel_table(chain, sc, args, times, peak):
             bytes_per = {"deramp": (din + 8) * burst,
                          "geo2rdr": GEO_BYTES_PER_GEO_PX * geo + GEO_BYTES_PER_BURST_PX * burst}
         bytes_per.update({"crossmul_looks": 16 * box_px + 20 * ml, "goldstein": 16 * ml})
+        if getattr(chain, "crossmul_fused", False):
+            # the geocoding reads each DEM height once per pair and writes one
+            # float4 of look sums per column and look row of the pair's union
+            # window instead of both geocoded windows; the crossmul stage reads
+            # the sums over the box
+            rl = chain.rowlook
+            union = 0
+            for a, b in zip(pls[0::2], pls[1::2]):
+                top = min(a.win_top, b.win_top) // rl * rl
+                n_rows = -(-(max(a.win_bottom, b.win_bottom) - top) // rl) * rl
+                union += n_rows * (max(a.win_right, b.win_right) - min(a.win_left, b.win_left))
+            geo_in = bytes_per["geo2rdr"] - GEO_BYTES_PER_GEO_PX * geo
+            bytes_per["geo2rdr"] = geo_in + 2 * union + 16 * union // rl
+            bytes_per["crossmul_looks"] = 16 * box_px // rl + 20 * ml
     else:
         pls = [p for pl in chain.pairs for p in pl] if args.config == "frame_pairs" else chain.plans
         n = len(pls)
@@ -600,7 +620,9 @@ def run_s1b(args):
                  "ifg_ml_shapes_first3": [list(r.ifg.shape) for r in res[:3]],
                  "batched": True, "cuda_graph": True, "tuning": chain.tuned,
                  "slc_samples": "complex int16" if args.samples == "ci16" else "complex64",
-                 "deramp": "fused into the geocoding gathers" if chain.deramp_fused else "separate kernel"}
+                 "deramp": "fused into the geocoding gathers" if chain.deramp_fused else "separate kernel",
+                 "crossmul": ("look sums formed in the geocoding (no geocoded windows)" if chain.crossmul_fused
+                              else "kernel reading the geocoded windows")}
         launches = chain.launches_per_step()
     elif args.config == "frame_pairs":
         extra = {"burst_pairs": len(chain.pairs), "burst_px_per_step": chain.burst_pixels,
@@ -618,8 +640,12 @@ def run_s1b(args):
     traffic = None
     if top == "geo2rdr":
         if args.config in FRAME_CONFIGS:  # one launch geocodes every burst
-            traffic = (GEO_FUSED_TRAFFIC_RATIO * table["geo2rdr"]["bytes_per_launch"] if chain.deramp_fused
-                       else GEO_DRAM_BYTES_PER_GEO_PX * sum(p.nrow * p.ncol for p in chain.plans))
+            if chain.crossmul_fused:
+                traffic = (GEO_XMUL_TRAFFIC_RATIO * table["geo2rdr"]["bytes_per_launch"]
+                           if GEO_XMUL_TRAFFIC_RATIO and chain.deramp_fused else None)
+            else:
+                traffic = (GEO_FUSED_TRAFFIC_RATIO * table["geo2rdr"]["bytes_per_launch"] if chain.deramp_fused
+                           else GEO_DRAM_BYTES_PER_GEO_PX * sum(p.nrow * p.ncol for p in chain.plans))
         else:
             pls = [p for pl in chain.pairs for p in pl] if args.config == "frame_pairs" else chain.plans
             traffic = GEO_DRAM_BYTES_PER_GEO_PX * sum(p.nrow * p.ncol for p in pls) / len(pls)

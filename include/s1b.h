@@ -467,6 +467,16 @@ int s1b_frame_set_sample_format(s1b_frame_t *frame, int32_t format);
  * deramp kernel writes every burst's deramped copy and the geocoding reads
  * it.  The products agree to float rounding (below 1e-6 rad of phase). */
 int s1b_frame_set_deramp_fusion(s1b_frame_t *frame, int32_t fused);
+/* Crossmul stage of later runs (no reference counterpart; the reference's
+ * crossmul_daemon reads the geocoded .gslc files, crossmul_daemon.cu:520-528,
+ * 921-975): 1 (the default when rowlook <= 128): the geocoding kernel
+ * geocodes both bursts of a pair at each DEM pixel and sums conj(ref) sec and
+ * both powers over each column's look rows; a second kernel adds the look
+ * columns of the overlap box.  No geocoded window is written.  0: the
+ * geocoding writes every burst's window and the crossmul kernel reads them.
+ * The products agree to float rounding (the sums are formed in the same
+ * order; the geocoding tiles differ).  S1B_ERR_UNSUPPORTED for rowlook > 128. */
+int s1b_frame_set_crossmul_fusion(s1b_frame_t *frame, int32_t fused);
 /* Slot of pair k in the product arrays: first element and capacity. */
 int s1b_frame_pair_slot(const s1b_frame_t *frame, int32_t pair, int64_t *ml_off, int32_t *max_nrow_ml,
                         int32_t *max_ncol_ml);

@@ -179,6 +179,7 @@ _SIGNATURES = {
     "s1b_frame_set_tuning": (c_int, [c_void_p, POINTER(c_int32)]),
     "s1b_frame_set_sample_format": (c_int, [c_void_p, c_int32]),
     "s1b_frame_set_deramp_fusion": (c_int, [c_void_p, c_int32]),
+    "s1b_frame_set_crossmul_fusion": (c_int, [c_void_p, c_int32]),
 }
 
 _lib = None

@@ -331,12 +331,16 @@ class BatchedFrameChain:
     ``deramp_fused`` (default): the geocoding deramps the samples of each
     bilinear gather itself (no deramped copy of the bursts); False runs a
     deramp kernel first.  The products agree to float rounding.
+    ``crossmul_fused`` (default): the geocoding kernel geocodes both bursts
+    of a pair at each DEM pixel and forms the crossmul's look-row sums (no
+    geocoded windows are written); False geocodes every window and runs the
+    crossmul kernel on them.  The products agree to float rounding.
     ``autotune`` picks the deramp and geocoding tile shapes and grid sizes on
     the actual frame.
     """
 
     def __init__(self, refs, secs, rsc, rowlook, collook, alpha, n_win=32, device="cuda", fill_seed=0,
-                 sample_format="c64", deramp_fused=True):
+                 sample_format="c64", deramp_fused=True, crossmul_fused=True):
         import ctypes
         if sample_format not in ("c64", "ci16"):
             raise ValueError("sample_format must be 'c64' (complex64) or 'ci16' (complex int16)")
@@ -367,6 +371,9 @@ class BatchedFrameChain:
             _lib.check(lib.s1b_frame_set_sample_format(handle, _lib.S1B_SAMPLES_CI16), "s1b_frame_set_sample_format")
         self.deramp_fused = bool(deramp_fused)
         _lib.check(lib.s1b_frame_set_deramp_fusion(handle, int(self.deramp_fused)), "s1b_frame_set_deramp_fusion")
+        self.crossmul_fused = bool(crossmul_fused) and self.rowlook <= 128
+        _lib.check(lib.s1b_frame_set_crossmul_fusion(handle, int(self.crossmul_fused)),
+                   "s1b_frame_set_crossmul_fusion")
         sz = _lib.FrameSizes()
         _lib.check(lib.s1b_frame_sizes(handle, ctypes.byref(sz)), "s1b_frame_sizes")
         self.sizes = sz

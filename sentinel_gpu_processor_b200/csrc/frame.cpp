@@ -201,6 +201,15 @@ extern "C" int s1b_frame_create(const s1b_burst_plan_t *plans, int32_t n_bursts,
     max_r = std::max(max_r, pr.max_nrow_ml);
     max_c = std::max(max_c, pr.max_ncol_ml);
     max_p = std::max(max_p, ni * nj);
+    // look-row sums of the fused crossmul over the union of the two windows
+    const s1b_burst_plan_t &a = plans[pr.ref], &c = plans[pr.sec];
+    const int top = std::min(a.win_top, c.win_top), bottom = std::max(a.win_bottom, c.win_bottom);
+    pr.part_top = top / rowlook * rowlook;
+    pr.part_rows = (bottom - pr.part_top + rowlook - 1) / rowlook;
+    pr.part_left = std::min(a.win_left, c.win_left);
+    pr.part_cols = std::max(a.win_right, c.win_right) - pr.part_left;
+    pr.part_off = work;
+    work = align_up(work + 2 * (int64_t)pr.part_rows * pr.part_cols);  // float4 = 2 complex64
   }
   f->slc_elems = slc;
   f->product_elems = ml;
@@ -233,6 +242,14 @@ extern "C" int s1b_frame_create(const s1b_burst_plan_t *plans, int32_t n_bursts,
   d.max_nrow_ml = max_r;
   d.max_ncol_ml = max_c;
   d.max_patches = max_p;
+  // crossmul fused into the geocoding when a look row fits a geocoding tile
+  d.fused_xmul = rowlook <= kFrameGeoRows ? 1 : 0;
+  d.xm_tiles_x = d.xm_tiles_y = 0;
+  if (d.fused_xmul)
+    for (const FramePair &pr : f->pairs) {
+      d.xm_tiles_x = std::max(d.xm_tiles_x, (pr.part_cols + kFrameXmCols - 1) / kFrameXmCols);
+      d.xm_tiles_y = std::max(d.xm_tiles_y, (pr.part_rows + kFrameGeoRows / rowlook - 1) / (kFrameGeoRows / rowlook));
+    }
   int s = set_tiles(f);
   if (s) {
     release(f);
@@ -296,6 +313,20 @@ extern "C" int s1b_frame_tuning(const s1b_frame_t *f, int32_t tuning[4]) {
 extern "C" int s1b_frame_set_deramp_fusion(s1b_frame_t *f, int32_t fused) {
   if (!f) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_frame_set_deramp_fusion: null frame");
   f->dev.fused_deramp = fused ? 1 : 0;
+  return S1B_OK;
+}
+
+extern "C" int s1b_frame_set_crossmul_fusion(s1b_frame_t *f, int32_t fused) {
+  if (!f) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_frame_set_crossmul_fusion: null frame");
+  if (fused && f->dev.rowlook > kFrameGeoRows)
+    return s1b_fail(S1B_ERR_UNSUPPORTED, "s1b_frame_set_crossmul_fusion: rowlook above 128");
+  if (fused && f->dev.xm_tiles_x == 0)
+    for (const FramePair &pr : f->pairs) {
+      f->dev.xm_tiles_x = std::max(f->dev.xm_tiles_x, (pr.part_cols + kFrameXmCols - 1) / kFrameXmCols);
+      f->dev.xm_tiles_y = std::max(f->dev.xm_tiles_y, (pr.part_rows + kFrameGeoRows / f->dev.rowlook - 1) /
+                                                          (kFrameGeoRows / f->dev.rowlook));
+    }
+  f->dev.fused_xmul = fused ? 1 : 0;
   return S1B_OK;
 }
 
@@ -364,6 +395,7 @@ extern "C" int s1b_frame_autotune(s1b_frame_t *f, const void *slc, const int16_t
       s = frame_launch_deramp(f->dev, io, f->tuning[0], f->tuning[1], f->split, st);
       continue;
     }
+    if (stage == 1 && f->dev.fused_xmul) continue;  // the fused kernel has one tile shape
     int best_shape = f->tuning[stage * 2], best_ctas = f->tuning[stage * 2 + 1];
     float best = 3.4e38f;
     for (int shape : shapes[stage]) {

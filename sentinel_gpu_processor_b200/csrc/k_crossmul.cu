@@ -51,6 +51,33 @@ struct XmArgs {
   uint64_t seed;
 };
 
+// Multilooked pixel o from its sums over the look window: mean over collook,
+// then over rowlook, like cpx_col_look / cpx_row_look; amplitudes; coherence
+// with the seeded fill; phase.
+__device__ __forceinline__ void xm_finish(float ir, float ii, float p1, float p2, int rowlook, int collook, int64_t o,
+                                          float2 *ifg, float *amp1, float *amp2, float *coh, float *phase,
+                                          uint64_t seed) {
+  const float fcl = (float)collook, frl = (float)rowlook;
+  ir = ir / fcl / frl;
+  ii = ii / fcl / frl;
+  // s1proc's powlooks returns |s| rather than |s|^2 when both looks are 1
+  // (s1proc/sario.py:416-418), so its amplitude is then sqrt(|s|); kept so
+  // that .amp and coherence values match the reference's.
+  const bool unit = (rowlook == 1 && collook == 1);
+  const float am1 = unit ? sqrtf(sqrtf(p1)) : sqrtf(p1 / fcl / frl);
+  const float am2 = unit ? sqrtf(sqrtf(p2)) : sqrtf(p2 / fcl / frl);
+  if (ifg) ifg[o] = make_float2(ir, ii);
+  if (amp1) amp1[o] = am1;
+  if (amp2) amp2[o] = am2;
+  if (coh) {
+    // s1proc/coherence.py:142-144
+    float c = hypotf(ir, ii) / (am1 + 1e-12f) / (am2 + 1e-12f);
+    if (c > 1.f) c = fill_uniform(seed, (uint64_t)o);
+    coh[o] = c;
+  }
+  if (phase) phase[o] = atan2f(ii, ir);
+}
+
 // One CTA: multilooked row i, columns [chunk * m_per_cta, ...).
 __device__ __forceinline__ void crossmul_tile(const XmArgs &a, int i, int chunk, float4 *smem4) {
   const int W = a.m_per_cta * a.collook;  // full-res columns of this CTA
@@ -83,25 +110,15 @@ __device__ __forceinline__ void crossmul_tile(const XmArgs &a, int i, int chunk,
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          // conj(r) * s  (sario.cu:207-208)
-          ir[q] += r[u][q].x * s[u][q].x + r[u][q].y * s[u][q].y;
-          ii[q] += -r[u][q].y * s[u][q].x + r[u][q].x * s[u][q].y;
-          p1[q] += r[u][q].x * r[u][q].x + r[u][q].y * r[u][q].y;
-          p2[q] += s[u][q].x * s[u][q].x + s[u][q].y * s[u][q].y;
-        }
+        for (int q = 0; q < 2; ++q) xm_accumulate(r[u][q], s[u][q], ir[q], ii[q], p1[q], p2[q]);
       }
     }
     for (; k < a.rowlook; ++k) {
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
         const int col = q ? cc : c;
-        const float2 r = __ldg(pr + (int64_t)k * a.ref_width + col);
-        const float2 s = __ldg(ps + (int64_t)k * a.sec_width + col);
-        ir[q] += r.x * s.x + r.y * s.y;
-        ii[q] += -r.y * s.x + r.x * s.y;
-        p1[q] += r.x * r.x + r.y * r.y;
-        p2[q] += s.x * s.x + s.y * s.y;
+        xm_accumulate(__ldg(pr + (int64_t)k * a.ref_width + col), __ldg(ps + (int64_t)k * a.sec_width + col), ir[q],
+                      ii[q], p1[q], p2[q]);
       }
     }
     sI[c] = make_float2(ir[0], ii[0]);
@@ -112,7 +129,6 @@ __device__ __forceinline__ void crossmul_tile(const XmArgs &a, int i, int chunk,
     }
   }
   __syncthreads();
-  const float fcl = (float)a.collook, frl = (float)a.rowlook;
   for (int m = threadIdx.x; m < mcta; m += XM_THREADS) {
     float ir = 0.f, ii = 0.f, p1 = 0.f, p2 = 0.f;
     const int base = m * a.collook;
@@ -124,26 +140,8 @@ __device__ __forceinline__ void crossmul_tile(const XmArgs &a, int i, int chunk,
       p1 += p.x;
       p2 += p.y;
     }
-    // mean over collook, then over rowlook, like cpx_col_look / cpx_row_look
-    ir = ir / fcl / frl;
-    ii = ii / fcl / frl;
-    // s1proc's powlooks returns |s| rather than |s|^2 when both looks are 1
-    // (s1proc/sario.py:416-418), so its amplitude is then sqrt(|s|); kept so
-    // that .amp and coherence values match the reference's.
-    const bool unit = (a.rowlook == 1 && a.collook == 1);
-    const float am1 = unit ? sqrtf(sqrtf(p1)) : sqrtf(p1 / fcl / frl);
-    const float am2 = unit ? sqrtf(sqrtf(p2)) : sqrtf(p2 / fcl / frl);
-    const int64_t o = (int64_t)i * a.ncol_ml + j0 + m;
-    if (a.ifg) a.ifg[o] = make_float2(ir, ii);
-    if (a.amp1) a.amp1[o] = am1;
-    if (a.amp2) a.amp2[o] = am2;
-    if (a.coh) {
-      // s1proc/coherence.py:142-144
-      float c = hypotf(ir, ii) / (am1 + 1e-12f) / (am2 + 1e-12f);
-      if (c > 1.f) c = fill_uniform(a.seed, (uint64_t)o);
-      a.coh[o] = c;
-    }
-    if (a.phase) a.phase[o] = atan2f(ii, ir);
+    xm_finish(ir, ii, p1, p2, a.rowlook, a.collook, (int64_t)i * a.ncol_ml + j0 + m, a.ifg, a.amp1, a.amp2, a.coh,
+              a.phase, a.seed);
   }
 }
 
@@ -168,7 +166,6 @@ __device__ __forceinline__ void crossmul_rows_tile(const XmArgs &a, int i0, int 
   const int64_t col0 = (int64_t)j0 * a.collook;
   const int i1 = min(i0 + XM_ROWS, a.nrow_ml);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const float fcl = (float)a.collook, frl = (float)a.rowlook;
   for (int i = i0; i < i1; ++i) {
     float4 *buf = smem4 + ((i - i0) & 1) * W;
     const int64_t row0 = (int64_t)i * a.rowlook;
@@ -191,24 +188,15 @@ __device__ __forceinline__ void crossmul_rows_tile(const XmArgs &a, int i0, int 
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
 #pragma unroll
-          for (int q = 0; q < 2; ++q) {
-            ir[q] += r[u][q].x * s[u][q].x + r[u][q].y * s[u][q].y;
-            ii[q] += -r[u][q].y * s[u][q].x + r[u][q].x * s[u][q].y;
-            p1[q] += r[u][q].x * r[u][q].x + r[u][q].y * r[u][q].y;
-            p2[q] += s[u][q].x * s[u][q].x + s[u][q].y * s[u][q].y;
-          }
+          for (int q = 0; q < 2; ++q) xm_accumulate(r[u][q], s[u][q], ir[q], ii[q], p1[q], p2[q]);
         }
       }
       for (; k < a.rowlook; ++k) {
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
           const int col = q ? cc : c;
-          const float2 r = __ldg(pr + (int64_t)k * a.ref_width + col);
-          const float2 s = __ldg(ps + (int64_t)k * a.sec_width + col);
-          ir[q] += r.x * s.x + r.y * s.y;
-          ii[q] += -r.y * s.x + r.x * s.y;
-          p1[q] += r.x * r.x + r.y * r.y;
-          p2[q] += s.x * s.x + s.y * s.y;
+          xm_accumulate(__ldg(pr + (int64_t)k * a.ref_width + col), __ldg(ps + (int64_t)k * a.sec_width + col),
+                        ir[q], ii[q], p1[q], p2[q]);
         }
       }
       buf[c] = make_float4(ir[0], ii[0], p1[0], p2[0]);
@@ -228,21 +216,8 @@ __device__ __forceinline__ void crossmul_rows_tile(const XmArgs &a, int i0, int 
         p1 += v.z;
         p2 += v.w;
       }
-      ir = ir / fcl / frl;
-      ii = ii / fcl / frl;
-      const bool unit = (a.rowlook == 1 && a.collook == 1);
-      const float am1 = unit ? sqrtf(sqrtf(p1)) : sqrtf(p1 / fcl / frl);
-      const float am2 = unit ? sqrtf(sqrtf(p2)) : sqrtf(p2 / fcl / frl);
-      const int64_t o = (int64_t)i * a.ncol_ml + j0 + m;
-      if (a.ifg) a.ifg[o] = make_float2(ir, ii);
-      if (a.amp1) a.amp1[o] = am1;
-      if (a.amp2) a.amp2[o] = am2;
-      if (a.coh) {
-        float c = hypotf(ir, ii) / (am1 + 1e-12f) / (am2 + 1e-12f);
-        if (c > 1.f) c = fill_uniform(a.seed, (uint64_t)o);
-        a.coh[o] = c;
-      }
-      if (a.phase) a.phase[o] = atan2f(ii, ir);
+      xm_finish(ir, ii, p1, p2, a.rowlook, a.collook, (int64_t)i * a.ncol_ml + j0 + m, a.ifg, a.amp1, a.amp2,
+                a.coh, a.phase, a.seed);
     }
   }
 }
@@ -345,7 +320,9 @@ __global__ void frame_box_kernel(const FrameDev d, s1b_frame_pair_t *pout) {
 
 // Crossmul + looks of every pair: blockIdx.z = pair, x = group of XM_ROWS
 // multilooked rows, y = column chunk; CTAs outside a pair's box return at once.
-__global__ __launch_bounds__(XM_THREADS) void frame_crossmul_kernel(const FrameDev d, const FrameIO io,
+// Compiled for 4 CTAs per SM (64 registers): left to itself the compiler
+// picks 48 registers and spills.
+__global__ __launch_bounds__(XM_THREADS, 4) void frame_crossmul_kernel(const FrameDev d, const FrameIO io,
                                                                    int m_per_cta) {
   extern __shared__ float4 smem4[];
   const int k = blockIdx.z;
@@ -373,6 +350,67 @@ __global__ __launch_bounds__(XM_THREADS) void frame_crossmul_kernel(const FrameD
   a.phase = nullptr;
   a.seed = d.fill_seed;
   crossmul_rows_tile(a, blockIdx.x * XM_ROWS, blockIdx.y, smem4);
+}
+
+// Crossmul fused into the geocoding: the geocoding kernel left, per pair,
+// the rowlook-row sums of every column of the pair's windows (one float4 per
+// column and look row: conj product re, im, both powers, summed like
+// crossmul_rows_tile sums them).  Each warp here takes 32 multilooked pixels
+// of a row of the box: it stages their contiguous span of column sums in
+// shared memory with coalesced loads, then each lane adds the collook
+// columns of its pixel in order and forms the outputs.
+// blockIdx.z = pair, y = multilooked row, x = groups of 128 multilooked columns.
+constexpr int XC_SPAN = 640;  // float4 per warp buffer (10 KB)
+
+__global__ __launch_bounds__(128) void frame_xm_cells_kernel(const FrameDev d, const FrameIO io) {
+  __shared__ float4 buf[4][XC_SPAN];
+  const int k = blockIdx.z, i = blockIdx.y, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const s1b_frame_pair_t &r = io.pout[k];
+  const int jw = blockIdx.x * 128 + w * 32;  // the warp's first multilooked column
+  if (!r.ok || i >= r.nrow_ml || jw >= r.ncol_ml) return;  // warp-uniform
+  const FramePair pr = d.pairs[k];
+  const int cl = d.collook;
+  const float4 *row = reinterpret_cast<const float4 *>(io.work + pr.part_off) +
+                      (int64_t)((r.box[1] - pr.part_top) / d.rowlook + i) * pr.part_cols + (r.box[0] - pr.part_left);
+  float2 *ifg = io.ifg + pr.ml_off;
+  float *amp1 = io.amp1 ? io.amp1 + pr.ml_off : nullptr, *amp2 = io.amp2 ? io.amp2 + pr.ml_off : nullptr;
+  float *coh = io.coh ? io.coh + pr.ml_off : nullptr;
+  if (cl > XC_SPAN) {  // very wide looks: each lane reads its own columns
+    const int j = jw + lane;
+    if (j >= r.ncol_ml) return;
+    float ir = 0.f, ii = 0.f, p1 = 0.f, p2 = 0.f;
+    for (int u = 0; u < cl; ++u) {
+      const float4 v = __ldcs(row + (int64_t)j * cl + u);
+      ir += v.x;
+      ii += v.y;
+      p1 += v.z;
+      p2 += v.w;
+    }
+    xm_finish(ir, ii, p1, p2, d.rowlook, cl, (int64_t)i * r.ncol_ml + j, ifg, amp1, amp2, coh, nullptr, d.fill_seed);
+    return;
+  }
+  const int per = min(32, XC_SPAN / cl);  // pixels per pass
+  for (int m0 = 0; m0 < 32; m0 += per) {
+    const int j0 = jw + m0, n = min(min(per, 32 - m0), r.ncol_ml - j0);
+    if (n <= 0) break;
+    const float4 *src = row + (int64_t)j0 * cl;
+    __syncwarp();  // the previous pass is done with the buffer
+    for (int e = lane; e < n * cl; e += 32) buf[w][e] = __ldcs(src + e);
+    __syncwarp();
+    if (lane < n) {
+      float ir = 0.f, ii = 0.f, p1 = 0.f, p2 = 0.f;
+      const float4 *b = buf[w] + lane * cl;
+      for (int u = 0; u < cl; ++u) {
+        const float4 v = b[u];
+        ir += v.x;
+        ii += v.y;
+        p1 += v.z;
+        p2 += v.w;
+      }
+      xm_finish(ir, ii, p1, p2, d.rowlook, cl, (int64_t)i * r.ncol_ml + j0 + lane, ifg, amp1, amp2, coh, nullptr,
+                d.fill_seed);
+    }
+  }
 }
 
 }  // namespace
@@ -469,6 +507,11 @@ int frame_launch_box(const FrameDev &d, const FrameIO &io, cudaStream_t st) {
 int frame_launch_crossmul(const FrameDev &d, const FrameIO &io, cudaStream_t st) {
   if (d.collook > XM_MAX_COLLOOK) return s1b_fail(S1B_ERR_TOO_LARGE, "frame crossmul: collook above 4096");
   if (d.max_nrow_ml <= 0 || d.max_ncol_ml <= 0) return S1B_OK;
+  if (d.fused_xmul) {  // the geocoding left the look-row sums: add the look columns
+    if (d.max_nrow_ml > 65535 || d.n_pairs > 65535) return s1b_fail(S1B_ERR_TOO_LARGE, "frame crossmul: grid too large");
+    frame_xm_cells_kernel<<<dim3((d.max_ncol_ml + 127) / 128, d.max_nrow_ml, d.n_pairs), 128, 0, st>>>(d, io);
+    return s1b_launch_status();
+  }
   const int m_per_cta = d.collook >= 512 ? 1 : 512 / d.collook;
   const size_t smem = (size_t)m_per_cta * d.collook * 2 * sizeof(float4);  // two buffers of float4
   if (smem > 48 * 1024) {

@@ -13,6 +13,7 @@
 //   * FP64 phases are reduced mod 2 pi in FP64, then rotated in FP32;
 //   * the non-zero-row search is folded into the geocoding epilogue.
 #include <climits>
+#include <cstddef>
 #include <type_traits>
 #include <cuda_runtime.h>
 
@@ -82,7 +83,8 @@ __device__ __forceinline__ void tops_column(const s1b_burst_plan_t &P, int c, do
 
 // Azimuth time of line r relative to the burst centre: eta_r = -L ati / 2 +
 // r ati (geo2rdr.cu:530-531).
-__device__ __forceinline__ double deramp_eta(const s1b_burst_plan_t &P, int r) {
+template <typename PL>
+__device__ __forceinline__ double deramp_eta(const PL &P, int r) {
   return -P.lines * P.ati / 2. + i32_to_f64(r) * P.ati;
 }
 
@@ -255,43 +257,37 @@ __device__ __forceinline__ float2 load_ro(const short2 *p) {
 // height is written as zeros without solving its pixels.  Every pixel seeds
 // its Newton iteration from the line model, so its result does not depend on
 // whether the blocks before it were culled.
-template <int TX, int RY, typename TSrc = float2, bool kFused = false>
-__device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const int16_t *__restrict__ dem,
-                                             int64_t pitch, const TSrc *__restrict__ burst,
-                                             float2 *__restrict__ out, int32_t *__restrict__ rows, int nrow,
-                                             int ncol, int tile_x, int tile_y, bool cull,
-                                             const double2 *__restrict__ tops = nullptr) {
-  const int tx = threadIdx.x, lane = tx & 31;
-  const int col = tile_x * TX + tx;
-  static_assert(RY % 32 == 0, "tile rows");
-  const int row0 = tile_y * RY;
-  // llh->ECEF trigonometry (orbit.cu:20-27): lane l holds the row terms of
-  // row r + l for the current 32 rows r .. r + 31 of the tile
-  double r_sin = 0.0, r_cos = 0.0, r_re = 0.0;
-  auto row_terms = [&](int r) {
-    const double lat = (P.lat0 + (row0 + r + lane) * P.dlat) * kPiD / 180;
-    sincos(lat, &r_sin, &r_cos);
-    r_re = kRaD / sqrt(1. - kRe2D * r_sin * r_sin);
-  };
-  row_terms(0);
-  double sinlon, coslon;
-  sincos((P.lon0 + col * P.dlon) * kPiD / 180, &sinlon, &coslon);
-  const bool colok = col < ncol;
-  const double inv_dmrg = 1.0 / P.dmrg, prf = 1.0 / P.dtaz, two_over_c = 2.0 / kSolD;
-  // One cubic orbit expansion per warp, at the zero-Doppler time of the
-  // warp's centre pixel, solved on the window polynomial from the burst
-  // centre (geo2rdr.cu:588-600).  The warp's 32 x RY pixels lie within
-  // ~0.2 s of it, where the dropped fourth-order term is < 1e-9 m.  Lanes 1
-  // to 3 solve three corners at the same time; the four solutions bound the
-  // warp's footprint in the burst, whose lines are prefetched into L2 before
-  // the per-pixel solves, so the bilinear gathers hit L2, and give the line
-  // model that seeds and culls the pixel solves.
-  __shared__ ZeroDopplerPatch s_zd[TX / 32];
-  const int wid = tx >> 5;
-  // the warp's pixels span rows rT .. rB and columns cL .. cR of the window
-  const int c0 = tile_x * TX + wid * 32;
-  const int rT = row0, rB = min(row0 + RY - 1, nrow - 1), cL = min(c0, ncol - 1), cR = min(c0 + 31, ncol - 1);
-  const int rC = min(row0 + RY / 2, nrow - 1), cC = min(c0 + 16, ncol - 1);
+// Per-burst constants of the pixel loop.
+struct GeoConsts {
+  double inv_dmrg, prf, two_over_c, k4_wvl;  // k4_wvl: two-way range phase, half-cycles per metre
+};
+
+template <typename PL>
+__device__ __forceinline__ GeoConsts geo_consts(const PL &P) {
+  return GeoConsts{1.0 / P.dmrg, 1.0 / P.dtaz, 2.0 / kSolD, 4.0 / P.wvl};
+}
+
+// Per-warp setup of one burst's geocoding.  The warp's pixels lie in window
+// rows rT .. rB and columns cL .. cR (inside the window); tile row r is
+// window row row0 + r.  One cubic orbit expansion per warp, at the
+// zero-Doppler time of the warp's centre pixel, solved on the window
+// polynomial from the burst centre (geo2rdr.cu:588-600).  The warp's 32 x RY
+// pixels lie within ~0.2 s of it, where the dropped fourth-order term is
+// < 1e-9 m.  Lanes 1 to 3 solve three corners at the same time; the four
+// solutions bound the warp's footprint in the burst, whose lines are
+// prefetched into L2 before the per-pixel solves, so the bilinear gathers
+// hit L2, and give the line model that seeds and culls the pixel solves.
+// Lane 0 writes the patch to zd and the seed model to seed; the result has
+// bit j set when block j of 32 tile rows is culled.
+template <int RY, typename TSrc, typename PL>
+__device__ __forceinline__ unsigned geo_warp_setup(const PL &P, const s1b_orbit_poly_t &orbit,
+                                                   const int16_t *__restrict__ dem, int64_t pitch,
+                                                   const TSrc *__restrict__ burst, int row0, int rT,
+                                                   int rB, int cL, int cR, bool cull, ZeroDopplerPatch &zd,
+                                                   double4 &seed) {
+  const int lane = threadIdx.x & 31;
+  const double inv_dmrg = 1.0 / P.dmrg, prf = 1.0 / P.dtaz;
+  const int rC = min(rT + RY / 2, rB), cC = min(cL + 16, cR);
   double faz = 0.0, frg = 0.0, zl = 0.0, kl = 0.0;
   bool conv = true;
   if (lane < 4) {
@@ -312,7 +308,7 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
       st.a[i] = P.amid[i];
     }
     double tc = P.tmid, drc[3];
-    conv = zero_doppler(P.orbit, pc, tc, st, drc) < 51;
+    conv = zero_doppler(orbit, pc, tc, st, drc) < 51;
     faz = (tc - P.tstart) * prf;
     frg = (sqrt(drc[0] * drc[0] + drc[1] * drc[1] + drc[2] * drc[2]) - P.rngstart) * inv_dmrg;
     // lines per metre of height: the zero-Doppler condition (p - X).V = 0
@@ -330,8 +326,8 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
     zl = faz - kl * hc;  // the point's line at zero height
     if (lane == 0) {
       OrbitCubic oc;
-      orbit_cubic(P.orbit, tc, oc);
-      zero_doppler_patch(oc, s_zd[wid]);
+      orbit_cubic(orbit, tc, oc);
+      zero_doppler_patch(oc, zd);
     }
   }
   {
@@ -370,39 +366,150 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
   // from the model measures its curvature; the cull margin covers four times
   // that, the heights (-32768 .. 32767 m, the slope with a quarter to spare
   // for its change over the warp and with height) and 2 lines.
-  // The seed model goes to shared memory as times from the centre's:
-  // h = s.x + s.y col + s.z r + s.w hgt; bit j of cullmask marks block j culled.
-  __shared__ double4 s_seed[TX / 32];
-  const int rmax = min(RY, nrow - row0);
+  // The seed model, as times from the centre's, in tile rows:
+  // h = s.x + s.y col + s.z r + s.w hgt.
   unsigned cullmask = 0;
-  {
-    const double zTL = __shfl_sync(0xffffffffu, zl, 1), zBR = __shfl_sync(0xffffffffu, zl, 2);
-    const double zTR = __shfl_sync(0xffffffffu, zl, 3), zC = __shfl_sync(0xffffffffu, zl, 0);
-    const double kC = __shfl_sync(0xffffffffu, kl, 0), fazC = __shfl_sync(0xffffffffu, faz, 0);
-    const double zr = rB > rT ? (zBR - zTR) * rcp_newton(rB - rT) : 0.0;
-    const double zc = cR > cL ? (zTR - zTL) * rcp_newton(cR - cL) : 0.0;
-    const double kmax = fmax(fmax(fabs(kC), fabs(__shfl_sync(0xffffffffu, kl, 1))),
-                             fmax(fabs(__shfl_sync(0xffffffffu, kl, 2)), fabs(__shfl_sync(0xffffffffu, kl, 3))));
-    const double resid = fabs(zC - (zTL + zr * (rC - rT) + zc * (cC - cL)));
-    const double slack = 2.0 + 4.0 * resid + 1.25 * 32768.0 * kmax;
-    // every corner converged and the model is sound (NaN fails each test)
-    if (__all_sync(0xffffffffu, conv) && cull && resid < 1.0 && slack < 1.0e4) {
-      const double zcs = zc * (cR - cL);  // the model's change across the warp's columns
+  const double zTL = __shfl_sync(0xffffffffu, zl, 1), zBR = __shfl_sync(0xffffffffu, zl, 2);
+  const double zTR = __shfl_sync(0xffffffffu, zl, 3), zC = __shfl_sync(0xffffffffu, zl, 0);
+  const double kC = __shfl_sync(0xffffffffu, kl, 0), fazC = __shfl_sync(0xffffffffu, faz, 0);
+  const double zr = rB > rT ? (zBR - zTR) * rcp_newton(rB - rT) : 0.0;
+  const double zc = cR > cL ? (zTR - zTL) * rcp_newton(cR - cL) : 0.0;
+  const double kmax = fmax(fmax(fabs(kC), fabs(__shfl_sync(0xffffffffu, kl, 1))),
+                           fmax(fabs(__shfl_sync(0xffffffffu, kl, 2)), fabs(__shfl_sync(0xffffffffu, kl, 3))));
+  const double resid = fabs(zC - (zTL + zr * (rC - rT) + zc * (cC - cL)));
+  const double slack = 2.0 + 4.0 * resid + 1.25 * 32768.0 * kmax;
+  const int rTr = rT - row0, rBr = rB - row0;  // tile rows of the warp's first and last rows
+  // every corner converged and the model is sound (NaN fails each test)
+  if (__all_sync(0xffffffffu, conv) && cull && resid < 1.0 && slack < 1.0e4) {
+    const double zcs = zc * (cR - cL);  // the model's change across the warp's columns
 #pragma unroll
-      for (int j = 0; j < RY / 32; ++j) {
-        const int rb = 32 * j, rend = min(rb + 32, rmax);
-        const double za = zTL + zr * rb, zb = zTL + zr * (rend - 1);
-        const double lo = fmin(za, zb) + fmin(zcs, 0.0) - slack, hi = fmax(za, zb) + fmax(zcs, 0.0) + slack;
-        if (rb < rmax && (hi < P.first_valid_line + 5 || lo >= P.last_valid_line - 5)) cullmask |= 1u << j;
-      }
+    for (int j = 0; j < RY / 32; ++j) {
+      const int ra = max(32 * j, rTr), re = min(32 * j + 32, rBr + 1);
+      const double za = zTL + zr * (ra - rTr), zb = zTL + zr * (re - 1 - rTr);
+      const double lo = fmin(za, zb) + fmin(zcs, 0.0) - slack, hi = fmax(za, zb) + fmax(zcs, 0.0) + slack;
+      if (ra < re && (hi < P.first_valid_line + 5 || lo >= P.last_valid_line - 5)) cullmask |= 1u << j;
     }
-    if (lane == 0)
-      s_seed[wid] = make_double4((zTL - zc * cL - fazC) * P.dtaz, zc * P.dtaz, zr * P.dtaz, kC * P.dtaz);
   }
+  if (lane == 0)
+    seed = make_double4((zTL - zr * rTr - zc * cL - fazC) * P.dtaz, zc * P.dtaz, zr * P.dtaz, kC * P.dtaz);
+  return cullmask;
+}
+
+// One pixel of a burst's geocoding: ECEF point p of height hgt, tile row r,
+// window column col.  `first` takes the chord slope of this point for the
+// block (f' changes by < 1e-3 over 32 rows); every point starts from the
+// warp's line model m, within ~1e-6 s of its root.  Returns the geocoded
+// sample, 0 outside the validity window.
+template <typename TSrc, bool kFused, typename PL>
+__device__ __forceinline__ float2 geo_pixel(const PL &P, const GeoConsts &gc,
+                                            const ZeroDopplerPatch &zd, const double4 &m, const double p[3],
+                                            double hgt, int r, int col, bool first, double &inv_c1,
+                                            const TSrc *__restrict__ burst, const double2 *__restrict__ tops) {
+  float2 res = make_float2(0.f, 0.f);
+  const ZeroDopplerPoint q = zero_doppler_point(zd, p);
+  if (first) inv_c1 = rcp_newton(q.c1);
+  double h = fma(m.w, hgt, fma(m.z, i32_to_f64(r), fma(m.y, i32_to_f64(col), m.x)));
+  const double rng = sqrt_heron(zero_doppler_solve(q, zd.c3, inv_c1, h));
+  const double t = zd.t0 + h;
+  const double rgoff = (rng - P.rngstart) * gc.inv_dmrg;
+  const double azoff = (t - P.tstart) * gc.prf;
+  // validity window, geo2rdr.cu:208-209
+  bool valid = rgoff > P.first_valid_sample && rgoff < P.last_valid_sample - 1 &&
+               azoff >= P.first_valid_line + 5 && azoff < P.last_valid_line - 5;
+  const int intr = (int)rgoff, inta = (int)azoff;
+  // the 2x2 neighbourhood must lie inside the burst even if the validity
+  // limits passed in exceed the raster
+  valid = valid && intr >= 0 && intr + 1 < P.samples && inta >= 0 && inta + 1 < P.lines;
+  if (valid) {
+    const double eta = -P.lines * P.dtaz / 2. + t - P.tstart;
+    const double frd = rgoff - i32_to_f64(intr);
+    // bilinear interpolation of the deramped burst (geo2rdr.cu:220-237)
+    const float fr = (float)frd, fa = (float)(azoff - i32_to_f64(inta));
+    const size_t i1 = (size_t)inta * P.samples + intr;
+    if constexpr (kFused) {
+      // the samples' deramp phases -kt (eta_line - etaref)^2 and the
+      // reramp + range phase (geo2rdr.cu:210-219, 238-243) in half-cycles
+      const double2 t0 = __ldg(tops + intr), t1 = __ldg(tops + intr + 1);
+      const double ed = eta - fma(frd, t1.y - t0.y, t0.y);
+      const double hr = fma(-fma(frd, t1.x - t0.x, t0.x), ed * ed, gc.k4_wvl * rng);
+      const double ea = deramp_eta(P, inta), eb = deramp_eta(P, inta + 1);
+      double d0 = ea - t0.y, d1 = ea - t1.y;
+      const double qa0 = t0.x * d0 * d0, qa1 = t1.x * d1 * d1;
+      d0 = eb - t0.y;
+      d1 = eb - t1.y;
+      const double qb0 = t0.x * d0 * d0, qb1 = t1.x * d1 * d1;
+      const float2 s2 = cmul(load_ro(burst + i1 + 1), rotation_pi(qa1 - qa0));
+      const float2 s4 = cmul(load_ro(burst + i1 + P.samples + 1), rotation_pi(qb1 - qb0));
+      const float2 ca = cmul(lerp2(load_ro(burst + i1), s2, fr), phasor_pi(hr + qa0));
+      const float2 cb = cmul(lerp2(load_ro(burst + i1 + P.samples), s4, fr), phasor_pi(hr + qb0));
+      res = lerp2(ca, cb, fa);
+    } else {
+      // per-pixel TOPS reramp (geo2rdr.cu:210-219); kt = ka ks / (ka - ks)
+      // and etac = -fnc / ka share one reciprocal of ka (ka - ks)
+      const double tr = rng * gc.two_over_c;
+      double dt = tr - P.fm[0];
+      const double ka = P.fm[1] + dt * (P.fm[2] + P.fm[3] * dt);
+      dt = tr - P.dc[0];
+      const double fnc = P.dc[1] + dt * (P.dc[2] + P.dc[3] * dt);
+      const double kmk = ka - P.ks;
+      const double inv = rcp_newton(ka * kmk);
+      const double kt = ka * P.ks * (ka * inv);
+      const double ed = eta - (-fnc * (kmk * inv) - P.etac0);
+      const float2 c1 = lerp2(__ldg(burst + i1), __ldg(burst + i1 + 1), fr);
+      const float2 c2 = lerp2(__ldg(burst + i1 + P.samples), __ldg(burst + i1 + P.samples + 1), fr);
+      // range phase and reramp (geo2rdr.cu:238-243): 4 pi rng / wvl + pi kt ed^2
+      // rad, formed in half-cycles
+      res = cmul(lerp2(c1, c2, fa), phasor_pi(fma(kt, ed * ed, gc.k4_wvl * rng)));
+    }
+  }
+  return res;
+}
+
+// ECEF point of a DEM pixel from its row terms (sin lat, cos lat, prime
+// vertical radius), column terms and height (orbit.cu:20-27).
+__device__ __forceinline__ void llh_point(double sinlat, double coslat, double re, double sinlon, double coslon,
+                                          double hgt, double p[3]) {
+  p[0] = (re + hgt) * coslat * coslon;
+  p[1] = (re + hgt) * coslat * sinlon;
+  p[2] = (re * (1 - kRe2D) + hgt) * sinlat;
+}
+
+template <int TX, int RY, typename TSrc = float2, bool kFused = false, typename PL = s1b_burst_plan_t>
+__device__ __forceinline__ void geo2rdr_tile(const PL &P, const s1b_orbit_poly_t &orbit,
+                                             const int16_t *__restrict__ dem, int64_t pitch,
+                                             const TSrc *__restrict__ burst,
+                                             float2 *__restrict__ out, int32_t *__restrict__ rows, int nrow,
+                                             int ncol, int tile_x, int tile_y, bool cull,
+                                             const double2 *__restrict__ tops = nullptr) {
+  const int tx = threadIdx.x, lane = tx & 31;
+  const int col = tile_x * TX + tx;
+  static_assert(RY % 32 == 0, "tile rows");
+  const int row0 = tile_y * RY;
+  // llh->ECEF trigonometry (orbit.cu:20-27): lane l holds the row terms of
+  // row r + l for the current 32 rows r .. r + 31 of the tile
+  double r_sin = 0.0, r_cos = 0.0, r_re = 0.0;
+  auto row_terms = [&](int r) {
+    const double lat = (P.lat0 + (row0 + r + lane) * P.dlat) * kPiD / 180;
+    sincos(lat, &r_sin, &r_cos);
+    r_re = kRaD / sqrt(1. - kRe2D * r_sin * r_sin);
+  };
+  row_terms(0);
+  double sinlon, coslon;
+  sincos((P.lon0 + col * P.dlon) * kPiD / 180, &sinlon, &coslon);
+  const bool colok = col < ncol;
+  const GeoConsts gc = geo_consts(P);
+  __shared__ ZeroDopplerPatch s_zd[TX / 32];
+  __shared__ double4 s_seed[TX / 32];
+  const int wid = tx >> 5;
+  // the warp's pixels span rows row0 .. rB and columns cL .. cR of the window
+  const int c0 = tile_x * TX + wid * 32;
+  const int rmax = min(RY, nrow - row0);
+  const unsigned cullmask = geo_warp_setup<RY>(P, orbit, dem, pitch, burst, row0, row0, row0 + rmax - 1,
+                                               min(c0, ncol - 1), min(c0 + 31, ncol - 1), cull, s_zd[wid],
+                                               s_seed[wid]);
   __syncwarp();  // lane 0's patch and seed models are visible to the warp
   const ZeroDopplerPatch &zd = s_zd[wid];
-  const double k4_wvl = 4.0 / P.wvl;  // two-way range phase, half-cycles per metre
-  double h = 0.0, inv_c1 = 0.0;
+  double inv_c1 = 0.0;
   int16_t hn = colok && rmax > 0 && !(cullmask & 1u) ? __ldg(dem + (int64_t)row0 * pitch + col) : 0;
   int rlo = INT_MAX, rhi = -1;
   for (int r = 0; r < rmax; ++r) {
@@ -418,87 +525,22 @@ __device__ __forceinline__ void geo2rdr_tile(const s1b_burst_plan_t &P, const in
       }
       if (r > 0) row_terms(r);
     }
-    {
-      const int row = row0 + r;
-      const double sinlat = __shfl_sync(0xffffffffu, r_sin, r & 31);
-      const double coslat = __shfl_sync(0xffffffffu, r_cos, r & 31);
-      const double re = __shfl_sync(0xffffffffu, r_re, r & 31);
-      const double hgt = i32_to_f64(hn);
-      if (colok && r + 1 < rmax) hn = __ldg(dem + (int64_t)(row + 1) * pitch + col);
-      float2 res = make_float2(0.f, 0.f);
-      if (colok) {
-        double p[3];
-        p[0] = (re + hgt) * coslat * coslon;
-        p[1] = (re + hgt) * coslat * sinlon;
-        p[2] = (re * (1 - kRe2D) + hgt) * sinlat;
-        const ZeroDopplerPoint q = zero_doppler_point(zd, p);
-        // the chord slope of the block's first point serves the block (f'
-        // changes by < 1e-3 over 32 rows); every point starts from the line
-        // model, within ~1e-6 s of its root
-        if ((r & 31) == 0) inv_c1 = rcp_newton(q.c1);
-        {
-          const double4 m = s_seed[wid];
-          h = fma(m.w, hgt, fma(m.z, i32_to_f64(r), fma(m.y, i32_to_f64(col), m.x)));
-        }
-        const double rng = sqrt_heron(zero_doppler_solve(q, zd.c3, inv_c1, h));
-        const double t = zd.t0 + h;
-        const double rgoff = (rng - P.rngstart) * inv_dmrg;
-        const double azoff = (t - P.tstart) * prf;
-        // validity window, geo2rdr.cu:208-209
-        bool valid = rgoff > P.first_valid_sample && rgoff < P.last_valid_sample - 1 &&
-                     azoff >= P.first_valid_line + 5 && azoff < P.last_valid_line - 5;
-        const int intr = (int)rgoff, inta = (int)azoff;
-        // the 2x2 neighbourhood must lie inside the burst even if the validity
-        // limits passed in exceed the raster
-        valid = valid && intr >= 0 && intr + 1 < P.samples && inta >= 0 && inta + 1 < P.lines;
-        if (valid) {
-          const double eta = -P.lines * P.dtaz / 2. + t - P.tstart;
-          const double frd = rgoff - i32_to_f64(intr);
-          // bilinear interpolation of the deramped burst (geo2rdr.cu:220-237)
-          const float fr = (float)frd, fa = (float)(azoff - i32_to_f64(inta));
-          const size_t i1 = (size_t)inta * P.samples + intr;
-          if constexpr (kFused) {
-            // the samples' deramp phases -kt (eta_line - etaref)^2 and the
-            // reramp + range phase (geo2rdr.cu:210-219, 238-243) in half-cycles
-            const double2 t0 = __ldg(tops + intr), t1 = __ldg(tops + intr + 1);
-            const double ed = eta - fma(frd, t1.y - t0.y, t0.y);
-            const double hr = fma(-fma(frd, t1.x - t0.x, t0.x), ed * ed, k4_wvl * rng);
-            const double ea = deramp_eta(P, inta), eb = deramp_eta(P, inta + 1);
-            double d0 = ea - t0.y, d1 = ea - t1.y;
-            const double qa0 = t0.x * d0 * d0, qa1 = t1.x * d1 * d1;
-            d0 = eb - t0.y;
-            d1 = eb - t1.y;
-            const double qb0 = t0.x * d0 * d0, qb1 = t1.x * d1 * d1;
-            const float2 s2 = cmul(load_ro(burst + i1 + 1), rotation_pi(qa1 - qa0));
-            const float2 s4 = cmul(load_ro(burst + i1 + P.samples + 1), rotation_pi(qb1 - qb0));
-            const float2 ca = cmul(lerp2(load_ro(burst + i1), s2, fr), phasor_pi(hr + qa0));
-            const float2 cb = cmul(lerp2(load_ro(burst + i1 + P.samples), s4, fr), phasor_pi(hr + qb0));
-            res = lerp2(ca, cb, fa);
-          } else {
-            // per-pixel TOPS reramp (geo2rdr.cu:210-219); kt = ka ks / (ka - ks)
-            // and etac = -fnc / ka share one reciprocal of ka (ka - ks)
-            const double tr = rng * two_over_c;
-            double dt = tr - P.fm[0];
-            const double ka = P.fm[1] + dt * (P.fm[2] + P.fm[3] * dt);
-            dt = tr - P.dc[0];
-            const double fnc = P.dc[1] + dt * (P.dc[2] + P.dc[3] * dt);
-            const double kmk = ka - P.ks;
-            const double inv = rcp_newton(ka * kmk);
-            const double kt = ka * P.ks * (ka * inv);
-            const double ed = eta - (-fnc * (kmk * inv) - P.etac0);
-            const float2 c1 = lerp2(__ldg(burst + i1), __ldg(burst + i1 + 1), fr);
-            const float2 c2 = lerp2(__ldg(burst + i1 + P.samples), __ldg(burst + i1 + P.samples + 1), fr);
-            // range phase and reramp (geo2rdr.cu:238-243): 4 pi rng / wvl + pi kt ed^2
-            // rad, formed in half-cycles
-            res = cmul(lerp2(c1, c2, fa), phasor_pi(fma(kt, ed * ed, k4_wvl * rng)));
-          }
-        }
-        __stcs(out + (size_t)row * ncol + col, res);
-      }
-      if (res.x != 0.f || res.y != 0.f) {
-        rlo = min(rlo, row);
-        rhi = row + 1;
-      }
+    const int row = row0 + r;
+    const double sinlat = __shfl_sync(0xffffffffu, r_sin, r & 31);
+    const double coslat = __shfl_sync(0xffffffffu, r_cos, r & 31);
+    const double re = __shfl_sync(0xffffffffu, r_re, r & 31);
+    const double hgt = i32_to_f64(hn);
+    if (colok && r + 1 < rmax) hn = __ldg(dem + (int64_t)(row + 1) * pitch + col);
+    float2 res = make_float2(0.f, 0.f);
+    if (colok) {
+      double p[3];
+      llh_point(sinlat, coslat, re, sinlon, coslon, hgt, p);
+      res = geo_pixel<TSrc, kFused>(P, gc, zd, s_seed[wid], p, hgt, r, col, (r & 31) == 0, inv_c1, burst, tops);
+      __stcs(out + (size_t)row * ncol + col, res);
+    }
+    if (res.x != 0.f || res.y != 0.f) {
+      rlo = min(rlo, row);
+      rhi = row + 1;
     }
   }
   // first / last non-zero output row (geo2rdr.cu:86-128): the warp's extent
@@ -519,7 +561,7 @@ __global__ __launch_bounds__(G_TX) void geo2rdr_kernel(
     const __grid_constant__ s1b_burst_plan_t P, const int16_t *__restrict__ dem, int64_t pitch,
     const float2 *__restrict__ burst, float2 *__restrict__ out, int32_t *__restrict__ rows,
     int nrow, int ncol, bool cull) {
-  geo2rdr_tile<G_TX, G_RY>(P, dem, pitch, burst, out, rows, nrow, ncol, blockIdx.x, blockIdx.y, cull);
+  geo2rdr_tile<G_TX, G_RY>(P, P.orbit, dem, pitch, burst, out, rows, nrow, ncol, blockIdx.x, blockIdx.y, cull);
 }
 
 // ------------------------------------------------------------ frame stages
@@ -548,15 +590,43 @@ __device__ __forceinline__ int frame_burst_of(const FrameDev &d, int64_t idx) {
   return lo;
 }
 
-// The plan table is an array of 8-byte-aligned structs whose size is a
-// multiple of 8 but not of 16: copy in 8-byte words.
-static_assert(sizeof(s1b_burst_plan_t) % 8 == 0 && alignof(s1b_burst_plan_t) == 8, "plan layout");
+// The scalar part of a burst plan, everything after its orbit polynomials,
+// laid out as in s1b_burst_plan_t.  The frame's geocoding CTAs copy only
+// this part to shared memory (0.34 KB instead of 12.5 KB), which leaves the
+// SM's L1 to the bilinear gathers; the orbit polynomials, read only by the
+// per-warp setup, stay in global memory.
+struct PlanTail {
+  int32_t lines, samples;
+  int32_t first_valid_line, last_valid_line, first_valid_sample, last_valid_sample;
+  int32_t win_left, win_top, win_right, win_bottom;
+  int32_t rsc_nlat, rsc_nlon;
+  double tstart, dtaz, ati;
+  double rngstart, dmrg;
+  double slant_range_time, range_sampling_rate;
+  double wvl, k4pi_wvl;
+  double tmid, xmid[3], vmid[3], amid[3];
+  double ks, etac0;
+  double fm[4];
+  double dc[4];
+  double lat0, lon0, dlat, dlon;
+  double latlon_box[4];
+};
+#define S1B_TAIL_AT(f) (offsetof(s1b_burst_plan_t, f) - offsetof(s1b_burst_plan_t, lines) == offsetof(PlanTail, f))
+static_assert(offsetof(s1b_burst_plan_t, lines) == sizeof(s1b_orbit_poly_t) &&
+                  sizeof(s1b_burst_plan_t) - sizeof(s1b_orbit_poly_t) == sizeof(PlanTail) && S1B_TAIL_AT(tstart) &&
+                  S1B_TAIL_AT(tmid) && S1B_TAIL_AT(fm) && S1B_TAIL_AT(lat0) && S1B_TAIL_AT(latlon_box),
+              "plan tail layout");
+#undef S1B_TAIL_AT
+// The plan table is an array of 8-byte-aligned structs: copy in 8-byte words.
+static_assert(sizeof(s1b_burst_plan_t) % 8 == 0 && alignof(s1b_burst_plan_t) == 8 &&
+                  sizeof(s1b_orbit_poly_t) % 8 == 0, "plan layout");
 
-__device__ __forceinline__ void frame_load_plan(s1b_burst_plan_t &sp, const s1b_burst_plan_t *src) {
+__device__ __forceinline__ void frame_load_plan(PlanTail &sp, const s1b_burst_plan_t *src) {
   __syncthreads();  // every thread is done with the previous burst's plan
-  const long long *s = reinterpret_cast<const long long *>(src);
+  const long long *s = reinterpret_cast<const long long *>(reinterpret_cast<const char *>(src) +
+                                                           sizeof(s1b_orbit_poly_t));
   long long *d = reinterpret_cast<long long *>(&sp);
-  for (int i = threadIdx.x; i < (int)(sizeof(s1b_burst_plan_t) / 8); i += blockDim.x) d[i] = s[i];
+  for (int i = threadIdx.x; i < (int)(sizeof(PlanTail) / 8); i += blockDim.x) d[i] = s[i];
   __syncthreads();
 }
 
@@ -617,16 +687,18 @@ void launch_deramp_grid(const FrameDev &d, const FrameIO &io, int rows, const in
 // One tile of the frame's geocoding: unfused from the burst's deramped copy,
 // fused from its raw samples and its column table (both at der_off).
 template <int TX, typename TSrc, bool kFused>
-__device__ __forceinline__ void frame_geo_tile(const s1b_burst_plan_t &sp, const FrameBurst &fb, const FrameIO &io,
-                                               int32_t *rows, int tx, int ty, bool cull) {
+__device__ __forceinline__ void frame_geo_tile(const PlanTail &sp, const s1b_orbit_poly_t &orbit,
+                                               const FrameBurst &fb, const FrameIO &io, int32_t *rows, int tx, int ty,
+                                               bool cull) {
   const int16_t *dem = io.dem + (int64_t)sp.win_top * io.dem_pitch + sp.win_left;
   if constexpr (kFused)
-    geo2rdr_tile<TX, kFrameGeoRows, TSrc, true>(sp, dem, io.dem_pitch, static_cast<const TSrc *>(io.slc) + fb.slc_off,
-                                                io.work + fb.geo_off, rows, fb.nrow, fb.ncol, tx, ty, cull,
+    geo2rdr_tile<TX, kFrameGeoRows, TSrc, true>(sp, orbit, dem, io.dem_pitch,
+                                                static_cast<const TSrc *>(io.slc) + fb.slc_off, io.work + fb.geo_off,
+                                                rows, fb.nrow, fb.ncol, tx, ty, cull,
                                                 reinterpret_cast<const double2 *>(io.work + fb.der_off));
   else
-    geo2rdr_tile<TX, kFrameGeoRows>(sp, dem, io.dem_pitch, io.work + fb.der_off, io.work + fb.geo_off, rows, fb.nrow,
-                                    fb.ncol, tx, ty, cull);
+    geo2rdr_tile<TX, kFrameGeoRows>(sp, orbit, dem, io.dem_pitch, io.work + fb.der_off, io.work + fb.geo_off, rows,
+                                    fb.nrow, fb.ncol, tx, ty, cull);
 }
 
 // Per-column TOPS coefficients (-kt, etaref) of every burst for the fused
@@ -649,7 +721,7 @@ constexpr int kGeoGridMinBlocks = TX == 256 ? 4 : 896 / TX;
 
 template <int TX, typename TSrc, bool kFused>
 __global__ __launch_bounds__(TX, kGeoGridMinBlocks<TX>) void frame_geo2rdr_kernel(const FrameDev d, const FrameIO io) {
-  __shared__ __align__(16) s1b_burst_plan_t sp;
+  __shared__ __align__(16) PlanTail sp;
   int cur = -1;
   for (int64_t idx = blockIdx.x; idx < d.n_geo_tiles; idx += gridDim.x) {
     const int b = frame_burst_of<true>(d, idx);
@@ -661,12 +733,12 @@ __global__ __launch_bounds__(TX, kGeoGridMinBlocks<TX>) void frame_geo2rdr_kerne
     const int tiles_x = (fb.ncol + TX - 1) / TX;
     const int64_t local = idx - fb.geo_tile0;
     const int ty = (int)(local / tiles_x), tx = (int)(local - (int64_t)ty * tiles_x);
-    frame_geo_tile<TX, TSrc, kFused>(sp, fb, io, d.rows + 2 * b, tx, ty, d.cull_geo != 0);
+    frame_geo_tile<TX, TSrc, kFused>(sp, d.plans[b].orbit, fb, io, d.rows + 2 * b, tx, ty, d.cull_geo != 0);
   }
 }
 
 // One CTA per tile: blockIdx.z is the burst, (x, y) the tile in its DEM
-// window.  The CTA copies its burst's plan (12.5 KB) to shared memory first:
+// window.  The CTA copies its burst's plan scalars to shared memory first:
 // the pixel loop's plan scalars then come from shared memory rather than
 // uniform global loads (measured 13.67 -> 13.28 ms per 27-pair frame).  The
 // grid spans the largest window; CTAs past a smaller one return before the
@@ -676,12 +748,186 @@ __global__ __launch_bounds__(TX, kGeoGridMinBlocks<TX>) void frame_geo2rdr_kerne
 // 9.32 -> 8.91 ms at TX 256 against 80 registers.
 template <int TX, typename TSrc, bool kFused>
 __global__ __launch_bounds__(TX, kGeoGridMinBlocks<TX>) void frame_geo2rdr_grid_kernel(const FrameDev d, const FrameIO io) {
-  __shared__ __align__(16) s1b_burst_plan_t sp;
+  __shared__ __align__(16) PlanTail sp;
   const int b = blockIdx.z;
   const FrameBurst &fb = d.bursts[b];
   if ((int)blockIdx.x * TX >= fb.ncol || (int)blockIdx.y * kFrameGeoRows >= fb.nrow) return;
   frame_load_plan(sp, d.plans + b);
-  frame_geo_tile<TX, TSrc, kFused>(sp, fb, io, d.rows + 2 * b, blockIdx.x, blockIdx.y, d.cull_geo != 0);
+  frame_geo_tile<TX, TSrc, kFused>(sp, d.plans[b].orbit, fb, io, d.rows + 2 * b, blockIdx.x, blockIdx.y,
+                                   d.cull_geo != 0);
+}
+
+// Crossmul fused into the geocoding.  One CTA per tile of a pair's grid of
+// look rows (blockIdx.z = pair) geocodes both bursts of the pair at every
+// DEM pixel of the union of their windows -- the DEM height, the ECEF point
+// and the row and column terms serve both -- and sums conj(ref) sec and the
+// two powers down each column over `rowlook` rows (xm_accumulate, in the
+// order crossmul_rows_tile sums them): one float4 per column and look row.
+// The geocoded windows are never written; the crop rows are voted as the
+// geocoding does.  A burst is zero outside its window, as the reference's
+// crossmul reads a .gslc (zero-filled around its crop).  Tiles hold whole
+// look rows, so no look row spans two CTAs and the sums need no atomics.
+constexpr int kXmTX = kFrameXmCols;  // columns per tile
+
+template <typename TSrc, bool kFused>
+__global__ __launch_bounds__(kXmTX, 5) void frame_geo_xmul_kernel(const FrameDev d, const FrameIO io) {
+  constexpr int RY = kFrameGeoRows;
+  __shared__ __align__(16) PlanTail sp[2];
+  __shared__ ZeroDopplerPatch s_zd[2][kXmTX / 32];
+  __shared__ double4 s_seed[2][kXmTX / 32];
+  __shared__ GeoConsts s_gc[2];
+  const FramePair pr = d.pairs[blockIdx.z];
+  const int lrows = RY / d.rowlook;  // look rows per tile
+  if ((int)blockIdx.x * kXmTX >= pr.part_cols || (int)blockIdx.y * lrows >= pr.part_rows) return;  // uniform
+  {
+    const long long *a = reinterpret_cast<const long long *>(&d.plans[pr.ref].lines);
+    const long long *b = reinterpret_cast<const long long *>(&d.plans[pr.sec].lines);
+    long long *ta = reinterpret_cast<long long *>(&sp[0]), *tb = reinterpret_cast<long long *>(&sp[1]);
+    for (int i = threadIdx.x; i < (int)(sizeof(PlanTail) / 8); i += blockDim.x) {
+      ta[i] = a[i];
+      tb[i] = b[i];
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) s_gc[threadIdx.x] = geo_consts(sp[threadIdx.x]);
+    __syncthreads();
+  }
+  const int tx = threadIdx.x, lane = tx & 31, wid = tx >> 5;
+  const int R0 = pr.part_top + (int)blockIdx.y * lrows * d.rowlook;  // RSC row of tile row 0
+  const int nr = min(lrows, pr.part_rows - (int)blockIdx.y * lrows) * d.rowlook;
+  const int Cw = pr.part_left + (int)blockIdx.x * kXmTX + wid * 32;  // RSC column of the warp's lane 0
+  const int C = Cw + lane;
+  const bool colin = C < pr.part_left + pr.part_cols;
+  // row and column terms on the RSC grid (the reference burst's plan)
+  const PlanTail &P0 = sp[0];
+  double r_sin = 0.0, r_cos = 0.0, r_re = 0.0;
+  auto row_terms = [&](int r) {
+    const double lat = (P0.lat0 + (R0 - P0.win_top + r + lane) * P0.dlat) * kPiD / 180;
+    sincos(lat, &r_sin, &r_cos);
+    r_re = kRaD / sqrt(1. - kRe2D * r_sin * r_sin);
+  };
+  double sinlon, coslon;
+  sincos((P0.lon0 + (C - P0.win_left) * P0.dlon) * kPiD / 180, &sinlon, &coslon);
+  // per burst: window row of tile row 0, window column of the thread, block masks
+  int row0w[2], colw[2], nrw[2];
+  unsigned off[2];  // bit j: block j of 32 rows culled or outside the window
+  int rlim = 0;     // tile rows below rlim lie inside the hull of the two windows
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const PlanTail &P = sp[q];
+    const FrameBurst &fb = d.bursts[q ? pr.sec : pr.ref];
+    row0w[q] = R0 - P.win_top;
+    colw[q] = C - P.win_left;
+    nrw[q] = fb.nrow;
+    rlim = max(rlim, min(nr, fb.nrow - row0w[q]));
+    const int c0 = Cw - P.win_left;
+    const int rT = max(row0w[q], 0), rB = min(row0w[q] + nr - 1, fb.nrow - 1);
+    const int cL = max(c0, 0), cR = min(c0 + 31, fb.ncol - 1);
+    off[q] = ~0u;
+    if (rT <= rB && cL <= cR) {  // warp-uniform
+      const int16_t *dem = io.dem + (int64_t)P.win_top * io.dem_pitch + P.win_left;
+      const TSrc *src = kFused ? static_cast<const TSrc *>(io.slc) + fb.slc_off
+                               : reinterpret_cast<const TSrc *>(io.work + fb.der_off);
+      off[q] = geo_warp_setup<RY>(P, d.plans[q ? pr.sec : pr.ref].orbit, dem, io.dem_pitch, src, row0w[q], rT, rB,
+                                  cL, cR, d.cull_geo != 0,
+                                  s_zd[q][wid], s_seed[q][wid]);
+#pragma unroll
+      for (int j = 0; j < RY / 32; ++j)
+        if (32 * j + 31 < rT - row0w[q] || 32 * j > rB - row0w[q]) off[q] |= 1u << j;
+    }
+    if (colw[q] < 0 || colw[q] >= fb.ncol) colw[q] = -1;  // the thread's column is outside this window
+  }
+  __syncwarp();  // lane 0's patch and seed models are visible to the warp
+  const TSrc *src0, *src1;
+  const double2 *tops0 = nullptr, *tops1 = nullptr;
+  {
+    const FrameBurst &f0 = d.bursts[pr.ref], &f1 = d.bursts[pr.sec];
+    if constexpr (kFused) {
+      src0 = static_cast<const TSrc *>(io.slc) + f0.slc_off;
+      src1 = static_cast<const TSrc *>(io.slc) + f1.slc_off;
+      tops0 = reinterpret_cast<const double2 *>(io.work + f0.der_off);
+      tops1 = reinterpret_cast<const double2 *>(io.work + f1.der_off);
+    } else {
+      src0 = reinterpret_cast<const TSrc *>(io.work + f0.der_off);
+      src1 = reinterpret_cast<const TSrc *>(io.work + f1.der_off);
+    }
+  }
+  const int16_t *demc = io.dem + (int64_t)R0 * io.dem_pitch + C;  // the thread's column at tile row 0
+  float4 *part = reinterpret_cast<float4 *>(io.work + pr.part_off) +
+                 (int64_t)blockIdx.y * lrows * pr.part_cols + (C - pr.part_left);
+  double inv_c1a = 0.0, inv_c1b = 0.0;
+  float ir = 0.f, ii = 0.f, p1 = 0.f, p2 = 0.f;
+  int lr = 0;  // rows summed into the current look row
+  int rlo0 = INT_MAX, rhi0 = -1, rlo1 = INT_MAX, rhi1 = -1;
+  for (int rb = 0; rb < nr; rb += 32) {
+    const int rend = min(rb + 32, nr), j = rb >> 5;
+    const bool on0 = !((off[0] >> j) & 1u), on1 = !((off[1] >> j) & 1u);  // warp-uniform
+    if (on0 || on1) {
+      row_terms(rb);
+      bool first0 = true, first1 = true;
+      int16_t hn = colin && rb < rlim ? __ldg(demc + (int64_t)rb * io.dem_pitch) : 0;
+      for (int r = rb; r < rend; ++r) {
+        const double sinlat = __shfl_sync(0xffffffffu, r_sin, r & 31);
+        const double coslat = __shfl_sync(0xffffffffu, r_cos, r & 31);
+        const double re = __shfl_sync(0xffffffffu, r_re, r & 31);
+        const double hgt = i32_to_f64(hn);
+        if (colin && r + 1 < rend && r + 1 < rlim) hn = __ldg(demc + (int64_t)(r + 1) * io.dem_pitch);
+        double p[3];
+        llh_point(sinlat, coslat, re, sinlon, coslon, hgt, p);
+        float2 v0 = make_float2(0.f, 0.f), v1 = make_float2(0.f, 0.f);
+        const int w0 = row0w[0] + r, w1 = row0w[1] + r;
+        if (on0 && colw[0] >= 0 && w0 >= 0 && w0 < nrw[0]) {
+          v0 = geo_pixel<TSrc, kFused>(sp[0], s_gc[0], s_zd[0][wid], s_seed[0][wid], p, hgt, r, colw[0], first0,
+                                       inv_c1a, src0, tops0);
+          first0 = false;
+          if (v0.x != 0.f || v0.y != 0.f) {
+            rlo0 = min(rlo0, w0);
+            rhi0 = w0 + 1;
+          }
+        }
+        if (on1 && colw[1] >= 0 && w1 >= 0 && w1 < nrw[1]) {
+          v1 = geo_pixel<TSrc, kFused>(sp[1], s_gc[1], s_zd[1][wid], s_seed[1][wid], p, hgt, r, colw[1], first1,
+                                       inv_c1b, src1, tops1);
+          first1 = false;
+          if (v1.x != 0.f || v1.y != 0.f) {
+            rlo1 = min(rlo1, w1);
+            rhi1 = w1 + 1;
+          }
+        }
+        xm_accumulate(v0, v1, ir, ii, p1, p2);
+        if (++lr == d.rowlook) {
+          if (colin) __stcs(part, make_float4(ir, ii, p1, p2));
+          part += pr.part_cols;
+          ir = ii = p1 = p2 = 0.f;
+          lr = 0;
+        }
+      }
+    } else {
+      // neither burst has a pixel to solve here: their samples are zero
+      for (int r = rb; r < rend; ++r) {
+        if (++lr == d.rowlook) {
+          if (colin) __stcs(part, make_float4(ir, ii, p1, p2));
+          part += pr.part_cols;
+          ir = ii = p1 = p2 = 0.f;
+          lr = 0;
+        }
+      }
+    }
+  }
+  // crop rows of both windows (geo2rdr.cu:86-128), one reduction pair per warp
+  rlo0 = __reduce_min_sync(0xffffffffu, rlo0);
+  rhi0 = __reduce_max_sync(0xffffffffu, rhi0);
+  rlo1 = __reduce_min_sync(0xffffffffu, rlo1);
+  rhi1 = __reduce_max_sync(0xffffffffu, rhi1);
+  if (lane == 0) {
+    if (rhi0 >= 0) {
+      atomicMin(d.rows + 2 * pr.ref, rlo0);
+      atomicMax(d.rows + 2 * pr.ref + 1, rhi0);
+    }
+    if (rhi1 >= 0) {
+      atomicMin(d.rows + 2 * pr.sec, rlo1);
+      atomicMax(d.rows + 2 * pr.sec + 1, rhi1);
+    }
+  }
 }
 
 template <typename K>
@@ -968,9 +1214,23 @@ int launch_geo(const FrameDev &d, const FrameIO &io, int cols, int ctas, cudaStr
   return s1b_launch_status();
 }
 
+template <typename TSrc, bool kFused>
+int launch_geo_xmul(const FrameDev &d, const FrameIO &io, cudaStream_t st) {
+  if (d.xm_tiles_x <= 0 || d.xm_tiles_y <= 0) return S1B_OK;
+  if (d.xm_tiles_y > 65535 || d.n_pairs > 65535) return s1b_fail(S1B_ERR_TOO_LARGE, "frame geo2rdr: grid too large");
+  frame_geo_xmul_kernel<TSrc, kFused>
+      <<<dim3((unsigned)d.xm_tiles_x, (unsigned)d.xm_tiles_y, (unsigned)d.n_pairs), kXmTX, 0, st>>>(d, io);
+  return s1b_launch_status();
+}
+
 int frame_launch_geo2rdr(const FrameDev &dev, const FrameIO &io, int cols, int ctas, cudaStream_t st) {
   FrameDev d = dev;
   d.cull_geo = g_cull_geo;
+  if (d.fused_xmul) {  // crossmul look-row sums instead of geocoded windows (tile shape fixed)
+    if (!d.fused_deramp) return launch_geo_xmul<float2, false>(d, io, st);
+    return d.sample_format == S1B_SAMPLES_CI16 ? launch_geo_xmul<short2, true>(d, io, st)
+                                               : launch_geo_xmul<float2, true>(d, io, st);
+  }
   if (!d.fused_deramp) return launch_geo<float2, false>(d, io, cols, ctas, st);
   return d.sample_format == S1B_SAMPLES_CI16 ? launch_geo<short2, true>(d, io, cols, ctas, st)
                                              : launch_geo<float2, true>(d, io, cols, ctas, st);

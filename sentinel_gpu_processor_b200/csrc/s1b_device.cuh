@@ -300,4 +300,14 @@ __device__ __forceinline__ void zero_doppler_cubic_chord(const OrbitCubic &o, co
   }
 }
 
+// One full-resolution pixel pair into the multilook sums of crossmul:
+// conj(r) * s (sario.cu:207-208) and both powers, each added in one
+// expression so that every kernel summing them rounds alike.
+__device__ __forceinline__ void xm_accumulate(float2 r, float2 s, float &ir, float &ii, float &p1, float &p2) {
+  ir += r.x * s.x + r.y * s.y;
+  ii += -r.y * s.x + r.x * s.y;
+  p1 += r.x * r.x + r.y * r.y;
+  p2 += s.x * s.x + s.y * s.y;
+}
+
 #endif

@@ -27,6 +27,12 @@ struct FramePair {
   int32_t max_nrow_ml, max_ncol_ml;  // slot capacity (multilooked pixels)
   int64_t ml_off;                    // first element of its slot in every product array
   int64_t scratch_off;               // Goldstein patches, complex64 elements into the workspace
+  // Look-row sums of the crossmul fused into the geocoding: one float4 per
+  // column and look row over the union of the two DEM windows, rows aligned
+  // to the looks on the RSC grid (row part_top, column part_left first).
+  int64_t part_off;                  // complex64 elements into the workspace
+  int32_t part_top, part_left;       // RSC grid row (a multiple of rowlook) and column of element 0
+  int32_t part_rows, part_cols;      // look rows, columns
 };
 
 // Everything a frame kernel needs, passed by value.
@@ -47,6 +53,8 @@ struct FrameDev {
   int32_t sample_format;                   // S1B_SAMPLES_C64 or S1B_SAMPLES_CI16
   int32_t fused_deramp;                    // 1: geocoding deramps its gathers (column tables only)
   int32_t cull_geo;                        // 1: geocoding culls blocks outside the valid lines (set per launch)
+  int32_t fused_xmul;                      // 1: geocoding forms the crossmul look-row sums (no geocoded windows)
+  int32_t xm_tiles_x, xm_tiles_y;          // fused geocoding + crossmul tiles of the largest pair, per axis
 };
 
 // Run-time buffers of one frame launch sequence.
@@ -77,6 +85,7 @@ struct FrameBurstList {
 // Tile-space helpers shared by host and device.
 constexpr int kFrameDerampCols = 512;  // columns of a deramp tile (256 threads x 2)
 constexpr int kFrameGeoRows = 128;     // rows of a geocoding tile (column walk length)
+constexpr int kFrameXmCols = 128;      // columns of a geocoding + crossmul tile
 
 // Launchers (k_geo2rdr.cu, k_crossmul.cu, k_goldstein.cu).  `ctas` is the
 // persistent grid; 0 launches one CTA per tile over (tile x, tile y, burst).

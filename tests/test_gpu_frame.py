@@ -165,3 +165,50 @@ def test_fused_deramp_matches_deramp_kernel(cuda, frame, fmt):
         outs.append(_products(bc))
         assert bc.launches_per_step() >= 7
     _check(outs[0], outs[1], exact=False)
+
+
+@pytest.mark.parametrize("fmt", ["c64", "ci16"])
+def test_fused_crossmul_matches_crossmul_kernel(cuda, frame, fmt):
+    """The geocoding that forms the crossmul look-row sums itself (no
+    geocoded windows) against geocoded windows + the crossmul kernel: the
+    same crops, boxes and headers, products within float rounding."""
+    outs = []
+    for fused in (True, False):
+        bc = BatchedFrameChain(frame.ref, frame.sec, frame.rsc, frame.rowlook, frame.collook, frame.alpha,
+                               device=cuda, sample_format=fmt, crossmul_fused=fused)
+        if fmt == "ci16":
+            for v, s in zip(bc.ref_views + bc.sec_views, frame.ref_slc + frame.sec_slc):
+                v.copy_(synth.cint16(s))
+        else:
+            bc.load(frame.ref_slc, frame.sec_slc)
+        bc.run(frame.dem)
+        outs.append(_products(bc))
+    _check(outs[0], outs[1], exact=False)
+
+
+@pytest.mark.parametrize("looks", [(3, 7), (1, 1), (5, 33)])
+def test_fused_crossmul_other_looks(cuda, frame, looks):
+    """Look windows that do not divide the tiles (3 x 7, 5 x 33) and single
+    looks: the fused and unfused crossmul agree."""
+    rl, cl = looks
+    outs = []
+    for fused in (True, False):
+        bc = BatchedFrameChain(frame.ref, frame.sec, frame.rsc, rl, cl, frame.alpha, device=cuda,
+                               crossmul_fused=fused)
+        bc.load(frame.ref_slc, frame.sec_slc)
+        bc.run(frame.dem)
+        outs.append(_products(bc))
+    _check(outs[0], outs[1], exact=False)
+
+
+def test_fused_crossmul_unfused_deramp(cuda, frame):
+    """Fused crossmul on the deramp kernel's copies agrees with the fused
+    deramp path."""
+    outs = []
+    for dfused in (True, False):
+        bc = BatchedFrameChain(frame.ref, frame.sec, frame.rsc, frame.rowlook, frame.collook, frame.alpha,
+                               device=cuda, deramp_fused=dfused)
+        bc.load(frame.ref_slc, frame.sec_slc)
+        bc.run(frame.dem)
+        outs.append(_products(bc))
+    _check(outs[0], outs[1], exact=False)
