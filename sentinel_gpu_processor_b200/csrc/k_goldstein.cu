@@ -193,7 +193,10 @@ __device__ __forceinline__ void goldstein_patch(const float2 *__restrict__ in, f
   const float inv = 1.0f / mean;
 #pragma unroll
   for (int y = 0; y < GN; ++y) {
-    const float w = powf(ok ? S[y] * inv : 0.0f, alpha);
+    // S^alpha through the hardware exp2/log2 (relative error ~1e-6, far
+    // below the filter's float tolerance); 0^alpha = 0 for alpha > 0, and a
+    // NaN weight (0^0) leaves F unscaled, as a weight of 1 would
+    const float w = __powf(ok ? S[y] * inv : 0.0f, alpha);
     if (w > 0.0f) {
       x[y].x *= w;
       x[y].y *= w;
