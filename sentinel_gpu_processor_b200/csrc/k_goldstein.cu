@@ -151,7 +151,9 @@ __device__ __forceinline__ void goldstein_patch(const float2 *__restrict__ in, f
   fft32<false>(x);
   __syncwarp();
 #pragma unroll
-  for (int r = 0; r < GN; ++r) M[r][lane] = hypotf(x[r].x, x[r].y);
+  // |F|: spectral magnitudes of a 32 x 32 patch of interferogram samples are
+  // far from float overflow, so the plain root of the squared sum serves
+  for (int r = 0; r < GN; ++r) M[r][lane] = sqrtf(fmaf(x[r].x, x[r].x, x[r].y * x[r].y));
   __syncwarp();
   // 7x7 circular smoothing of |F| (goldstein.cu:105-119) and its patch sum.
   // The table is even in both offsets, g[ky][kx] = g[|ky|][|kx|], so
