@@ -413,12 +413,14 @@ int s1b_stitch(const s1b_stitch_burst_t *bursts, int32_t n, const void *data, in
 
 /* ------------------------------------------------------------ batched frame
  * All burst pairs of a frame (e.g. 3 subswaths x 9 bursts of uneven size)
- * processed with one launch per stage over a per-burst descriptor table:
- * deramp and geocoding run one CTA per tile over (tile x, tile y, burst)
- * grids, or as persistent kernels over the flat tile space of every burst
- * (the autotuner picks); the crossmul box of each pair is formed on the device from the
- * crop rows, so a run has no host synchronisation and can be captured in a
- * CUDA graph.  Replaces running geo2rdr per burst, crossmul_daemon and
+ * processed with one launch per stage over a per-burst descriptor table.  By
+ * default the deramp runs inside the geocoding's gathers and the geocoding
+ * of both bursts of each pair forms the crossmul's look-row sums (one CTA
+ * per tile of a pair's DEM windows); otherwise deramp and geocoding run one
+ * CTA per tile over (tile x, tile y, burst) grids, or as persistent kernels
+ * over the flat tile space of every burst (the autotuner picks).  The
+ * crossmul box of each pair is formed on the device from the crop rows, so a
+ * run has no host synchronisation and can be captured in a CUDA graph.  Replaces running geo2rdr per burst, crossmul_daemon and
  * goldstein per pair (csrc/src/geo2rdr.cu:316-651, crossmul_daemon.cu:566-975,
  * goldstein.cu:328-408); the per-pair results are those of s1b_deramp,
  * s1b_geo2rdr, s1b_crossmul_box, s1b_crossmul_looks and s1b_goldstein. */
@@ -436,7 +438,8 @@ typedef struct {
 } s1b_frame_pair_t;
 
 typedef struct {
-  size_t workspace_bytes;   /* device scratch: deramped bursts, geocoded windows, patches */
+  size_t workspace_bytes;   /* device scratch: deramped bursts (or column tables), geocoded windows,
+                               crossmul look-row sums, Goldstein patches */
   int64_t slc_elems;        /* samples of the SLC buffer: bursts back to back */
   int64_t product_elems;    /* elements of each product array (all pairs' slots) */
   int32_t max_nrow_ml, max_ncol_ml;
@@ -497,14 +500,17 @@ int s1b_frame_run(s1b_frame_t *frame, const void *slc, const int16_t *dem, int64
  * the deramp and geocoding stages on these buffers (`reps` runs each, CUDA
  * events on `stream`), keeps the fastest in the frame for later runs and
  * synchronises the stream.  Not capturable.  Every candidate produces the
- * same results. */
+ * same results.  Stages with a single form are not timed: the deramp fused
+ * into the gathers, the geocoding with the crossmul sums. */
 int s1b_frame_autotune(s1b_frame_t *frame, const void *slc, const int16_t *dem, int64_t dem_pitch,
                        void *workspace, void *ifg, float *amp1, float *amp2, float *coh, void *filt,
                        s1b_frame_pair_t *pairs, int32_t reps, void *stream);
 
 /* One run with CUDA events between its stages (synchronises the stream):
- * stage_ms[5] = deramp, geocoding, box, crossmul, Goldstein (patches and
- * overlap-add), in milliseconds.  For measurement; not capturable. */
+ * stage_ms[5] = deramp (or the column tables), geocoding (with the crossmul
+ * look-row sums when fused), box, crossmul (the look columns when fused),
+ * Goldstein (patches and overlap-add), in milliseconds.  For measurement; not
+ * capturable. */
 int s1b_frame_profile(s1b_frame_t *frame, const void *slc, const int16_t *dem, int64_t dem_pitch,
                       void *workspace, void *ifg, float *amp1, float *amp2, float *coh, void *filt,
                       s1b_frame_pair_t *pairs, float *stage_ms, void *stream);

@@ -212,3 +212,20 @@ def test_fused_crossmul_unfused_deramp(cuda, frame):
         bc.run(frame.dem)
         outs.append(_products(bc))
     _check(outs[0], outs[1], exact=False)
+
+
+def test_tall_looks_fall_back_to_the_crossmul_kernel(cuda, frame):
+    """A look row taller than a geocoding tile (rowlook > 128) cannot be summed
+    inside one tile: the frame refuses the fused crossmul
+    (S1B_ERR_UNSUPPORTED) and the chain runs the crossmul kernel instead."""
+    from sentinel_gpu_processor_b200 import _lib
+    bc = BatchedFrameChain(frame.ref, frame.sec, frame.rsc, 130, 4, frame.alpha, device=cuda)
+    assert not bc.crossmul_fused
+    assert _lib.load().s1b_frame_set_crossmul_fusion(bc._handle, 1) == _lib.S1B_ERR_UNSUPPORTED
+    bc.load(frame.ref_slc, frame.sec_slc)
+    bc.run(frame.dem)
+    # the small windows may hold no whole look row of 130 rows: any pair that
+    # does is formed by the crossmul kernel
+    for r in bc.results():
+        if r is not None:
+            assert r.ifg.shape[0] >= 1 and torch.isfinite(r.coh).all()
