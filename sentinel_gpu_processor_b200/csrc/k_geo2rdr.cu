@@ -767,6 +767,9 @@ __global__ __launch_bounds__(TX, kGeoGridMinBlocks<TX>) void frame_geo2rdr_grid_
 // geocoding does.  A burst is zero outside its window, as the reference's
 // crossmul reads a .gslc (zero-filled around its crop).  Tiles hold whole
 // look rows, so no look row spans two CTAs and the sums need no atomics.
+// Compiled for 5 CTAs per SM (96 registers): with two bursts' state per warp,
+// 72 or 80 registers spill and measured slower (9.74, 9.81 against 9.60 ms
+// per 27-pair frame).
 constexpr int kXmTX = kFrameXmCols;  // columns per tile
 
 template <typename TSrc, bool kFused>
@@ -828,8 +831,7 @@ __global__ __launch_bounds__(kXmTX, 5) void frame_geo_xmul_kernel(const FrameDev
       const TSrc *src = kFused ? static_cast<const TSrc *>(io.slc) + fb.slc_off
                                : reinterpret_cast<const TSrc *>(io.work + fb.der_off);
       off[q] = geo_warp_setup<RY>(P, d.plans[q ? pr.sec : pr.ref].orbit, dem, io.dem_pitch, src, row0w[q], rT, rB,
-                                  cL, cR, d.cull_geo != 0,
-                                  s_zd[q][wid], s_seed[q][wid]);
+                                  cL, cR, d.cull_geo != 0, s_zd[q][wid], s_seed[q][wid]);
 #pragma unroll
       for (int j = 0; j < RY / 32; ++j)
         if (32 * j + 31 < rT - row0w[q] || 32 * j > rB - row0w[q]) off[q] |= 1u << j;
