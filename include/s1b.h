@@ -336,13 +336,17 @@ int s1b_goldstein(const void *in, void *out, int32_t nrow, int32_t ncol, int32_t
  * exits.  No counterpart in the reference.
  *   - Images needing more than S1B_GOLDSTEIN_NOALLOC_MAX_PATCHES patches
  *     return S1B_ERR_TOO_LARGE (use s1b_goldstein then).
- *   - The first call on each device looks up the array's device address
- *     (cudaGetSymbolAddress, with that device current); make that first call
- *     before any stream capture.
+ *   - The array's device address belongs to a CUDA context: the first call
+ *     in each context (the device's primary context, or a context the host
+ *     application made current) looks it up with cudaGetSymbolAddress and
+ *     caches it under that context; make that first call before any stream
+ *     capture.
  *   - All calls share the one array: calls that can run at the same time on
  *     the GPU (different streams, or threads without ordering) race and
  *     corrupt each other's results; serialise them.
- *   - in/out: complex64 [nrow * ncol] device, n_win must be 32. */
+ *   - in/out: complex64 [nrow * ncol] device, n_win must be 32.  in and out
+ *     may be the same buffer: every read of `in` (the patch kernel) is
+ *     ordered on the stream before the first write of `out` (the gather). */
 int s1b_goldstein_noalloc(const void *in, void *out, int32_t nrow, int32_t ncol, int32_t n_win,
                           float alpha, void *stream);
 

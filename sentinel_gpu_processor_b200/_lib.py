@@ -27,6 +27,7 @@ S1B_INTERP_SINC8 = 1
 S1B_SAMPLES_C64 = 0
 S1B_SAMPLES_CI16 = 1
 MAX_WIN = MAX_STATE_VECTORS - 3
+S1B_GOLDSTEIN_NOALLOC_MAX_PATCHES = 4096
 
 
 class S1BError(RuntimeError):

@@ -13,11 +13,13 @@
 //   2. goldstein_gather_kernel -- one thread per output pixel sums the (up to
 //      16) weighted patches covering it in a fixed order and divides by the
 //      summed weights.  No atomics: the result is deterministic.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
 
 #include "s1b.h"
+#include "s1b_ctx_cache.h"
 #include "s1b_device.cuh"
 #include "s1b_frame.h"
 #include "s1b_internal.h"
@@ -367,26 +369,66 @@ namespace {
 constexpr size_t kNoAllocMaxPatches = S1B_GOLDSTEIN_NOALLOC_MAX_PATCHES;
 __device__ __align__(256) float2 g_goldstein_scratch[kNoAllocMaxPatches * GN * GN];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_scratch_mu;
-void *g_scratch_ptr[kMaxDevices] = {};
+// The array's device address, per CUDA context (see s1b_ctx_cache.h).
+ContextKeyedCache<64> g_scratch_cache;
 
-// Device address of g_goldstein_scratch on the current device.  The symbol
-// name is only a host-side handle; the address is looked up once per device
-// (with that device current) and cached.
-int noalloc_scratch(void **ptr) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return s1b_fail(S1B_ERR_CUDA, cudaGetErrorString(e));
-  if (dev < 0 || dev >= kMaxDevices) return s1b_fail(S1B_ERR_UNSUPPORTED, "s1b_goldstein_noalloc: device ordinal above 63");
-  std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_ptr[dev]) {
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long *);
+
+// The calling thread's current context and its unique id, through the
+// driver entry points the runtime hands out (no link against libcuda).
+// ctx is null when no context is current; cacheable is false when the
+// driver cannot give the id, and then nothing is cached.
+int current_context(const void **ctx, uint64_t *id, bool *cacheable) {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
     void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_goldstein_scratch);
-    if (e != cudaSuccess) return s1b_fail(S1B_ERR_CUDA, cudaGetErrorString(e));
-    g_scratch_ptr[dev] = p;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(p);
+    p = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(p);
+    cudaGetLastError();
+  });
+  *ctx = nullptr;
+  *id = 0;
+  *cacheable = false;
+  if (!get_current) return S1B_OK;
+  CUcontext c = nullptr;
+  if (get_current(&c) != CUDA_SUCCESS) return s1b_fail(S1B_ERR_CUDA, "s1b_goldstein_noalloc: cuCtxGetCurrent failed");
+  *ctx = c;
+  unsigned long long u = 0;
+  if (c && get_id && get_id(c, &u) == CUDA_SUCCESS) {
+    *id = u;
+    *cacheable = true;
   }
-  *ptr = g_scratch_ptr[dev];
+  return S1B_OK;
+}
+
+// Device address of g_goldstein_scratch in the calling thread's current
+// context.  The symbol name is only a host-side handle.  The address is
+// looked up with cudaGetSymbolAddress the first time a context calls (which
+// makes the device's primary context current when none is) and cached under
+// that context's handle and id.
+int noalloc_scratch(void **ptr) {
+  const void *ctx;
+  uint64_t id;
+  bool cacheable;
+  int s = current_context(&ctx, &id, &cacheable);
+  if (s) return s;
+  if (cacheable && g_scratch_cache.find(ctx, id, ptr)) return S1B_OK;
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_goldstein_scratch);
+  if (e != cudaSuccess) return s1b_fail(S1B_ERR_CUDA, cudaGetErrorString(e));
+  s = current_context(&ctx, &id, &cacheable);  // the context the lookup ran in
+  if (s) return s;
+  if (cacheable) g_scratch_cache.put(ctx, id, p);
+  *ptr = p;
   return S1B_OK;
 }
 
