@@ -55,6 +55,9 @@ GEO_FUSED_TRAFFIC_RATIO = 1.182
 # the same with the crossmul look sums formed in the geocoding (391.7 MB / 290.7 MB)
 GEO_XMUL_TRAFFIC_RATIO = 1.347
 RESAMPLE_DRAM_BYTES_PER_PX = 24.75
+# what bounds the frame geocoding, from its ncu counters (issue and warp stalls)
+GEO_LIMITER = ("latency: per-pixel chain of FP64 solve, gathers and phasors at 20 resident warps per SM "
+               "(issue active 47 %, FP64 pipe 24 %); not HBM")
 
 
 def parse():
@@ -66,12 +69,16 @@ def parse():
     ap.add_argument("--config", default="frame",
                     choices=["frame", "frame_small", "frame_pairs", "c1", "c1geo", "c0", "small", "adjoint"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the checker leg (pair 0 against the reference executables and the float64 oracle)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="frame: skip the extra measurements (complex int16 variant, radar-grid kernels, adjoint)")
     ap.add_argument("--deramp", default="fused", choices=["fused", "kernel"],
                     help="frame deramp: inside the geocoding's gathers, or a separate kernel writing deramped bursts")
     ap.add_argument("--crossmul", default="fused", choices=["fused", "kernel"],
                     help="frame: crossmul look sums formed in the geocoding (fused) or a crossmul kernel reading "
                          "geocoded windows")
-    ap.add_argument("--samples", default="ci16", choices=["ci16", "c64"],
+    ap.add_argument("--samples", default="c64", choices=["ci16", "c64"],
                     help="frame SLC sample type: complex int16 as in the measurement TIFF (widened on the GPU), "
                          "or complex64 as the reference's geo2rdr pipe carries it")
     return ap.parse_args()
@@ -219,6 +226,43 @@ def peaks():
 # the batched frame: the full IW frame, and a small one (1 subswath x 3 bursts
 # at half size, default tuning) for quick runs and profiler captures
 FRAME_CONFIGS = ("frame", "frame_small")
+FRAME_SEED = 20261203 + 2000
+
+
+def frame_scene(config, rank, device, boxes_of, slc_pairs=None):
+    """The frame workload of both arms: the seeded synthetic frame on a DEM
+    grid where the reference geo2rdr runs of burst pair 0 stay inside their
+    buffers (both arms time the same frame on the same grid).
+    ``boxes_of(acq)``: the bursts' footprint boxes (the library's planner in
+    the s1b arm, the oracle's restatement in the reference arm; the grid
+    search gives the same grid for either).  ``slc_pairs``: make the SLCs of
+    the first pairs only."""
+    from sentinel_gpu_processor_b200 import synth
+    small = config == "frame_small"
+    sc = synth.make_frame(seed=FRAME_SEED + rank, device=device, slc_pairs=slc_pairs,
+                          **(dict(n_swaths=1, n_bursts=3, scale=0.5) if small else {}))
+    return synth.on_reference_safe_grid(sc, boxes_of, pairs=(0,))
+
+
+def frame_config(args, sc, world):
+    """``config`` of the frame workload: the same dict in both arms."""
+    small = args.config == "frame_small"
+    n = len(sc.ref)
+    head = (f"small frame: {n} burst pairs (1 subswath x 3) of half-size bursts" if small else
+            f"full IW frame: {n} burst pairs (3 subswaths x 9) of uneven size, lines 1480-1530, samples "
+            f"20000-25500, 100-line overlap, Doppler rate per subswath in -1700..-1400 Hz/s, coherence per "
+            f"burst in 0.3..0.9")
+    samples = "complex int16" if args.samples == "ci16" else "complex64"
+    r = sc.rsc
+    return {"workload": f"{head}; {samples} SLC samples; int16 fBm DEM (0-3000 m) on a 1/7200-degree grid",
+            "seed": int(sc.seed), "burst_pairs": n,
+            "burst_px_per_step": int(sum(a.radar.lines_per_burst * a.radar.samples_per_burst for a in sc.ref)),
+            "slc_samples": samples, "looks": [sc.rowlook, sc.collook],
+            "goldstein": {"alpha": sc.alpha, "n_win": 32, "step": 8},
+            "dem_grid": {"nlat": r.nlat, "nlon": r.nlon, "latmax": r.latmax, "lonmin": r.lonmin, "dlat": r.dlat,
+                         "dlon": r.dlon},
+            "l2": "inputs larger than L2 (>= 160 MB per burst, read once per step)",
+            "parallelism": f"replicas{world}"}
 
 
 def make_scene(config, seed, device):
@@ -230,38 +274,71 @@ def make_scene(config, seed, device):
 # CPU baseline: the float64 oracle on a bounded sample of the same workload
 # ----------------------------------------------------------------------------
 
-def cpu_baseline():
+# the CPU baseline's unit of work: one burst pair of the frame's geometry and
+# processing (looks 4 x 20, Goldstein alpha 0.5), 256 lines x 1024 samples
+CPU_PAIR = dict(lines=256, samples=1024, rowlook=4, collook=20, alpha=0.5)
+
+
+def _cpu_pair_worker(seed):
+    """The float64 oracle chain on one seeded burst pair, in a spawned worker
+    process with one thread: geo2rdr of both SLCs, crossmul + looks, amplitude
+    looks and coherence, Goldstein.  Returns (burst pixels, seconds)."""
+    for v in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[v] = "1"
+    if ROOT not in sys.path:
+        sys.path.insert(0, ROOT)
     import numpy as np
+    import torch
+    torch.set_num_threads(1)
 
     from oracle import coherence as oc
     from oracle import crossmul as ox
     from oracle import geo2rdr as og2
     from oracle import goldstein as ogs
     from sentinel_gpu_processor_b200 import synth
-    sc = synth.make_pair("small", seed=99)  # 160 x 640 burst, same geometry and processing
+    if seed is None:  # warm-up: imports only
+        return 0, 0.0
+    sc = synth.make_pair("c0", seed=seed, **CPU_PAIR)
     rsc = og2.Rsc(**sc.rsc.__dict__)
-    times = []
-    for _ in range(2):
+    t0 = time.perf_counter()
+    outs = []
+    for acq, slc in ((sc.ref[0], sc.ref_slc[0]), (sc.sec[0], sc.sec_slc[0])):
+        r = og2.Radar(**{k: getattr(acq.radar, k) for k in og2.Radar.__dataclass_fields__})
+        b = og2.BurstMeta(**{k: getattr(acq.bursts[0], k) for k in og2.BurstMeta.__dataclass_fields__})
+        outs.append(og2.geo2rdr_burst(slc.numpy(), sc.dem.numpy(), rsc, r, acq.orbit, acq.fm, acq.dc, b))
+    (h1, d1), (h2, d2) = outs
+    box = ox.intersection_box(h1, h2, sc.rowlook, sc.collook)
+    ifg = ox.crossmul_looks(ox.crop(h1, d1, box), ox.crop(h2, d2, box), sc.rowlook, sc.collook)
+    a1 = np.sqrt(oc.powlooks(ox.crop(h1, d1, box), sc.rowlook, sc.collook))
+    a2 = np.sqrt(oc.powlooks(ox.crop(h2, d2, box), sc.rowlook, sc.collook))
+    oc.coherence(ifg, a1, a2)
+    if min(ifg.shape) >= 32:
+        ogs.goldstein(ifg, 32, sc.alpha)
+    return sc.burst_pixels, time.perf_counter() - t0
+
+
+def cpu_baseline():
+    """The float64 NumPy oracle chain on the host's cores: one spawned worker
+    per core (spawned, so no worker inherits this process's CUDA context),
+    each running the whole chain on its own seeded burst pair; the rate is
+    the pixels of all pairs over the wall time of the batch."""
+    import multiprocessing as mp
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        pool.map(_cpu_pair_worker, [None] * cores)  # workers started and modules imported before timing
+        seeds = [20261203 + 4000 + k for k in range(cores)]
         t0 = time.perf_counter()
-        outs = []
-        for acq, slc in ((sc.ref[0], sc.ref_slc[0]), (sc.sec[0], sc.sec_slc[0])):
-            r = og2.Radar(**{k: getattr(acq.radar, k) for k in og2.Radar.__dataclass_fields__})
-            b = og2.BurstMeta(**{k: getattr(acq.bursts[0], k) for k in og2.BurstMeta.__dataclass_fields__})
-            outs.append(og2.geo2rdr_burst(slc.numpy(), sc.dem.numpy(), rsc, r, acq.orbit, acq.fm, acq.dc, b))
-        (h1, d1), (h2, d2) = outs
-        box = ox.intersection_box(h1, h2, sc.rowlook, sc.collook)
-        ifg = ox.crossmul_looks(ox.crop(h1, d1, box), ox.crop(h2, d2, box), sc.rowlook, sc.collook)
-        a1 = np.sqrt(oc.powlooks(ox.crop(h1, d1, box), sc.rowlook, sc.collook))
-        a2 = np.sqrt(oc.powlooks(ox.crop(h2, d2, box), sc.rowlook, sc.collook))
-        oc.coherence(ifg, a1, a2)
-        if min(ifg.shape) >= 32:
-            ogs.goldstein(ifg, 32, sc.alpha)
-        times.append(time.perf_counter() - t0)
-    dt = min(times)
-    px = sc.burst_pixels
-    return {"value": px / dt, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"float64 NumPy oracle chain on a 160 x 640 burst pair of the same geometry and processing "
-                      f"({px} burst px, best of 2 runs, {dt:.2f} s)"}
+        res = pool.map(_cpu_pair_worker, seeds, chunksize=1)
+        wall = time.perf_counter() - t0
+    px = sum(r[0] for r in res)
+    busy = sum(r[1] for r in res)
+    return {"value": px / wall, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": (f"float64 NumPy oracle chain (geo2rdr x2, crossmul + looks, amplitude looks + coherence, "
+                       f"Goldstein) on {cores} seeded burst pairs of {CPU_PAIR['lines']} x {CPU_PAIR['samples']} "
+                       f"of the frame's geometry and processing, one per worker process, {cores} processes; "
+                       f"{px} burst px in {wall:.1f} s wall ({busy / max(len(res), 1):.1f} s per pair)"),
+            "os_cpu_count": os.cpu_count()}
 
 
 # ----------------------------------------------------------------------------
@@ -276,9 +353,9 @@ def _workload(args, rank, dev):
         import torch
 
         from sentinel_gpu_processor_b200.chain import BatchedFrameChain
+        from sentinel_gpu_processor_b200 import plan as _plan
         small = args.config == "frame_small"
-        sc = synth.make_frame(seed=20261203 + 2000 + rank, device=dev,
-                              **(dict(n_swaths=1, n_bursts=3, scale=0.5) if small else {}))
+        sc = frame_scene(args.config, rank, dev, _plan.footprint_boxes)
         chain = BatchedFrameChain(sc.ref, sc.sec, sc.rsc, sc.rowlook, sc.collook, sc.alpha, device=dev,
                                   sample_format=args.samples, deramp_fused=args.deramp == "fused",
                                   crossmul_fused=args.crossmul == "fused")
@@ -563,17 +640,220 @@ def _kernel_table(chain, sc, args, times, peak):
     return rows
 
 
+def _timed_replays(run, steps, warm=3):
+    """ms per step of ``run`` over ``steps`` steps, CUDA events on the current stream."""
+    import torch
+    for _ in range(warm):
+        run()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        run()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / steps
+
+
+def _ci16_variant(chain, sc, steps):
+    """The same frame from complex int16 samples (the measurement TIFF's type,
+    round(2000 s), widened on the GPU), with the complex64 run's tile shapes:
+    device-resident rate."""
+    import torch
+
+    from sentinel_gpu_processor_b200 import synth
+    from sentinel_gpu_processor_b200.chain import BatchedFrameChain
+    v = BatchedFrameChain(sc.ref, sc.sec, sc.rsc, sc.rowlook, sc.collook, sc.alpha, device=chain.dev,
+                          sample_format="ci16", deramp_fused=chain.deramp_fused, crossmul_fused=chain.crossmul_fused)
+    for dst, src in zip(v.ref_views + v.sec_views, chain.ref_views + chain.sec_views):
+        dst.copy_(synth.cint16(src))
+    v.set_tuning(**chain.tuning())
+    v.capture(sc.dem)
+    ms = _timed_replays(v.replay, steps)
+    del v
+    torch.cuda.empty_cache()
+    return {"value": chain.burst_pixels / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
+            "slc_samples": "complex int16 (round(2000 s), widened on the GPU)", "tuning": chain.tuning()}
+
+
+def _radar_extras(dev, peak, steps=10):
+    """Radar-grid kernels on one 1500 x 21000 burst pair (8-tap sinc
+    resampling, 5 x 5 box coherence): per-kernel times from CUDA events
+    around each entry point over eager steps, and their HBM fractions."""
+    import torch
+
+    from sentinel_gpu_processor_b200 import synth
+    from sentinel_gpu_processor_b200.chain import RadarChain
+    sc = synth.make_radar_pair("c1", seed=20261203 + 1000, device=dev)
+    chain = RadarChain(sc.ref, sc.sec, sc.ref_slc.shape[0], sc.ref_slc.shape[1], sc.rowlook, sc.collook, sc.alpha,
+                       device=dev)
+    ins = _radar_inputs(sc)
+    for _ in range(3):
+        chain.run(*ins)
+    torch.cuda.synchronize()
+    if not chain.staging_ok():
+        raise SystemExit("a shared-memory staging copy did not complete")
+    times = _instrumented(lambda: chain.run(*ins), steps)
+    px = chain.burst_pixels
+    bytes_per = {"geo2rdr_offsets": 32 * px, "resample": 24 * px, "box_coherence": 20 * px}
+    out = {"workload": f"one burst pair {chain.L} x {chain.S} complex64, float64 lat/lon/hgt rasters",
+           "peak_gbs": peak}
+    for name, b in bytes_per.items():
+        ts = times.get(name)
+        if not ts:
+            continue
+        ms = sum(ts) / len(ts)
+        gbs = b / (ms / 1e3) / 1e9
+        out[name] = {"avg_ms": ms, "bytes_per_launch": b, "achieved_gbs": gbs, "frac": gbs / peak,
+                     "launches": len(ts)}
+    del chain, sc
+    torch.cuda.empty_cache()
+    return out
+
+
+def _workdir(need_bytes):
+    """A scratch directory on /dev/shm when it has room, else on disk."""
+    base = None
+    if os.path.isdir("/dev/shm"):
+        st = os.statvfs("/dev/shm")
+        if st.f_bavail * st.f_frsize > 2 * need_bytes:
+            base = "/dev/shm"
+    return tempfile.mkdtemp(prefix="s1b_check_", dir=base)
+
+
+def parity_leg(pair, dem_host, rsc, looks, alpha, plans, dem_dev):
+    """Checker (outside every timed region): burst pair 0 of the frame run
+    through the reference executables (sm_100a builds of its sources in
+    oracle/_ref: geo2rdr x 2, crossmul_daemon, goldstein) on the same inputs
+    in its file formats, and the reference's NumPy amplitude-look and
+    coherence formulas on their outputs; compared with the batched frame's
+    products of pair 0.  The geocoding's sample coordinates
+    (s1b_geo2rdr_grid_offsets) are compared with the float64 oracle on rows
+    spread over both bursts' DEM windows.
+
+    ``pair``: dict with the acquisitions, complex64 SLCs (numpy) and the
+    frame's products of pair 0 (numpy)."""
+    import numpy as np
+
+    from oracle import coherence as oc
+    from oracle import crossmul as ox
+    from oracle import geo2rdr as og2
+    from oracle import refrun
+    from sentinel_gpu_processor_b200 import formats, kernels
+    out = {"pair": 0}
+    rl, cl = looks
+    # sample coordinates of the geocoding against the float64 oracle
+    off = {}
+    for tag, acq, pl in (("ref", pair["ref"], plans[0]), ("sec", pair["sec"], plans[1])):
+        az, rg = kernels.geo2rdr_grid_offsets(pl, dem_dev)
+        rows = np.linspace(0, pl.nrow - 1, 8).round().astype(np.int64)
+        r = og2.Radar(**{k: getattr(acq.radar, k) for k in og2.Radar.__dataclass_fields__})
+        b = og2.BurstMeta(**{k: getattr(acq.bursts[0], k) for k in og2.BurstMeta.__dataclass_fields__})
+        win = dem_host[pl.win_top:pl.win_bottom, pl.win_left:pl.win_right]
+        oaz, org = og2.window_offsets(win, rows, r, acq.orbit, b, rsc.latmax + rsc.dlat * pl.win_top,
+                                      rsc.lonmin + rsc.dlon * pl.win_left, rsc.dlat, rsc.dlon)
+        gaz, grg = az.cpu().numpy()[rows], rg.cpu().numpy()[rows]
+        used = ((org > b.first_valid_sample) & (org < b.last_valid_sample - 1) & (oaz >= b.first_valid_line + 5)
+                & (oaz < b.last_valid_line - 5))
+        off[tag] = {"rows": int(len(rows)), "pixels": int(oaz.size), "pixels_in_burst": int(used.sum()),
+                    "max_az_px": float(np.abs(gaz - oaz)[used].max()) if used.any() else None,
+                    "max_rg_px": float(np.abs(grg - org)[used].max()) if used.any() else None,
+                    "max_az_px_whole_window": float(np.abs(gaz - oaz).max()),
+                    "max_rg_px_whole_window": float(np.abs(grg - org).max())}
+        del az, rg
+    vals = [v for t in off.values() for v in (t["max_az_px"], t["max_rg_px"]) if v is not None]
+    out["offset_px"] = max(vals) if vals else None
+    out["offsets_vs_float64_oracle"] = off
+    if not refrun.available():
+        out["reference"] = "unavailable: reference executables not built in oracle/_ref"
+        return out
+    wd = _workdir(dem_host.nbytes + 2 * pair["ref_slc"].nbytes)
+    try:
+        rscf, demf = refrun.write_dem(wd, rsc, dem_host)
+        gs = {}
+        for tag in ("ref", "sec"):
+            db = refrun.write_geo2rdr_inputs(wd, tag, pair[tag], [pair[tag + "_slc"]], rscf, demf)
+            o, _ = refrun.geo2rdr(db, os.path.join(wd, tag), 1)
+            gs[tag] = o[0]
+        f1, f2 = os.path.join(wd, "ref_burst_0.gslc"), os.path.join(wd, "sec_burst_0.gslc")
+        fo = os.path.join(wd, "pair.int")
+        refrun.crossmul_daemon([(f1, f2, fo)], os.path.join(wd, "tasks.txt"), rl, cl, manual=False)
+        wh, wifg = formats.read_raster(fo)
+        (h1, d1), (h2, d2) = gs["ref"], gs["sec"]
+        box = (int(wh[2]) * cl, int(wh[3]) * rl, int(wh[4]) * cl, int(wh[5]) * rl)
+        wa1 = np.sqrt(oc.powlooks(ox.crop(h1, d1, box), rl, cl))
+        wa2 = np.sqrt(oc.powlooks(ox.crop(h2, d2, box), rl, cl))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            wc = np.abs(wifg) / (wa1 + 1e-12) / (wa2 + 1e-12)
+        gf = os.path.join(wd, "ifg.int")
+        np.ascontiguousarray(wifg, dtype=np.complex64).tofile(gf)
+        wfilt, _ = refrun.goldstein(gf, wifg.shape[0], wifg.shape[1], 32, alpha)
+    finally:
+        shutil.rmtree(wd, ignore_errors=True)
+    ifg, a1, a2, coh, filt = (pair[k] for k in ("ifg", "amp1", "amp2", "coh", "filt"))
+    gh = np.asarray(pair["header"][:6])
+    out["ifg_header_equal"] = bool(np.array_equal(gh, np.asarray(wh[:6])))
+    out["ifg_headers"] = {"ours": [int(v) for v in gh], "reference": [int(v) for v in wh[:6]]}
+    out["gslc_crop_rows"] = {"ours": [[int(h[3]), int(h[5])] for h in pair["gslc_headers"]],
+                             "reference": [[int(h1[3]), int(h1[5])], [int(h2[3]), int(h2[5])]]}
+    # common multilooked region of the two interferograms (the reference's crop
+    # rows can be narrower, geo2rdr.cu:115-122; every row of its box is one it
+    # kept, so the common region holds identical inputs)
+    l0, t0 = max(gh[2], wh[2]), max(gh[3], wh[3])
+    r0, b0 = min(gh[4], wh[4]), min(gh[5], wh[5])
+    if r0 <= l0 or b0 <= t0:
+        out["common_region"] = "empty"
+        return out
+
+    def cut(a, h):
+        return a[t0 - h[3]:b0 - h[3], l0 - h[2]:r0 - h[2]]
+
+    ifg_c, a1_c, a2_c, coh_c = (cut(x, gh) for x in (ifg, a1, a2, coh))
+    wifg_c, wa1_c, wa2_c, wc_c = (cut(x, wh) for x in (wifg, wa1, wa2, wc))
+    out["common_ml_pixels"] = int(ifg_c.size)
+    both = (np.abs(ifg_c) > 0) & (np.abs(wifg_c) > 0)
+    d = np.angle(ifg_c[both].astype(np.complex128) * np.conj(wifg_c[both].astype(np.complex128)))
+    out["rms_phase_rad"] = float(np.sqrt(np.mean(d * d))) if d.size else None
+    out["ifg_rel_err"] = float(np.abs(ifg_c.astype(np.complex128) - wifg_c).max() / np.abs(wifg_c).max())
+    out["validity_mismatch_frac"] = float(((np.abs(ifg_c) > 0) != (np.abs(wifg_c) > 0)).mean())
+    out["amp_rel_err"] = float(max(np.abs(a1_c - wa1_c).max() / wa1_c.max(), np.abs(a2_c - wa2_c).max() / wa2_c.max()))
+    # coherence: pixels where neither side takes the > 1 fill (seeded here,
+    # unseeded rand() in the reference)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        raw = np.abs(ifg_c.astype(np.float64)) / (a1_c + 1e-12) / (a2_c + 1e-12)
+    m = both & np.isfinite(wc_c) & (wc_c <= 1.0) & (raw <= 1.0)
+    out["max_dcoh"] = float(np.abs(coh_c[m] - wc_c[m]).max()) if m.any() else None
+    if out["ifg_header_equal"]:
+        gfilt, src = filt, "the frame's own interferogram"
+    else:  # the patch grids differ with the image extent: filter the reference's interferogram
+        import torch
+
+        from sentinel_gpu_processor_b200 import kernels as K
+        gfilt = K.goldstein(torch.from_numpy(np.ascontiguousarray(wifg, dtype=np.complex64)).cuda(), alpha).cpu().numpy()
+        src = "the reference's interferogram (headers differ)"
+    fm = (np.abs(gfilt) > 0) & (np.abs(wfilt) > 1e-3 * np.abs(wfilt).max())
+    d = np.angle(gfilt[fm].astype(np.complex128) * np.conj(wfilt[fm].astype(np.complex128)))
+    out["goldstein_rms_phase_rad"] = float(np.sqrt(np.mean(d * d))) if d.size else None
+    out["goldstein_input"] = src
+    out["against"] = ("reference executables geo2rdr x2, crossmul_daemon, goldstein (cuFFT), sm_100a builds of its "
+                      "sources, and its NumPy amplitude-look and coherence formulas; same inputs in its file formats")
+    out["tolerances"] = {"rms_phase_rad": 1e-3, "max_dcoh": 1e-4, "offset_px": 1e-4}
+    return out
+
+
 def run_s1b(args):
     import torch
     rank, world, local = dist_setup(args.gpus)
     dev = torch.device("cuda", local)
     sc, chain, run, desc = _workload(args, rank, dev)
+    frame = args.config in FRAME_CONFIGS
     warm = max(args.warmup, 3)
     res = None
     for _ in range(warm):
         res = run()
     torch.cuda.synchronize()
-    if args.config in FRAME_CONFIGS:
+    if frame:
         res = chain.results()
     if res is None or (isinstance(res, list) and any(r is None for r in res)):
         raise SystemExit("empty interferogram for the synthetic input")
@@ -598,13 +878,9 @@ def run_s1b(args):
     elapsed_ms = max_over_ranks(start.elapsed_time(stop), world)
     value = job_rate(world, args.steps, chain.burst_pixels, elapsed_ms)
     e2e, h2d, d2h = _e2e(chain, sc, args, world)
-
-    if isinstance(res, list):
-        chain.last = res
-    else:
-        chain.last = res
+    chain.last = res
     peak, peak_kind = peaks()
-    if args.config in FRAME_CONFIGS:
+    if frame:
         times = {}
         for _ in range(max(2, min(args.steps, 10))):
             for name, ms in chain.profile(sc.dem).items():
@@ -614,32 +890,31 @@ def run_s1b(args):
                               max(2, min(args.steps, 10)))
     table = _kernel_table(chain, sc, args, times, peak)
     top = max(table, key=lambda n: table[n]["total_ms"])
-    if args.config in FRAME_CONFIGS:
-        extra = {"burst_pairs": chain.n_pairs, "burst_px_per_step": chain.burst_pixels,
-                 "geo_px_total": sum(chain.geo_pixels()),
-                 "ifg_ml_shapes_first3": [list(r.ifg.shape) for r in res[:3]],
-                 "batched": True, "cuda_graph": True, "tuning": chain.tuned,
-                 "slc_samples": "complex int16" if args.samples == "ci16" else "complex64",
-                 "deramp": "fused into the geocoding gathers" if chain.deramp_fused else "separate kernel",
-                 "crossmul": ("look sums formed in the geocoding (no geocoded windows)" if chain.crossmul_fused
-                              else "kernel reading the geocoded windows")}
+    run_info = {"implementation": desc}
+    if frame:
+        run_info.update({"geo_px_total": sum(chain.geo_pixels()),
+                         "ifg_ml_shapes_first3": [list(r.ifg.shape) for r in res[:3]],
+                         "batched": True, "cuda_graph": True, "tuning": chain.tuned,
+                         "deramp": "fused into the geocoding gathers" if chain.deramp_fused else "separate kernel",
+                         "crossmul": ("look sums formed in the geocoding (no geocoded windows)"
+                                      if chain.crossmul_fused else "kernel reading the geocoded windows")})
         launches = chain.launches_per_step()
     elif args.config == "frame_pairs":
-        extra = {"burst_pairs": len(chain.pairs), "burst_px_per_step": chain.burst_pixels,
-                 "geo_px_total": sum(chain.geo_pixels()),
-                 "ifg_ml_shapes_first3": [list(r.ifg.shape) for r in res[:3]], "batched": False}
+        run_info.update({"burst_pairs": len(chain.pairs), "burst_px_per_step": chain.burst_pixels,
+                         "geo_px_total": sum(chain.geo_pixels()),
+                         "ifg_ml_shapes_first3": [list(r.ifg.shape) for r in res[:3]], "batched": False})
         launches = chain.launches_per_step()
     elif args.config == "c1":
-        extra = {"lines": chain.L, "samples": chain.S, "ifg_ml": list(res["ifg"].shape), "interp": chain.interp,
-                 "coherence_window": chain.win, "cuda_graph": True}
+        run_info.update({"lines": chain.L, "samples": chain.S, "ifg_ml": list(res["ifg"].shape),
+                         "interp": chain.interp, "coherence_window": chain.win, "cuda_graph": True})
         launches = chain.launches_per_step()
     else:
-        extra = {"lines": chain.plans[0].lines, "samples": chain.plans[0].samples,
-                 "geo_px_total": sum(p.nrow * p.ncol for p in chain.plans), "ifg_ml": list(res.ifg.shape)}
+        run_info.update({"lines": chain.plans[0].lines, "samples": chain.plans[0].samples,
+                         "geo_px_total": sum(p.nrow * p.ncol for p in chain.plans), "ifg_ml": list(res.ifg.shape)})
         launches = chain.launches_per_step()
     traffic = None
     if top == "geo2rdr":
-        if args.config in FRAME_CONFIGS:  # one launch geocodes every burst
+        if frame:  # one launch geocodes every burst
             if chain.crossmul_fused:
                 traffic = (GEO_XMUL_TRAFFIC_RATIO * table["geo2rdr"]["bytes_per_launch"]
                            if GEO_XMUL_TRAFFIC_RATIO and chain.deramp_fused else None)
@@ -651,30 +926,60 @@ def run_s1b(args):
             traffic = GEO_DRAM_BYTES_PER_GEO_PX * sum(p.nrow * p.ncol for p in pls) / len(pls)
     elif top == "resample":
         traffic = RESAMPLE_DRAM_BYTES_PER_PX * chain.burst_pixels
-    cfg = {"workload": desc, "looks": [sc.rowlook, sc.collook],
-           "goldstein": {"alpha": sc.alpha, "n_win": 32, "step": 8},
-           "l2": "inputs larger than L2 (>= 252 MB per SLC, read once per step)", "parallelism": f"replicas{world}"}
-    cfg.update(extra)
+    if frame:
+        cfg = frame_config(args, sc, world)
+    else:
+        cfg = {"workload": desc, "looks": [sc.rowlook, sc.collook],
+               "goldstein": {"alpha": sc.alpha, "n_win": 32, "step": 8},
+               "l2": "inputs larger than L2 (>= 252 MB per SLC, read once per step)",
+               "parallelism": f"replicas{world}"}
     t = table[top]
+    samples = "ci16 input widened to c64" if (frame and args.samples == "ci16") else "c64"
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": warm, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64 geometry + c64", "data": "synthetic",
-        "config": cfg,
+        "scaling": "weak", "vs_baseline": None, "dtype": f"f64 geometry + {samples}", "data": "synthetic",
+        "config": cfg, "run": run_info,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches * args.steps,
         "roofline": {"bound": "hbm", "kernel": top, "achieved": t["achieved_gbs"], "peak": peak, "unit": "GB/s",
                      "frac": t["frac"], "traffic": traffic, "peak_kind": peak_kind,
                      "bytes_per_launch": t["bytes_per_launch"], "launch_ms": t["avg_ms"],
-                     "timed": ("CUDA events between the stages of profiled frame runs" if args.config in FRAME_CONFIGS
+                     "timed": ("CUDA events between the stages of profiled frame runs" if frame
                                else "CUDA events around every launch of the entry point over instrumented eager steps"),
-                     "note": ("FP64-compute bound (zero-Doppler Newton): low HBM fraction by design"
-                              if top in ("geo2rdr", "geo2rdr_offsets") else "HBM-bound")},
+                     "limiter": GEO_LIMITER if top == "geo2rdr" else "HBM"},
         "kernels": table,
     }
     if clk is not None:
         line["clocks"] = clk
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    checker = rank == 0 and world == 1
+    pair0 = None
+    if frame and checker and not args.no_parity:
+        # pair 0's inputs and products, kept on the host for the checker leg
+        p0 = res[0]
+        views = (chain.ref_views[0], chain.sec_views[0])
+        if chain.sample_format == "ci16":
+            views = tuple(torch.view_as_complex(v.float()) for v in views)
+        pair0 = {"ref": sc.ref[0], "sec": sc.sec[0], "ref_slc": views[0].cpu().numpy(),
+                 "sec_slc": views[1].cpu().numpy(), "header": list(p0.header[:6]),
+                 "gslc_headers": [list(h[:6]) for h in p0.gslc_headers],
+                 **{k: getattr(p0, k).cpu().numpy() for k in ("ifg", "amp1", "amp2", "coh", "filt")}}
+        plans0 = (chain.plans[0], chain.plans[1])
+    if frame and not args.no_extras:
+        extras = {"complex_int16": _ci16_variant(chain, sc, args.steps)}
+        line["value_ci16"] = extras["complex_int16"]["value"]
+    if frame:
+        res = out = None
+        del chain, run
+        torch.cuda.empty_cache()
+        if not args.no_extras:
+            extras["radar_grid_c1"] = _radar_extras(dev, peak)
+            extras["adjoint_c3"] = adjoint_measure(dev, max(3, min(args.steps, 10)), world, compact=True)
+            line["extras"] = extras
+        if pair0 is not None:
+            line["parity"] = parity_leg(pair0, sc.dem.cpu().numpy(), sc.rsc, (sc.rowlook, sc.collook), sc.alpha,
+                                        plans0, sc.dem)
+    if checker and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -687,7 +992,25 @@ def run_s1b(args):
 # reference arm
 # ----------------------------------------------------------------------------
 
+def _repo_libraries_mapped():
+    """Shared objects from this repository mapped into this process."""
+    try:
+        with open("/proc/self/maps") as f:
+            paths = {ln.split()[-1] for ln in f if ln.rstrip().endswith(".so") or ".so." in ln}
+    except OSError:
+        return None
+    return sorted(p for p in paths if p.startswith(ROOT) and "baseline/_ref" not in p)
+
+
 def run_reference(args):
+    """The reference's own implementation on the same workload: its CUDA
+    executables (sm_100a builds of its sources in oracle/_ref) geo2rdr x 2,
+    crossmul_daemon and goldstein, and its NumPy amplitude-look and coherence
+    formulas, with the inputs in its file formats.  Frame configurations: a
+    bounded sample of the frame, burst pair 0, per step (the reference runs
+    geo2rdr once per burst for bursts of uneven size).  The scene is built
+    without the s1b library (the oracle's footprint boxes pick the same DEM
+    grid), so this process maps none of the repository's shared objects."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
@@ -697,37 +1020,45 @@ def run_reference(args):
     from oracle import coherence as oc
     from oracle import crossmul as ox
     from oracle import refrun
-    from sentinel_gpu_processor_b200 import formats, synth
+    from sentinel_gpu_processor_b200 import formats
     if not refrun.available():
         print(json.dumps({"impl": "reference", "unavailable": "reference executables not built in oracle/_ref "
                                                               "(python oracle/build_ref.py)"}))
         return
-    if args.config in ("frame", "frame_small", "frame_pairs"):
-        # a bounded sample of the frame: its first burst pair (the reference
-        # runs geo2rdr once per burst for uneven burst sizes)
-        frame = synth.make_frame(seed=20261203 + 2000, device="cuda",
-                                 **(dict(n_swaths=1, n_bursts=3, scale=0.5) if args.config == "frame_small" else {}))
-        base_sc = synth.frame_pair(frame, 0)
-        del frame
-        base_sc.dem = base_sc.dem.cpu()
-        base_sc.ref_slc = [t.cpu() for t in base_sc.ref_slc]
-        base_sc.sec_slc = [t.cpu() for t in base_sc.sec_slc]
-        sample = "first burst pair of the frame per step"
+    frame = args.config in FRAME_CONFIGS
+    if frame:
+        import torch
+        dev = "cuda" if torch.cuda.is_available() else "cpu"
+        sc = frame_scene(args.config, 0, dev, refrun.footprint_boxes, slc_pairs=1)
+        cfg = frame_config(args, sc, world)
+        dem = sc.dem.cpu().numpy()
+        slcs = {"ref": sc.ref_slc[0].cpu().numpy(), "sec": sc.sec_slc[0].cpu().numpy()}
+        if args.samples == "ci16":  # the reference's pipe carries the widened samples
+            from sentinel_gpu_processor_b200 import synth
+            slcs = {k: torch.view_as_complex(synth.cint16(torch.from_numpy(v)).float()).numpy()
+                    for k, v in slcs.items()}
+        sc.dem = sc.ref_slc = sc.sec_slc = None
+        if dev == "cuda":
+            torch.cuda.empty_cache()
+        sample = "burst pair 0 of the frame per step"
     else:
         base_sc = make_scene(args.config, 20261203 + 1000, "cpu")
+        sc = refrun.make_reference_safe(base_sc)
+        cfg = {"workload": f"burst pair {args.config}", "looks": [sc.rowlook, sc.collook],
+               "goldstein": {"alpha": sc.alpha, "n_win": 32, "step": 8}, "parallelism": f"replicas{world}"}
+        dem = sc.dem.numpy()
+        slcs = {"ref": sc.ref_slc[0].numpy(), "sec": sc.sec_slc[0].numpy()}
         sample = "one burst pair per step"
-    # the reference geo2rdr overruns its DEM/output buffers on some grids
-    # (oracle/refrun.geo2rdr_buffers_safe); run it only on a checked-safe grid
-    sc = refrun.make_reference_safe(base_sc)
-    base = "/dev/shm" if os.path.isdir("/dev/shm") else None
-    wd = tempfile.mkdtemp(prefix="s1b_refbench_", dir=base)
+    rl, cl = sc.rowlook, sc.collook
+    L = sc.ref[0].radar.lines_per_burst
+    S = sc.ref[0].radar.samples_per_burst
+    wd = _workdir(dem.nbytes + 2 * slcs["ref"].nbytes)
     try:
-        rscf, demf = refrun.write_dem(wd, sc.rsc, sc.dem.numpy())
+        rscf, demf = refrun.write_dem(wd, sc.rsc, dem)
         dbs = {}
-        for tag, acq, slc in (("ref", sc.ref[0], sc.ref_slc[0]), ("sec", sc.sec[0], sc.sec_slc[0])):
-            dbs[tag] = refrun.write_geo2rdr_inputs(wd, tag, acq, [slc.numpy()], rscf, demf)
-        L = sc.ref[0].radar.lines_per_burst
-        S = sc.ref[0].radar.samples_per_burst
+        for tag, acq in (("ref", sc.ref[0]), ("sec", sc.sec[0])):
+            dbs[tag] = refrun.write_geo2rdr_inputs(wd, tag, acq, [slcs[tag]], rscf, demf)
+        del dem, slcs
 
         def step():
             t0 = time.perf_counter()
@@ -737,14 +1068,13 @@ def run_reference(args):
                 outs[tag] = o[0]
             f1, f2 = os.path.join(wd, "ref_burst_0.gslc"), os.path.join(wd, "sec_burst_0.gslc")
             fo = os.path.join(wd, "pair.int")
-            refrun.crossmul_daemon([(f1, f2, fo)], os.path.join(wd, "tasks.txt"), sc.rowlook, sc.collook,
-                                   manual=False)
+            refrun.crossmul_daemon([(f1, f2, fo)], os.path.join(wd, "tasks.txt"), rl, cl, manual=False)
             ih, ifg = formats.read_raster(fo)
             # coherence: the reference's NumPy amplitude looks + coherence formula
-            box = (int(ih[2]) * sc.collook, int(ih[3]) * sc.rowlook, int(ih[4]) * sc.collook, int(ih[5]) * sc.rowlook)
+            box = (int(ih[2]) * cl, int(ih[3]) * rl, int(ih[4]) * cl, int(ih[5]) * rl)
             (h1, d1), (h2, d2) = outs["ref"], outs["sec"]
-            a1 = np.sqrt(oc.powlooks(ox.crop(h1, d1, box), sc.rowlook, sc.collook))
-            a2 = np.sqrt(oc.powlooks(ox.crop(h2, d2, box), sc.rowlook, sc.collook))
+            a1 = np.sqrt(oc.powlooks(ox.crop(h1, d1, box), rl, cl))
+            a2 = np.sqrt(oc.powlooks(ox.crop(h2, d2, box), rl, cl))
             oc.coherence(ifg, a1, a2)
             gf = os.path.join(wd, "ifg.int")
             ifg.astype(np.complex64).tofile(gf)
@@ -762,40 +1092,37 @@ def run_reference(args):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64 geometry + c64", "data": "synthetic",
-        "config": {"workload": f"{args.config}: {sample}, burst {L} x {S} complex64", "lines": L, "samples": S,
-                   "looks": [sc.rowlook, sc.collook], "goldstein": {"alpha": sc.alpha, "n_win": 32, "step": 8},
-                   "files": "reference formats on /dev/shm"},
+        "vs_baseline": None, "dtype": "f64 geometry + c64", "data": "synthetic", "config": cfg,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                         "sample": f"{sample}: the reference executables geo2rdr x2, crossmul_daemon, goldstein "
-                                   "(sm_100a builds of the reference sources) + its NumPy coherence, wall clock"},
+                         "sample": f"{sample} (burst {L} x {S}, complex64): the reference executables geo2rdr x2, "
+                                   "crossmul_daemon (its auto-tuned host workers), goldstein (sm_100a builds of the "
+                                   "reference sources) + its NumPy coherence, wall clock, inputs in its file formats"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "world_size_requested": world,
+        "repo_libraries_mapped": _repo_libraries_mapped(),
     }
     print(json.dumps(line), flush=True)
 
 
-def run_adjoint(args):
+def adjoint_measure(dev, steps, world, compact=False):
     """Adjoint of the coherence objective on 8 bursts of 1500 x 21000: gradient
     evaluations per second through the fused adjoint, against central finite
     differences of every parameter plus one height-error direction run with
-    the fused forward on the same GPU; a 50-step Adam refinement."""
+    the fused forward on the same GPU; a 50-step Adam refinement.  Returns a
+    dict of the measurements (``compact``: no end-to-end or per-step details)."""
     import torch
 
     from sentinel_gpu_processor_b200 import synth
     from sentinel_gpu_processor_b200.refine import CoherenceObjective, CoregProblem, refine
-    rank, world, local = dist_setup(args.gpus)
-    dev = torch.device("cuda", local)
     n = 8
-    st = synth.make_refine_stack(n_bursts=n, config="c1", seed=20261203 + 3000 + rank, device=dev)
+    st = synth.make_refine_stack(n_bursts=n, config="c1", seed=20261203 + 3000, device=dev)
     pr = CoregProblem(st.sec_plans, st.ref, st.sec, st.az0, st.rg0, st.daz_dh, st.drg_dh, st.rowlook, st.collook)
     L, S = st.az0.shape[1:]
     params = torch.zeros((n, 6), dtype=torch.float32, device=dev)
     dh = torch.zeros((n, L, S), dtype=torch.float32, device=dev)
     gp = torch.empty_like(params)
     gh = torch.empty_like(dh)
-    warm = max(args.warmup, 3)
-    for _ in range(warm):
+    for _ in range(3):
         pr.gradient(params, dh, gp, gh)
         pr.objective(params, dh)
     torch.cuda.synchronize()
@@ -812,11 +1139,8 @@ def run_adjoint(args):
         torch.cuda.synchronize()
         return max_over_ranks(a.elapsed_time(b), world) / k
 
-    clocks = Clocks(local)
-    clocks.start()
-    t_adj = timed(lambda: pr.gradient(params, dh, gp, gh), args.steps)
-    t_fwd = timed(lambda: pr.objective(params, dh), args.steps)
-    clk = clocks.stop()
+    t_adj = timed(lambda: pr.gradient(params, dh, gp, gh), steps)
+    t_fwd = timed(lambda: pr.objective(params, dh), steps)
     # finite differences as one would run them: central differences of all
     # 6 n parameters and one height-error direction, forward evaluations only
     gd = torch.Generator(device=dev)
@@ -843,20 +1167,29 @@ def run_adjoint(args):
     adj_dir = float((gh.double() * d.double()).sum())
     rel_p = float((gp.double() - fd).norm() / fd.norm())
     rel_h = abs(adj_dir - float(fd_dir)) / abs(float(fd_dir))
-    # e2e: the public autograd API, with pinned H2D of params and dh and D2H of both gradients
-    ph, hh = params.cpu().pin_memory(), dh.cpu().pin_memory()
-    gph, ghh = torch.empty_like(ph).pin_memory(), torch.empty_like(hh).pin_memory()
+    out = {"workload": f"{n} bursts of {L} x {S} complex64, offset polynomials (6 per burst, N(0, 0.05 px)) and a "
+                       f"height-error field (10 m rms, 31-px Gaussian); looks {st.rowlook} x {st.collook}",
+           "evals_per_s": 1e3 / t_adj, "gradient_ms": t_adj, "forward_ms": t_fwd,
+           "finite_differences": {"evaluations": 12 * n + 2, "ms": t_fd, "speedup_adjoint_vs_fd": t_fd / t_adj,
+                                  "step_px": step_p, "step_m": step_h,
+                                  "rel_err_params_vs_gpu_fd": rel_p, "rel_err_height_direction_vs_gpu_fd": rel_h}}
+    if not compact:
+        # e2e: the public autograd API, pinned H2D of params and dh, D2H of both gradients
+        ph, hh = params.cpu().pin_memory(), dh.cpu().pin_memory()
+        gph, ghh = torch.empty_like(ph).pin_memory(), torch.empty_like(hh).pin_memory()
 
-    def e2e_step():
-        p_ = ph.to(dev, non_blocking=True).requires_grad_(True)
-        h_ = hh.to(dev, non_blocking=True).requires_grad_(True)
-        J = CoherenceObjective.apply(p_, h_, pr)
-        J.backward()
-        gph.copy_(p_.grad, non_blocking=True)
-        ghh.copy_(h_.grad, non_blocking=True)
+        def e2e_step():
+            p_ = ph.to(dev, non_blocking=True).requires_grad_(True)
+            h_ = hh.to(dev, non_blocking=True).requires_grad_(True)
+            J = CoherenceObjective.apply(p_, h_, pr)
+            J.backward()
+            gph.copy_(p_.grad, non_blocking=True)
+            ghh.copy_(h_.grad, non_blocking=True)
 
-    e2e_step()
-    t_e2e = timed(e2e_step, max(3, args.steps // 4))
+        e2e_step()
+        t_e2e = timed(e2e_step, max(3, steps // 4))
+        out["e2e"] = {"value": 1e3 / t_e2e, "unit": "evals/s", "h2d_bytes_per_step": (ph.numel() + hh.numel()) * 4,
+                      "d2h_bytes_per_step": (gph.numel() + ghh.numel()) * 4}
     # refinement: 50 Adam steps from zero
     J0 = float(pr.objective(params, dh))
     a0, b0 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -877,28 +1210,37 @@ def run_adjoint(args):
             e2 += float((ea ** 2 + er ** 2).mean())
         return (e2 / n) ** 0.5
 
-    px = n * L * S
+    out["refinement"] = {"adam_steps": 50, "ms": a0.elapsed_time(b0), "J_start": J0, "J_end": hist[-1],
+                         "offset_rms_px_start": offset_rms(torch.zeros_like(p_est), torch.zeros_like(h_est)),
+                         "offset_rms_px_end": offset_rms(p_est, h_est)}
+    out["burst_px_per_s"] = n * L * S * 1e3 / t_adj
+    out["achieved_gbs"] = 40.0 * n * L * S / (t_adj / 1e3) / 1e9
+    del pr, st, params, dh, gp, gh, d
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_adjoint(args):
+    """The adjoint measurement as its own bench line (metric: adjoint evals/s)."""
+    import torch
+    rank, world, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", local)
+    clocks = Clocks(local)
+    clocks.start()
+    m = adjoint_measure(dev, args.steps, world)
+    clk = clocks.stop()
     line = {
         "metric": "adjoint evals/s (dJ/d offset polynomials and height field, J = -mean multilooked coherence)",
-        "value": 1e3 / t_adj, "unit": "evals/s", "n_gpus": world, "steps": args.steps, "warmup": warm,
-        "ms_per_step": t_adj, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 (f64 geometry and reductions)", "data": "synthetic",
-        "config": {"workload": f"{n} bursts of {L} x {S} complex64, offset polynomials (6 per burst, N(0, 0.05 px)) "
-                               f"and a height-error field (10 m rms, 31-px Gaussian); looks {st.rowlook} x "
-                               f"{st.collook}; fused resample -> crossmul -> multilook -> coherence -> gradient",
+        "value": m["evals_per_s"], "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": m["gradient_ms"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 geometry and reductions)", "data": "synthetic",
+        "config": {"workload": m["workload"] + "; fused resample -> crossmul -> multilook -> coherence -> gradient",
                    "l2": "inputs larger than L2", "parallelism": f"replicas{world}"},
-        "forward_ms": t_fwd, "burst_px_per_s": px * 1e3 / t_adj,
-        "finite_differences": {"evaluations": 12 * n + 2, "ms": t_fd, "speedup_adjoint_vs_fd": t_fd / t_adj,
-                               "step_px": step_p, "step_m": step_h,
-                               "rel_err_params_vs_gpu_fd": rel_p, "rel_err_height_direction_vs_gpu_fd": rel_h},
-        "refinement": {"adam_steps": 50, "ms": a0.elapsed_time(b0), "J_start": J0, "J_end": hist[-1],
-                       "offset_rms_px_start": offset_rms(torch.zeros_like(p_est), torch.zeros_like(h_est)),
-                       "offset_rms_px_end": offset_rms(p_est, h_est)},
-        "e2e": {"value": 1e3 / t_e2e, "unit": "evals/s", "h2d_bytes_per_step": (ph.numel() + hh.numel()) * 4,
-                "d2h_bytes_per_step": (gph.numel() + ghh.numel()) * 4},
+        "forward_ms": m["forward_ms"], "burst_px_per_s": m["burst_px_per_s"],
+        "finite_differences": m["finite_differences"], "refinement": m["refinement"], "e2e": m["e2e"],
         "gpu_launches": 3 * args.steps,
-        "roofline": {"bound": "fp32", "kernel": "adjoint_kernel<grad>", "note": "FP32 taps: 3 interpolations x 64 "
-                     "complex x real FMA per pixel; HBM bytes 40 B/px", "achieved_gbs": 40.0 * px / (t_adj / 1e3) / 1e9},
+        "roofline": {"bound": "hbm", "kernel": "adjoint_kernel<grad>", "achieved": m["achieved_gbs"], "unit": "GB/s",
+                     "limiter": "FP32 taps: 3 interpolations x 64 complex x real FMA per pixel; HBM bytes 40 B/px"},
     }
     if clk is not None:
         line["clocks"] = clk

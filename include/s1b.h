@@ -200,6 +200,16 @@ int s1b_deramp_ci16(const s1b_burst_plan_t *plan, const void *in, void *out, voi
 int s1b_geo2rdr(const s1b_burst_plan_t *plan, const int16_t *dem, int64_t dem_pitch,
                 const void *deramped, void *out, int32_t *rows, void *stream);
 
+/* Sample coordinates of every pixel of the plan's DEM window as the
+ * geocoding solves them (per-warp orbit patch, line-model seeds, chord
+ * Newton, in the frame's 128-row tiles, every pixel solved): az = line,
+ * rg = sample of the burst, float64 [(win_bottom-win_top) * (win_right-
+ * win_left)] device.  The reference computes them in-register and never
+ * writes them (azoff/rgoff of reproject, csrc/src/geo2rdr.cu:197-207); here
+ * they state the geocoding's offset error against an FP64 restatement. */
+int s1b_geo2rdr_grid_offsets(const s1b_burst_plan_t *plan, const int16_t *dem, int64_t dem_pitch,
+                             double *az, double *rg, void *stream);
+
 /* Culling of geocoding work outside the burst's valid lines, on by default,
  * for every later s1b_geo2rdr and frame launch in the process (a frame's
  * captured graph keeps the setting it was captured with).  Blocks of 32

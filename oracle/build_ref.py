@@ -15,7 +15,10 @@ Outputs
     system ``libsqlite3.so.0`` through the prototype-only header in
     ``oracle/ref_shim/``.  They run on the B200 box only.
 
-Usage: ``python oracle/build_ref.py [--reference DIR] [--geom-only]``.
+Usage: ``python oracle/build_ref.py [--reference DIR] [--geom-only]``.  The
+reference source tree is the argument, else the ``S1B_REFERENCE_DIR``
+environment variable, else the recipe's default location; when none of them
+holds the sources nothing is built (a prebuilt ``oracle/_ref`` is kept).
 """
 from __future__ import annotations
 
@@ -29,6 +32,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SQLITE_SO = "/usr/lib/x86_64-linux-gnu/libsqlite3.so.0"
+DEFAULT_REFERENCE = "/root/reference"
+
+
+def reference_dir(reference=None):
+    return reference or os.environ.get("S1B_REFERENCE_DIR") or DEFAULT_REFERENCE
 
 
 def _run(cmd, log):
@@ -41,7 +49,8 @@ def _run(cmd, log):
         raise RuntimeError(f"reference build step failed: {' '.join(cmd[:3])} ... (see {log.name})")
 
 
-def build(reference="/root/reference", geom_only=False, quiet=True):
+def build(reference=None, geom_only=False, quiet=True):
+    reference = reference_dir(reference)
     src = os.path.join(reference, "csrc", "src")
     inc = os.path.join(reference, "csrc", "include")
     if not os.path.isdir(src):
@@ -72,7 +81,7 @@ def build(reference="/root/reference", geom_only=False, quiet=True):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=None)
     ap.add_argument("--geom-only", action="store_true")
     a = ap.parse_args()
     ok = build(a.reference, a.geom_only)

@@ -277,6 +277,31 @@ def reproject(dem_win: np.ndarray, deramped: np.ndarray, radar: Radar, orbit, bu
     return out
 
 
+def window_offsets(dem_win: np.ndarray, rows, radar: Radar, orbit, burst: BurstMeta, latmax0: float,
+                   lonmin0: float, dlat: float, dlon: float):
+    """(azoff, rgoff) float64 [len(rows), ncol] of the given rows of a DEM
+    window, as reproject forms them (geo2rdr.cu:195-207: llh2xyz at
+    lat = latmax0 + row dlat, lon = lonmin0 + col dlon, orbitrangetime seeded
+    at the burst centre, then the line and sample of tline and |dr|)."""
+    tt, xx, vv = orbit
+    rows = np.asarray(rows, dtype=np.int64)
+    ncol = dem_win.shape[1]
+    L = radar.lines_per_burst
+    tstart = burst.azimuth_time
+    dtaz = 1.0 / radar.prf
+    tmid = (tstart + (tstart + (L - 1) * dtaz)) * 0.5
+    rngstart = radar.slant_range_time * SOL / 2.0
+    dmrg = SOL / 2.0 / radar.range_sampling_rate
+    xmid, vmid = geo.intp_orbit(tt, xx, vv, np.float64(tmid))
+    lat = np.broadcast_to((latmax0 + rows.astype(np.float64) * dlat)[:, None], (len(rows), ncol))
+    lon = np.broadcast_to((lonmin0 + np.arange(ncol, dtype=np.float64) * dlon)[None, :], (len(rows), ncol))
+    h = dem_win[rows].astype(np.float64)
+    xyz = geo.llh2xyz(np.stack([lat, lon, h], axis=-1))
+    tline, dr, _ = geo.orbitrangetime(tt, xx, vv, xyz, tmid, xmid, vmid)
+    rngpix = np.sqrt(dr[..., 0] * dr[..., 0] + dr[..., 1] * dr[..., 1] + dr[..., 2] * dr[..., 2])
+    return (tline - tstart) / dtaz, (rngpix - rngstart) / dmrg
+
+
 def nonzero_rows(out: np.ndarray):
     """find_nonzero_rows, geo2rdr.cu:86-128 + 273-299: (first, last_excl) or None."""
     nz = np.any((out.real != 0) | (out.imag != 0), axis=1)

@@ -151,67 +151,25 @@ def geo2rdr_buffers_safe(acq, rsc):
     return all(w.nrow * w.ncol <= nrow_buf * ncol_buf for w in wins)
 
 
-def make_reference_safe(sc, steps=4000):
-    """Return ``sc`` with its DEM grid origin shifted by a fraction of a pixel,
-    if needed, so that ``geo2rdr_buffers_safe`` holds for every acquisition
-    (the DEM is regenerated on the shifted grid; the terrain is the same
-    function of latitude/longitude).  Rows and columns are independent: the
-    window is one larger than the buffer along an axis exactly when the
-    fractional parts of the window start and of the footprint extent add up
-    to one or more, so each axis offset is searched on its own."""
-    import dataclasses
-    import math
-
+def footprint_boxes(acq):
+    """Footprint box (latmin, latmax, lonmin, lonmax) of every burst of one
+    geo2rdr run, from the oracle's restatement of bounds (geo2rdr.cu:387-400)."""
     from oracle import geo2rdr as og2
+    r = og2.Radar(**{k: getattr(acq.radar, k) for k in og2.Radar.__dataclass_fields__})
+    return [tuple(float(v) for v in og2.burst_latlon_box(
+        r, acq.orbit, og2.BurstMeta(**{k: getattr(b, k) for k in og2.BurstMeta.__dataclass_fields__})))
+        for b in acq.bursts]
+
+
+def make_reference_safe(sc, acqs=None):
+    """Return ``sc`` on a DEM grid where the reference geo2rdr stays inside its
+    buffers for every acquisition in ``acqs`` (default: all of the scene's),
+    moved by a fraction of a pixel if needed (synth.reference_safe_rsc, fed
+    with the oracle's footprint boxes); the DEM is regenerated there."""
     from sentinel_gpu_processor_b200 import synth
-    acqs = list(sc.ref) + list(sc.sec)
-    if all(geo2rdr_buffers_safe(a, sc.rsc) for a in acqs):
-        return sc
-    boxes = []
-    for acq in acqs:
-        r = og2.Radar(**{k: getattr(acq.radar, k) for k in og2.Radar.__dataclass_fields__})
-        bb = []
-        for b in acq.bursts:
-            bm = og2.BurstMeta(**{k: getattr(b, k) for k in og2.BurstMeta.__dataclass_fields__})
-            bb.append(og2.burst_latlon_box(r, acq.orbit, bm))
-        boxes.append(bb)
-    r0 = sc.rsc
-
-    def axis_ok(origin, step, lo_idx, hi_idx, flip):
-        for bb in boxes:
-            buf = max(int((b[hi_idx] - b[lo_idx]) / abs(step) + 1) for b in bb)
-            for b in bb:
-                if flip:  # latitude: top = int((latmax - origin)/dlat), bottom from latmin
-                    a0 = int((b[1] - origin) / step)
-                    a1 = int((b[0] - origin) / step + 1)
-                else:     # longitude: left from lonmin, right from lonmax
-                    a0 = int((b[2] - origin) / step)
-                    a1 = int((b[3] - origin) / step + 1)
-                if a1 - a0 > buf:
-                    return False
-        return True
-
-    def search(origin0, step, lo_idx, hi_idx, flip, sign):
-        for k in range(steps):
-            v = float("{0:.14f}".format(origin0 + sign * (k / steps) * abs(step)))
-            if axis_ok(v, step, lo_idx, hi_idx, flip):
-                return v
-        return None
-
-    # the footprints' fractional extents depend on the spacing: when no
-    # origin works for every acquisition, stretch the grid by parts per million
-    for m in range(400):
-        f = float("{0:.14f}".format(1.0 + 1e-5 * m))
-        dlat = float("{0:.14f}".format(r0.dlat * f))
-        dlon = float("{0:.14f}".format(r0.dlon * f))
-        lat = search(r0.latmax, dlat, 0, 1, True, +1)
-        lon = search(r0.lonmin, dlon, 2, 3, False, -1)
-        if lat is not None and lon is not None:
-            break
-    else:
-        raise RuntimeError("no DEM grid keeps the reference geo2rdr buffers in bounds")
-    r = formats.Rsc(r0.nlat, r0.nlon, lat, lon, dlat, dlon)
-    if not all(geo2rdr_buffers_safe(a, r) for a in acqs):
-        raise RuntimeError("reference buffer check disagrees with the axis search")
-    dem = synth.make_dem(r, sc.seed, sc.extra["hmax"], device=sc.dem.device)
-    return dataclasses.replace(sc, rsc=r, dem=dem)
+    acqs = list(sc.ref) + list(sc.sec) if acqs is None else list(acqs)
+    rsc = synth.reference_safe_rsc(sc.rsc, [footprint_boxes(a) for a in acqs])
+    out = synth.regrid(sc, rsc)
+    if not all(geo2rdr_buffers_safe(a, out.rsc) for a in acqs):
+        raise RuntimeError("reference buffer check disagrees with the grid search")
+    return out

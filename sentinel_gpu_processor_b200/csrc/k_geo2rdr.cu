@@ -279,7 +279,7 @@ __device__ __forceinline__ GeoConsts geo_consts(const PL &P) {
 // hit L2, and give the line model that seeds and culls the pixel solves.
 // Lane 0 writes the patch to zd and the seed model to seed; the result has
 // bit j set when block j of 32 tile rows is culled.
-template <int RY, typename TSrc, typename PL>
+template <int RY, typename TSrc, typename PL, bool kPrefetch = true>
 __device__ __forceinline__ unsigned geo_warp_setup(const PL &P, const s1b_orbit_poly_t &orbit,
                                                    const int16_t *__restrict__ dem, int64_t pitch,
                                                    const TSrc *__restrict__ burst, int row0, int rT,
@@ -349,7 +349,7 @@ __device__ __forceinline__ unsigned geo_warp_setup(const PL &P, const s1b_orbit_
     const int l0 = max(0, (int)fmax(a0 - 2.0, -1.0)), l1 = min(P.lines - 1, (int)fmin(a1 + 3.0, 1e9));
     const int s0 = max(0, (int)fmax(g0 - 2.0, -1.0)), s1 = min(P.samples - 1, (int)fmin(g1 + 3.0, 1e9));
     const int nl = l1 - l0 + 1;
-    if (nl > 0 && nl <= 3 * RY && s1 >= s0 && s1 - s0 < 256) {
+    if (kPrefetch && nl > 0 && nl <= 3 * RY && s1 >= s0 && s1 - s0 < 256) {
       const int nch = (((s1 - s0 + 1) * (int)sizeof(TSrc)) + 127) / 128 + 1;  // 128-byte lines per line segment
       for (int k = lane; k < nl * nch; k += 32) {
         const int li = k / nch, ch = k - li * nch;
@@ -562,6 +562,60 @@ __global__ __launch_bounds__(G_TX) void geo2rdr_kernel(
     const float2 *__restrict__ burst, float2 *__restrict__ out, int32_t *__restrict__ rows,
     int nrow, int ncol, bool cull) {
   geo2rdr_tile<G_TX, G_RY>(P, P.orbit, dem, pitch, burst, out, rows, nrow, ncol, blockIdx.x, blockIdx.y, cull);
+}
+
+// Zero-Doppler sample coordinates of every DEM pixel of a burst's window, as
+// the geocoding solves them: the same per-warp orbit patch, line-model seeds
+// and chord Newton (geo_warp_setup, zero_doppler_point, zero_doppler_solve)
+// in tiles of kFrameGeoRows rows, as the frame's geocoding, with no culling
+// and no gathers.  az = line (geo2rdr.cu:205-207 azoff), rg = sample (rgoff),
+// float64 [nrow * ncol].
+template <int TX, int RY>
+__global__ __launch_bounds__(TX) void geo2rdr_grid_offsets_kernel(const __grid_constant__ s1b_burst_plan_t P,
+                                                                  const int16_t *__restrict__ dem, int64_t pitch,
+                                                                  double *__restrict__ az, double *__restrict__ rg,
+                                                                  int nrow, int ncol) {
+  const int tx = threadIdx.x, lane = tx & 31, wid = tx >> 5;
+  const int col = blockIdx.x * TX + tx, row0 = blockIdx.y * RY;
+  double r_sin = 0.0, r_cos = 0.0, r_re = 0.0;
+  auto row_terms = [&](int r) {
+    const double lat = (P.lat0 + (row0 + r + lane) * P.dlat) * kPiD / 180;
+    sincos(lat, &r_sin, &r_cos);
+    r_re = kRaD / sqrt(1. - kRe2D * r_sin * r_sin);
+  };
+  row_terms(0);
+  double sinlon, coslon;
+  sincos((P.lon0 + col * P.dlon) * kPiD / 180, &sinlon, &coslon);
+  const bool colok = col < ncol;
+  const GeoConsts gc = geo_consts(P);
+  __shared__ ZeroDopplerPatch s_zd[TX / 32];
+  __shared__ double4 s_seed[TX / 32];
+  const int c0 = blockIdx.x * TX + wid * 32;
+  const int rmax = min(RY, nrow - row0);
+  geo_warp_setup<RY, float2, s1b_burst_plan_t, false>(P, P.orbit, dem, pitch, nullptr, row0, row0, row0 + rmax - 1,
+                                                      min(c0, ncol - 1), min(c0 + 31, ncol - 1), false, s_zd[wid],
+                                                      s_seed[wid]);
+  __syncwarp();
+  const ZeroDopplerPatch &zd = s_zd[wid];
+  const double4 m = s_seed[wid];
+  double inv_c1 = 0.0;
+  for (int r = 0; r < rmax; ++r) {
+    if ((r & 31) == 0 && r > 0) row_terms(r);
+    const double sinlat = __shfl_sync(0xffffffffu, r_sin, r & 31);
+    const double coslat = __shfl_sync(0xffffffffu, r_cos, r & 31);
+    const double re = __shfl_sync(0xffffffffu, r_re, r & 31);
+    if (!colok) continue;
+    const double hgt = i32_to_f64(__ldg(dem + (int64_t)(row0 + r) * pitch + col));
+    double p[3];
+    llh_point(sinlat, coslat, re, sinlon, coslon, hgt, p);
+    const ZeroDopplerPoint q = zero_doppler_point(zd, p);
+    if ((r & 31) == 0) inv_c1 = rcp_newton(q.c1);
+    double h = fma(m.w, hgt, fma(m.z, i32_to_f64(r), fma(m.y, i32_to_f64(col), m.x)));
+    const double rng = sqrt_heron(zero_doppler_solve(q, zd.c3, inv_c1, h));
+    const size_t o = (size_t)(row0 + r) * ncol + col;
+    az[o] = (zd.t0 + h - P.tstart) * gc.prf;
+    rg[o] = (rng - P.rngstart) * gc.inv_dmrg;
+  }
 }
 
 // ------------------------------------------------------------ frame stages
@@ -1078,6 +1132,21 @@ extern "C" int s1b_geo2rdr(const s1b_burst_plan_t *plan, const int16_t *dem, int
   if (grid.y > 65535) return s1b_fail(S1B_ERR_TOO_LARGE, "s1b_geo2rdr: DEM window too tall");
   geo2rdr_kernel<<<grid, G_TX, 0, st>>>(*plan, dem, dem_pitch, (const float2 *)deramped,
                                          (float2 *)out, rows, nrow, ncol, g_cull_geo != 0);
+  return s1b_launch_status();
+}
+
+extern "C" int s1b_geo2rdr_grid_offsets(const s1b_burst_plan_t *plan, const int16_t *dem, int64_t dem_pitch,
+                                        double *az, double *rg, void *stream) {
+  if (!plan || !dem || !az || !rg) return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_geo2rdr_grid_offsets: null argument");
+  const int nrow = plan->win_bottom - plan->win_top;
+  const int ncol = plan->win_right - plan->win_left;
+  if (nrow <= 0 || ncol <= 0) return s1b_fail(S1B_ERR_EMPTY, "s1b_geo2rdr_grid_offsets: empty DEM window");
+  if (dem_pitch < ncol)
+    return s1b_fail(S1B_ERR_INVALID_ARGUMENT, "s1b_geo2rdr_grid_offsets: dem_pitch < window width");
+  dim3 grid((ncol + G_TX - 1) / G_TX, (nrow + kFrameGeoRows - 1) / kFrameGeoRows);
+  if (grid.y > 65535) return s1b_fail(S1B_ERR_TOO_LARGE, "s1b_geo2rdr_grid_offsets: DEM window too tall");
+  geo2rdr_grid_offsets_kernel<G_TX, kFrameGeoRows><<<grid, G_TX, 0, (cudaStream_t)stream>>>(*plan, dem, dem_pitch,
+                                                                                             az, rg, nrow, ncol);
   return s1b_launch_status();
 }
 

@@ -93,6 +93,28 @@ def geo2rdr(plan: _lib.BurstPlan, dem: torch.Tensor, deramped: torch.Tensor, out
     return out, rows
 
 
+def geo2rdr_grid_offsets(plan: _lib.BurstPlan, dem: torch.Tensor):
+    """Burst line and sample (float64 [nrow, ncol] each) of every pixel of the
+    plan's DEM window, solved as the geocoding solves them
+    (``s1b_geo2rdr_grid_offsets``).  ``dem``: the full RSC-grid DEM or the
+    window itself (int16)."""
+    _need_cuda(dem)
+    if dem.dtype != torch.int16:
+        raise ValueError("dem must be int16")
+    nrow, ncol = plan.nrow, plan.ncol
+    if nrow <= 0 or ncol <= 0:
+        raise _lib.S1BError(_lib.S1B_ERR_EMPTY, "geo2rdr_grid_offsets")
+    win = dem[plan.win_top:plan.win_bottom, plan.win_left:plan.win_right] \
+        if dem.shape == (plan.rsc_nlat, plan.rsc_nlon) else dem
+    if tuple(win.shape) != (nrow, ncol) or win.stride(1) != 1:
+        raise ValueError("dem does not cover the plan's window")
+    az = torch.empty((nrow, ncol), dtype=torch.float64, device=dem.device)
+    rg = torch.empty_like(az)
+    _lib.check(_lib.load().s1b_geo2rdr_grid_offsets(ctypes.byref(plan), _lib.dptr(win), win.stride(0), _lib.dptr(az),
+                                                    _lib.dptr(rg), _lib.stream_ptr()), "s1b_geo2rdr_grid_offsets")
+    return az, rg
+
+
 def set_geocode_culling(on: bool) -> bool:
     """Switch the geocoding's culling of blocks outside the burst's valid
     lines for later geo2rdr and frame launches of the process (on by default;

@@ -103,3 +103,10 @@ def crossmul_box(h1, h2, rowlook, collook, use_union=False):
         return None, list(hdr)
     _lib.check(st, "s1b_crossmul_box")
     return list(box), list(hdr)
+
+
+def footprint_boxes(acq):
+    """Footprint box (latmin, latmax, lonmin, lonmax) of every burst of an
+    acquisition (the burst bounds of geo2rdr.cu:387-400), from the planner."""
+    return [tuple(float(v) for v in burst_plan(acq.radar, acq.orbit, acq.fm, acq.dc, b, None).latlon_box)
+            for b in acq.bursts]

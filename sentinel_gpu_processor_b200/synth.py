@@ -423,11 +423,15 @@ def make_pair(config="c0", seed=20261203, device="cpu", baseline=150.0, coherenc
 def make_frame(seed=20261203, device="cpu", n_swaths=3, n_bursts=9, baseline=150.0,
                line_range=(1480, 1530), sample_range=(20000, 25500), overlap=100,
                kt_range=(-1700.0, -1400.0), coh_range=(0.3, 0.9), rowlook=4, collook=20,
-               alpha=0.5, hmax=3000.0, scale=1.0):
+               alpha=0.5, hmax=3000.0, scale=1.0, slc_pairs=None, with_dem=True):
     """A full IW frame: ``n_swaths`` x ``n_bursts`` bursts of uneven size.
 
     Each burst is its own Acquisition (the reference handles one burst size
     per subswath run).  ``scale`` shrinks line/sample counts for tests.
+    ``slc_pairs``: make the SLCs of the first ``slc_pairs`` burst pairs only
+    (the others are None); they are the same values as in the whole frame,
+    since the speckle of the pairs is drawn in order from one generator.
+    ``with_dem=False`` leaves the DEM out (geometry only).
     """
     import torch
     rng = np.random.Generator(np.random.PCG64(seed))
@@ -455,21 +459,134 @@ def make_frame(seed=20261203, device="cpu", n_swaths=3, n_bursts=9, baseline=150
             ref = Acquisition(radar=radar, orbit=orbit_ref, fm=fm, dc=dc, bursts=[burst])
             sec = Acquisition(radar=radar, orbit=orbit_sec, fm=fm.copy(), dc=dc.copy(), bursts=[burst])
             g = float(rng.uniform(*coh_range))
-            s_ref = speckle(L, S, gen, device)
-            noise = speckle(L, S, gen, device)
-            s_sec = g * s_ref + math.sqrt(1 - g * g) * noise
+            if slc_pairs is None or len(refs) < slc_pairs:
+                s_ref = speckle(L, S, gen, device)
+                noise = speckle(L, S, gen, device)
+                s_sec = g * s_ref + math.sqrt(1 - g * g) * noise
+                ref_slc.append(tops_modulate(s_ref, ref, burst).contiguous())
+                sec_slc.append(tops_modulate(s_sec, sec, burst).contiguous())
+                del s_ref, noise, s_sec
+            else:
+                ref_slc.append(None)
+                sec_slc.append(None)
             refs.append(ref)
             secs.append(sec)
-            ref_slc.append(tops_modulate(s_ref, ref, burst).contiguous())
-            sec_slc.append(tops_modulate(s_sec, sec, burst).contiguous())
             cohs.append(g)
             t += (L - int(overlap * scale)) * AZIMUTH_INTERVAL
             acq_dur = max(acq_dur, t)
     rsc = footprint_rsc(refs + secs, 0.0, hmax, margin=0.02)
-    dem = make_dem(rsc, seed, hmax, device=device)
+    dem = make_dem(rsc, seed, hmax, device=device) if with_dem else None
     return PairScene(name="frame", seed=seed, ref=refs, sec=secs, rsc=rsc, dem=dem, ref_slc=ref_slc,
                      sec_slc=sec_slc, rowlook=rowlook, collook=collook, alpha=alpha,
                      extra={"coherence": cohs, "hmax": hmax})
+
+
+def _window(box, rsc):
+    """DEM window [left, top, right, bottom) of a footprint box (latmin,
+    latmax, lonmin, lonmax) on an RSC grid: C int() truncation of each end
+    (csrc/src/geo2rdr.cu:569-586), unclamped."""
+    latmin, latmax, lonmin, lonmax = box
+    return (int((lonmin - rsc.lonmin) / rsc.dlon), int((latmax - rsc.latmax) / rsc.dlat),
+            int((lonmax - rsc.lonmin) / rsc.dlon + 1), int((latmin - rsc.latmax) / rsc.dlat + 1))
+
+
+def reference_geo2rdr_fits(boxes, rsc):
+    """True when the reference geo2rdr's buffers hold every burst window of
+    one run.  ``boxes``: the footprint boxes of the bursts of one geo2rdr run.
+
+    geo2rdr.cu:408-423 sizes its host DEM buffer and device output as
+    ``int((latmin - latmax)/dlat + 1) x int((lonmax - lonmin)/dlon + 1)`` (max
+    over the bursts) while each burst window (569-586) truncates its two ends
+    separately and can be one row or column larger; both buffers are flat, so
+    the element count must fit."""
+    nrow_buf = max(int((b[0] - b[1]) / rsc.dlat + 1) for b in boxes)
+    ncol_buf = max(int((b[3] - b[2]) / rsc.dlon + 1) for b in boxes)
+    for b in boxes:
+        l, t, r, bt = _window(b, rsc)
+        l, t, r, bt = max(0, l), max(0, t), min(rsc.nlon, r), min(rsc.nlat, bt)
+        if (bt - t) * (r - l) > nrow_buf * ncol_buf:
+            return False
+    return True
+
+
+def _axis_terms(b, origin, step, lat):
+    """The three C int() arguments of one axis of a burst's footprint: the
+    buffer extent (geo2rdr.cu:408-423) and the window's two ends (569-586)."""
+    if lat:
+        return (b[0] - b[1]) / step + 1, (b[1] - origin) / step, (b[0] - origin) / step + 1
+    return (b[3] - b[2]) / step + 1, (b[2] - origin) / step, (b[3] - origin) / step + 1
+
+
+def reference_safe_rsc(rsc, runs, steps=4000, margin=1e-6):
+    """An RSC grid on which the reference geo2rdr stays inside its buffers
+    for every run in ``runs`` (a list of footprint-box lists, one per geo2rdr
+    run): ``rsc`` itself when it already is, else ``rsc`` with its origin
+    moved by a fraction of a pixel (and, when no origin serves every run, its
+    spacing stretched by parts per million).  Along each axis the window
+    exceeds the buffer exactly when the fractional parts of the window start
+    and of the footprint extent add up to one or more, so each axis offset is
+    searched on its own.
+
+    A grid is only taken when every int() argument of the windows and
+    buffers lies at least ``margin`` pixels from an integer, so the choice is
+    the same for footprint boxes that differ in the last bits (the library's
+    planner evaluates the orbit through its polynomials, a restatement of
+    the reference through the Hermite form).  The values go through the RSC
+    text form, as the reference reads them."""
+    import math
+
+    def robust(x):
+        f = x - math.floor(x)
+        return margin < f < 1.0 - margin
+
+    def axis_ok(origin, step, lat):
+        for bb in runs:
+            terms = [_axis_terms(b, origin, step, lat) for b in bb]
+            if not all(robust(x) for t in terms for x in t):
+                return False
+            buf = max(int(t[0]) for t in terms)
+            if max(int(t[2]) - int(t[1]) for t in terms) > buf:
+                return False
+        return True
+
+    def search(origin0, step, lat, sign):
+        for k in range(steps):
+            v = float("{0:.14f}".format(origin0 + sign * (k / steps) * abs(step)))
+            if axis_ok(v, step, lat):
+                return v
+        return None
+
+    for m in range(400):
+        f = float("{0:.14f}".format(1.0 + 1e-5 * m))
+        dlat = float("{0:.14f}".format(rsc.dlat * f)) if m else rsc.dlat
+        dlon = float("{0:.14f}".format(rsc.dlon * f)) if m else rsc.dlon
+        lat = search(rsc.latmax, dlat, True, +1)
+        lon = search(rsc.lonmin, dlon, False, -1)
+        if lat is not None and lon is not None:
+            out = formats.rsc_roundtrip(formats.Rsc(rsc.nlat, rsc.nlon, lat, lon, dlat, dlon))
+            if out == rsc or all(reference_geo2rdr_fits(bb, out) for bb in runs):
+                return out
+    raise RuntimeError("no DEM grid keeps the reference geo2rdr buffers in bounds")
+
+
+def regrid(sc: PairScene, rsc) -> PairScene:
+    """``sc`` on another RSC grid: the DEM regenerated there (the terrain is
+    the same function of latitude and longitude)."""
+    import dataclasses
+    if rsc == sc.rsc:
+        return sc
+    dev = sc.dem.device if sc.dem is not None else "cpu"
+    return dataclasses.replace(sc, rsc=rsc, dem=make_dem(rsc, sc.seed, sc.extra["hmax"], device=dev))
+
+
+def on_reference_safe_grid(sc: PairScene, boxes_of, pairs=(0,)) -> PairScene:
+    """``sc`` on a DEM grid where the reference geo2rdr, run on each burst of
+    the given pairs, stays inside its buffers (``reference_safe_rsc``);
+    ``boxes_of(acq)`` gives an acquisition's footprint boxes (the library's
+    planner, ``plan.footprint_boxes``, or any restatement of the reference's
+    bounds that agrees with it bit for bit)."""
+    runs = [boxes_of(a) for k in pairs for a in (sc.ref[k], sc.sec[k])]
+    return regrid(sc, reference_safe_rsc(sc.rsc, runs))
 
 
 def cint16(slc, scale: float = 2000.0):
