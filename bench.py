@@ -821,7 +821,7 @@ def parity_leg(pair, dem_host, rsc, looks, alpha, plans, dem_dev):
     # coherence: pixels where neither side takes the > 1 fill (seeded here,
     # unseeded rand() in the reference)
     with np.errstate(divide="ignore", invalid="ignore"):
-        raw = np.abs(ifg_c.astype(np.float64)) / (a1_c + 1e-12) / (a2_c + 1e-12)
+        raw = np.abs(ifg_c.astype(np.complex128)) / (a1_c + 1e-12) / (a2_c + 1e-12)
     m = both & np.isfinite(wc_c) & (wc_c <= 1.0) & (raw <= 1.0)
     out["max_dcoh"] = float(np.abs(coh_c[m] - wc_c[m]).max()) if m.any() else None
     if out["ifg_header_equal"]:

@@ -310,6 +310,15 @@ int s1b_resample(const s1b_burst_plan_t *plan, const void *sec, const float *az_
                  const float *rg_off, int32_t lines, int32_t samples, int32_t interp, void *out,
                  int32_t *status, void *stream);
 
+/* Polls each shared-memory staging wait of the TMA resampler makes before it
+ * gives up, for later s1b_resample calls of the process (default 2^22).  A
+ * wait that gives up sets the call's status word to 1, waits (with the
+ * default limit) for the block's copies in flight and ends the block.  A
+ * test hook for that error path: with 0 every wait gives up at once.  No
+ * reference counterpart.  Returns the previous limit (pass it back to
+ * restore). */
+uint32_t s1b_set_staging_poll_limit(uint32_t polls);
+
 /* Coherence |sum conj(ref) sec| / sqrt(sum |ref|^2 sum |sec|^2) over win x win
  * boxes at full resolution (win odd, <= 9; windows clipped at the raster
  * border), sums compensated in float32.  ref/sec: complex64 [lines *

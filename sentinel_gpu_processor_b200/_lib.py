@@ -149,6 +149,7 @@ _SIGNATURES = {
     "s1b_goldstein": (c_int, [c_void_p, c_void_p, c_int32, c_int32, c_int32, c_float, c_void_p, c_size_t,
                               c_void_p]),
     "s1b_geo2rdr_grid_offsets": (c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_void_p]),
+    "s1b_set_staging_poll_limit": (ctypes.c_uint32, [ctypes.c_uint32]),
     "s1b_goldstein_noalloc": (c_int, [c_void_p, c_void_p, c_int32, c_int32, c_int32, c_float, c_void_p]),
     "s1b_amp_looks": (c_int, [c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32, c_int32, c_int32, c_int32,
                               c_int32, c_void_p, c_void_p]),

@@ -161,8 +161,8 @@ __device__ __forceinline__ uint32_t smem_addr(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (uint32_t i = 0; i < kSpinLimit; ++i) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint32_t limit = kSpinLimit) {
+  for (uint32_t i = 0; i < limit; ++i) {
     uint32_t done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
@@ -562,7 +562,8 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap &m, int
 __global__ __launch_bounds__(RT_THREADS, 2) void resample_tma_kernel(
     const __grid_constant__ s1b_burst_plan_t P, const __grid_constant__ CUtensorMap tsec,
     const __grid_constant__ CUtensorMap taz, const __grid_constant__ CUtensorMap trg, const float2 *__restrict__ sec,
-    int L, int S, int sinc, int ntx, int ntiles, float2 *__restrict__ out, int *__restrict__ status) {
+    int L, int S, int sinc, int ntx, int ntiles, float2 *__restrict__ out, int *__restrict__ status,
+    uint32_t poll_limit) {
   extern __shared__ __align__(1024) unsigned char rt_raw[];
   RtSmem &sm = *reinterpret_cast<RtSmem *>(rt_raw);
   const int tid = threadIdx.x, tx = tid % R_TX, ty = tid / R_TX, lane = tid % 32, warp = tid / 32;
@@ -623,7 +624,7 @@ __global__ __launch_bounds__(RT_THREADS, 2) void resample_tma_kernel(
   // issue its window and the offsets of tile j + 1.  Returns false on a
   // failed wait (uniform over the block).
   auto prepare = [&](int j, Window &w) -> bool {
-    const bool ok_wait = mbar_wait(smem_addr(&sm.bar_off[j % 3]), (j / 3) & 1);
+    const bool ok_wait = mbar_wait(smem_addr(&sm.bar_off[j % 3]), (j / 3) & 1, poll_limit);
     if (tid == 0 && ok_wait) pending &= ~(1u << (j % 3));
     int mna = INT_MAX, xna = INT_MIN, mnr = INT_MAX, xnr = INT_MIN;
     if (ok_wait) {
@@ -693,7 +694,7 @@ __global__ __launch_bounds__(RT_THREADS, 2) void resample_tma_kernel(
     const int s = i & 1;
     bool ok_wait = true;
     if (cur.staged) {
-      ok_wait = mbar_wait(smem_addr(&sm.bar_win[s]), (wphase >> s) & 1);
+      ok_wait = mbar_wait(smem_addr(&sm.bar_win[s]), (wphase >> s) & 1, poll_limit);
       if (ok_wait) {
         wphase ^= 1u << s;
         if (tid == 0) pending &= ~(8u << s);
@@ -1182,6 +1183,17 @@ extern "C" int s1b_geo2rdr_offsets_dh(const s1b_burst_plan_t *plan, const s1b_bu
   return s1b_launch_status();
 }
 
+// Polls of each staging wait of the TMA resampler before it gives up
+// (s1b_set_staging_poll_limit; the drain after a failed wait always uses
+// kSpinLimit, so every copy in flight lands before the block exits).
+static uint32_t g_stage_poll_limit = kSpinLimit;
+
+extern "C" uint32_t s1b_set_staging_poll_limit(uint32_t polls) {
+  const uint32_t prev = g_stage_poll_limit;
+  g_stage_poll_limit = polls;
+  return prev;
+}
+
 extern "C" int s1b_resample(const s1b_burst_plan_t *plan, const void *sec, const float *az_off,
                             const float *rg_off, int32_t lines, int32_t samples, int32_t interp, void *out,
                             int32_t *status, void *stream) {
@@ -1208,7 +1220,7 @@ extern "C" int s1b_resample(const s1b_burst_plan_t *plan, const void *sec, const
     const int grid = (int)std::min<long long>(ntiles, slots);
     resample_tma_kernel<<<grid, RT_THREADS, sizeof(RtSmem), st>>>(*plan, msec, maz, mrg, (const float2 *)sec, lines,
                                                                   samples, sinc, ntx, (int)ntiles, (float2 *)out,
-                                                                  status);
+                                                                  status, g_stage_poll_limit);
     return s1b_launch_status();
   }
   dim3 block(R_TX, R_TY);
