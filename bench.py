@@ -1002,6 +1002,97 @@ def _repo_libraries_mapped():
     return sorted(p for p in paths if p.startswith(ROOT) and "baseline/_ref" not in p)
 
 
+def _kbench_inputs(wd, sc, dem, slcs):
+    """Inputs of the reference's kernels for burst pair 0, for the
+    kernel-only harness (oracle/_ref/bin/kbench_chain): the host-side values
+    the reference geo2rdr computes before its launches (geo2rdr.cu:469-613),
+    from the oracle's restatement of them, and the raw arrays.  Returns the
+    manifest entries (the crossmul box is added once the reference has run)."""
+    import numpy as np
+
+    from oracle import geo2rdr as og2
+    from oracle import geometry as og
+    m = {}
+    r = sc.rsc
+    orsc = og2.Rsc(nlat=r.nlat, nlon=r.nlon, latmax=r.latmax, lonmin=r.lonmin, dlat=r.dlat, dlon=r.dlon)
+    for tag, acq in (("ref", sc.ref[0]), ("sec", sc.sec[0])):
+        rad = og2.Radar(**{k: getattr(acq.radar, k) for k in og2.Radar.__dataclass_fields__})
+        b = og2.BurstMeta(**{k: getattr(acq.bursts[0], k) for k in og2.BurstMeta.__dataclass_fields__})
+        co = og2.burst_coefficients(rad, acq.orbit, acq.fm, acq.dc, b)
+        w = og2.dem_window(og2.burst_latlon_box(rad, acq.orbit, b), orsc)
+        tt, xx, vv = (np.ascontiguousarray(a, dtype=np.float64) for a in acq.orbit)
+        L, S = rad.lines_per_burst, rad.samples_per_burst
+        dtaz = 1.0 / rad.prf
+        tstart = b.azimuth_time
+        tmid = (tstart + (tstart + (L - 1) * dtaz)) * 0.5
+        xmid, vmid = og.intp_orbit(tt, xx, vv, np.float64(tmid))
+        p = f"{tag}_"
+        arrays = {"slc": np.ascontiguousarray(slcs[tag], dtype=np.complex64), "kt": co.kt, "etaref": co.etaref,
+                  "eta": co.eta, "tt": tt, "xx": xx, "vv": vv,
+                  "dem": np.ascontiguousarray(dem[w.top:w.bottom, w.left:w.right], dtype=np.int16)}
+        for name, a in arrays.items():
+            path = os.path.join(wd, f"kb_{p}{name}.bin")
+            a.tofile(path)
+            m[p + name] = path
+        m.update({p + "L": L, p + "S": S, p + "nstat": len(tt), p + "nrow": w.nrow, p + "ncol": w.ncol,
+                  p + "win_left": w.left, p + "win_top": w.top, p + "fvl": b.first_valid_line,
+                  p + "lvl": b.last_valid_line, p + "fvs": b.first_valid_sample, p + "lvs": b.last_valid_sample,
+                  p + "tmid": tmid, p + "latmax0": r.latmax + r.dlat * w.top,
+                  p + "lonmin0": r.lonmin + r.dlon * w.left, p + "dlat": r.dlat, p + "dlon": r.dlon,
+                  p + "rngstart": rad.slant_range_time * 299792458.0 / 2.0,
+                  p + "tstart": tstart, p + "dmrg": 299792458.0 / 2.0 / rad.range_sampling_rate, p + "dtaz": dtaz,
+                  p + "etac0": co.etac0, p + "ks": co.ks, p + "wvl": rad.wvl})
+        for i in range(4):
+            m[p + f"fm{i}"] = co.fm[i]
+            m[p + f"dc{i}"] = co.dc[i]
+        for i in range(3):
+            m[p + f"xmid{i}"] = float(xmid[i])
+            m[p + f"vmid{i}"] = float(vmid[i])
+    return m
+
+
+def _kbench_run(wd, m, ifg_header, looks, alpha, burst_px, reps=5):
+    """The reference's kernels on device-resident inputs (kernel-only
+    harnesses oracle/_ref/bin/kbench_chain and kbench_goldstein, built from
+    its sources): per-kernel median times for burst pair 0 and the rate they
+    give in burst pixels per second."""
+    import numpy as np
+
+    from oracle import refrun
+    rl, cl = looks
+    h = ifg_header
+    m = dict(m, box_left=int(h[2]) * cl, box_top=int(h[3]) * rl, box_right=int(h[4]) * cl,
+             box_bottom=int(h[5]) * rl, rowlook=rl, collook=cl)
+    man = os.path.join(wd, "kbench_manifest.txt")
+    with open(man, "w") as f:
+        for k, v in m.items():
+            if isinstance(v, str):
+                f.write(f"{k} {v}\n")
+            elif isinstance(v, (int, np.integer)):
+                f.write(f"{k} {int(v)}\n")
+            else:
+                f.write(f"{k} {float(v)!r}\n")
+    ifg = os.path.join(wd, "kbench_ifg.bin")
+    _, out = refrun.run([os.path.join(refrun.BIN, "kbench_chain"), man, str(reps), ifg])
+    chain = json.loads(out.strip().splitlines()[-1])
+    nr, nc = chain["ifg_shape"]
+    _, out = refrun.run([os.path.join(refrun.BIN, "kbench_goldstein"), ifg, str(nr), str(nc), "32", repr(float(alpha)),
+                         str(reps)])
+    gold = json.loads(out.strip().splitlines()[-1])
+    pair_ms = (sum(chain["deramp_ms"]) + sum(chain["reproject_ms"]) + sum(chain["nonzero_rows_ms"])
+               + chain["crossmul_looks_ms"] + gold["goldstein_ms"])
+    return {"value": burst_px / (pair_ms / 1e3), "unit": UNIT, "pair_ms": pair_ms,
+            "kernels": {"deramp_burst_ms": chain["deramp_ms"], "reproject_ms": chain["reproject_ms"],
+                        "find_nonzero_rows_ms": chain["nonzero_rows_ms"],
+                        "conj_mul_col_row_look_ms": chain["crossmul_looks_ms"],
+                        "goldstein_filter_cuda_host_ms": gold["goldstein_ms"], "cufft_plan_ms": gold["plan_ms"]},
+            "geo_px": chain["geo_px"], "ifg_shape": chain["ifg_shape"], "reps": reps,
+            "how": ("the reference's kernels (sm_100a builds of its geo2rdr.cu, sario.cu, goldstein.cu) on "
+                    "device-resident inputs of burst pair 0, its launch configurations, CUDA events, median of "
+                    f"{reps} after a warm-up; no process start-up, SQLite, file I/O or host copies except the "
+                    "filtered image's copy inside goldstein_filter_cuda_host")}
+
+
 def run_reference(args):
     """The reference's own implementation on the same workload: its CUDA
     executables (sm_100a builds of its sources in oracle/_ref) geo2rdr x 2,
@@ -1058,6 +1149,9 @@ def run_reference(args):
         dbs = {}
         for tag, acq in (("ref", sc.ref[0]), ("sec", sc.sec[0])):
             dbs[tag] = refrun.write_geo2rdr_inputs(wd, tag, acq, [slcs[tag]], rscf, demf)
+        kb_inputs = None
+        if os.path.exists(os.path.join(refrun.BIN, "kbench_chain")):
+            kb_inputs = _kbench_inputs(wd, sc, dem, slcs)
         del dem, slcs
 
         def step():
@@ -1084,6 +1178,13 @@ def run_reference(args):
         for _ in range(args.warmup):
             step()
         times = [step() for _ in range(args.steps)]
+        kernel_only = None
+        if kb_inputs is not None:
+            ih, _ = formats.read_raster(os.path.join(wd, "pair.int"))
+            try:
+                kernel_only = _kbench_run(wd, kb_inputs, ih, (rl, cl), sc.alpha, L * S)
+            except (RuntimeError, OSError, ValueError) as e:
+                kernel_only = {"unavailable": f"kernel-only harness failed: {e}"[:300]}
     finally:
         shutil.rmtree(wd, ignore_errors=True)
     mean = sum(times) / len(times)
@@ -1101,6 +1202,8 @@ def run_reference(args):
         "world_size_requested": world,
         "repo_libraries_mapped": _repo_libraries_mapped(),
     }
+    if kernel_only is not None:
+        line["kernel_only"] = kernel_only
     print(json.dumps(line), flush=True)
 
 

@@ -14,6 +14,9 @@ Outputs
     with the source lists of ``csrc/CMakeLists.txt:67-71``.  geo2rdr links the
     system ``libsqlite3.so.0`` through the prototype-only header in
     ``oracle/ref_shim/``.  They run on the B200 box only.
+  * ``bin/kbench_chain``, ``bin/kbench_goldstein`` -- kernel-only timing
+    harnesses (``oracle/ref_shim/kbench_*.cu``) that include the reference's
+    geo2rdr.cu / goldstein.cu and time its kernels on device-resident inputs.
 
 Usage: ``python oracle/build_ref.py [--reference DIR] [--geom-only]``.  The
 reference source tree is the argument, else the ``S1B_REFERENCE_DIR``
@@ -76,6 +79,15 @@ def build(reference=None, geom_only=False, quiet=True):
                        "-o", os.path.join(OUT, "bin", "crossmul")], log)
         _run(common + [os.path.join(src, "goldstein.cu"), "-lcufft",
                        "-o", os.path.join(OUT, "bin", "goldstein")], log)
+        # kernel-only timing harnesses: the reference's kernels on device-resident
+        # inputs (the harness sources include the reference files where they lie)
+        shim = os.path.join(HERE, "ref_shim")
+        _run(common + ["-rdc=true", "-I" + src, os.path.join(shim, "kbench_chain.cu"),
+                       os.path.join(src, "sql_mod.cpp"), os.path.join(src, "orbit.cu"), os.path.join(src, "sario.cu"),
+                       os.path.join(src, "bounds.cu"), "-Xlinker", SQLITE_SO,
+                       "-o", os.path.join(OUT, "bin", "kbench_chain")], log)
+        _run(common + ["-I" + src, os.path.join(shim, "kbench_goldstein.cu"), "-lcufft",
+                       "-o", os.path.join(OUT, "bin", "kbench_goldstein")], log)
     return True
 
 
