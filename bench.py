@@ -1207,6 +1207,11 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+ADJ_MARGIN = 16      # samples of the burst left out of the refinement grid on every side
+ADJ_STEP_PX = 1e-3   # central-difference step of the offset parameters (samples)
+ADJ_STEP_M = 0.4     # central-difference step along the height-error direction (metres)
+
+
 def adjoint_measure(dev, steps, world, compact=False):
     """Adjoint of the coherence objective on 8 bursts of 1500 x 21000: gradient
     evaluations per second through the fused adjoint, against central finite
@@ -1218,7 +1223,10 @@ def adjoint_measure(dev, steps, world, compact=False):
     from sentinel_gpu_processor_b200 import synth
     from sentinel_gpu_processor_b200.refine import CoherenceObjective, CoregProblem, refine
     n = 8
-    st = synth.make_refine_stack(n_bursts=n, config="c1", seed=20261203 + 3000, device=dev)
+    # the reference grid is the burst's interior (16 samples off every edge):
+    # no pixel's sinc support reaches the secondary burst's edge under the
+    # perturbations, where J would jump as pixels enter or leave the support
+    st = synth.make_refine_stack(n_bursts=n, config="c1", seed=20261203 + 3000, device=dev, margin=ADJ_MARGIN)
     pr = CoregProblem(st.sec_plans, st.ref, st.sec, st.az0, st.rg0, st.daz_dh, st.drg_dh, st.rowlook, st.collook)
     L, S = st.az0.shape[1:]
     params = torch.zeros((n, 6), dtype=torch.float32, device=dev)
@@ -1250,7 +1258,9 @@ def adjoint_measure(dev, steps, world, compact=False):
     gd.manual_seed(11)
     d = synth.gaussian_smooth(torch.randn((n, L, S), generator=gd, device=dev), 31.0)
     d = (d / d.std()).contiguous()
-    step_p, step_h = 1e-3, 1e-1
+    # steps large enough that the float32 forward's rounding in J (~5e-11)
+    # stays below 1e-3 of the difference, small enough for the truncation error
+    step_p, step_h = ADJ_STEP_PX, ADJ_STEP_M
     fd = torch.zeros((n, 6), dtype=torch.float64, device=dev)
     fd_dir = torch.zeros(1, dtype=torch.float64, device=dev)
 

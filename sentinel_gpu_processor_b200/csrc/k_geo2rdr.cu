@@ -328,6 +328,7 @@ __device__ __forceinline__ unsigned geo_warp_setup(const PL &P, const s1b_orbit_
       OrbitCubic oc;
       orbit_cubic(orbit, tc, oc);
       zero_doppler_patch(oc, zd);
+      zd.inv_c1 = rcp_newton(fp);  // f' at the centre point: the chord slope of the warp's pixels
     }
   }
   {
@@ -826,6 +827,96 @@ __global__ __launch_bounds__(TX, kGeoGridMinBlocks<TX>) void frame_geo2rdr_grid_
 // per 27-pair frame).
 constexpr int kXmTX = kFrameXmCols;  // columns per tile
 
+// Both bursts of a pair at one DEM pixel (bit q of MASK: burst q is solved
+// in this block; act[q]: the pixel lies in burst q's window).  The solves
+// are straight-line (zero_doppler_solve2 with the warp patch's chord slope),
+// so the two bursts' instruction streams interleave; gathers are predicated
+// on the validity window.  Fused (raw samples + column table): the TOPS
+// phases of the two gathered lines relative to the pixel's reramp are formed
+// in FP32 from differences that are small by construction: with
+// K = kt, u = eta_line - etaref_c0 and the pixel's eta - etaref = u + w,
+//   kt_p (u + w)^2 - K0 u^2 = K0 w (2u + w) + frd (K1 - K0) (u + w)^2,
+// a few half-cycles, so FP32 keeps them to ~1e-6 half-cycles; only the
+// two-way range phase 4 R / wvl (~6e7 half-cycles) is reduced in FP64.  The
+// phasors use the hardware sine and cosine (~4e-7 rad).  The column rotation
+// of the second sample of a line is likewise
+//   -K1 (u - de)^2 + K0 u^2 = K0 de (2u - de) - (K1 - K0) (u - de)^2.
+template <typename TSrc, bool kFused, int MASK>
+__device__ __forceinline__ void geo_pair_pixel(const PlanTail *sp, const GeoConsts *gc, const ZeroDopplerPatch *zd0,
+                                               const ZeroDopplerPatch *zd1, const double4 *m0, const double4 *m1,
+                                               const double p[3], double hgt, int r, const int *colw,
+                                               const bool *act, const TSrc *__restrict__ src0,
+                                               const TSrc *__restrict__ src1, const double2 *__restrict__ tops0,
+                                               const double2 *__restrict__ tops1, float2 *v) {
+  double h[2], r2[2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    if (!((MASK >> q) & 1)) continue;
+    const ZeroDopplerPatch &z = q ? *zd1 : *zd0;
+    const double4 &m = q ? *m1 : *m0;
+    const ZeroDopplerPoint pt = zero_doppler_point(z, p);
+    h[q] = fma(m.w, hgt, fma(m.z, i32_to_f64(r), fma(m.y, i32_to_f64(colw[q]), m.x)));
+    r2[q] = zero_doppler_solve2(pt, z.c3, z.inv_c1, h[q], act[q]);
+  }
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    v[q] = make_float2(0.f, 0.f);
+    if (!((MASK >> q) & 1)) continue;
+    const PlanTail &P = sp[q];
+    const ZeroDopplerPatch &z = q ? *zd1 : *zd0;
+    const TSrc *burst = q ? src1 : src0;
+    const double rng = sqrt_heron(r2[q]);
+    const double t = z.t0 + h[q];
+    const double rgoff = (rng - P.rngstart) * gc[q].inv_dmrg;
+    const double azoff = (t - P.tstart) * gc[q].prf;
+    // validity window, geo2rdr.cu:208-209, and the 2 x 2 neighbourhood inside the burst
+    bool valid = act[q] && rgoff > P.first_valid_sample && rgoff < P.last_valid_sample - 1 &&
+                 azoff >= P.first_valid_line + 5 && azoff < P.last_valid_line - 5;
+    const int intr = valid ? (int)rgoff : 0, inta = valid ? (int)azoff : 0;
+    valid = valid && intr >= 0 && intr + 1 < P.samples && inta >= 0 && inta + 1 < P.lines;
+    if (!valid) continue;
+    const double frd = rgoff - i32_to_f64(intr);
+    const float fr = (float)frd, fa = (float)(azoff - i32_to_f64(inta));
+    const size_t i1 = (size_t)inta * P.samples + intr;
+    const double eta = -P.lines * P.dtaz / 2. + t - P.tstart;
+    if constexpr (kFused) {
+      const double2 *tops = q ? tops1 : tops0;
+      const double2 c0 = __ldg(tops + intr), c1 = __ldg(tops + intr + 1);  // (-kt, etaref)
+      const double ea = deramp_eta(P, inta);
+      const float k0 = (float)(-c0.x), dk = (float)(c0.x - c1.x), de = (float)(c1.y - c0.y);
+      const float u = (float)(ea - c0.y), ati = (float)P.ati;
+      const float w = fmaf(-fr, de, (float)(eta - ea));
+      const float ub = u + ati, wb = w - ati, e = u + w;
+      const float kfe = fr * dk * e * e;
+      const float ta = fmaf(k0 * w, 2.f * u + w, kfe), tb = fmaf(k0 * wb, 2.f * ub + wb, kfe);
+      const float ua = u - de, uc = ub - de;
+      const float ra = fmaf(k0 * de, 2.f * u - de, -dk * ua * ua);
+      const float rb = fmaf(k0 * de, 2.f * ub - de, -dk * uc * uc);
+      const double hr = gc[q].k4_wvl * rng;  // two-way range phase, half-cycles
+      const float rr = (float)fma(-2.0, rint(0.5 * hr), hr);
+      const float2 s2 = cmul(load_ro(burst + i1 + 1), rotation_pi_f(ra));
+      const float2 s4 = cmul(load_ro(burst + i1 + P.samples + 1), rotation_pi_f(rb));
+      const float2 ca = cmul(lerp2(load_ro(burst + i1), s2, fr), phasor_pi_f(rr + ta));
+      const float2 cb = cmul(lerp2(load_ro(burst + i1 + P.samples), s4, fr), phasor_pi_f(rr + tb));
+      v[q] = lerp2(ca, cb, fa);
+    } else {
+      // per-pixel TOPS reramp of the deramped burst (geo2rdr.cu:210-219, 238-243)
+      const double tr = rng * gc[q].two_over_c;
+      double dt = tr - P.fm[0];
+      const double ka = P.fm[1] + dt * (P.fm[2] + P.fm[3] * dt);
+      dt = tr - P.dc[0];
+      const double fnc = P.dc[1] + dt * (P.dc[2] + P.dc[3] * dt);
+      const double kmk = ka - P.ks;
+      const double inv = rcp_newton(ka * kmk);
+      const double kt = ka * P.ks * (ka * inv);
+      const double ed = eta - (-fnc * (kmk * inv) - P.etac0);
+      const float2 a1 = lerp2(__ldg(burst + i1), __ldg(burst + i1 + 1), fr);
+      const float2 a2 = lerp2(__ldg(burst + i1 + P.samples), __ldg(burst + i1 + P.samples + 1), fr);
+      v[q] = cmul(lerp2(a1, a2, fa), phasor_pi(fma(kt, ed * ed, gc[q].k4_wvl * rng)));
+    }
+  }
+}
+
 template <typename TSrc, bool kFused>
 __global__ __launch_bounds__(kXmTX, 5) void frame_geo_xmul_kernel(const FrameDev d, const FrameIO io) {
   constexpr int RY = kFrameGeoRows;
@@ -910,53 +1001,54 @@ __global__ __launch_bounds__(kXmTX, 5) void frame_geo_xmul_kernel(const FrameDev
   const int16_t *demc = io.dem + (int64_t)R0 * io.dem_pitch + C;  // the thread's column at tile row 0
   float4 *part = reinterpret_cast<float4 *>(io.work + pr.part_off) +
                  (int64_t)blockIdx.y * lrows * pr.part_cols + (C - pr.part_left);
-  double inv_c1a = 0.0, inv_c1b = 0.0;
   float ir = 0.f, ii = 0.f, p1 = 0.f, p2 = 0.f;
   int lr = 0;  // rows summed into the current look row
   int rlo0 = INT_MAX, rhi0 = -1, rlo1 = INT_MAX, rhi1 = -1;
+  // the rows rb .. rend - 1 of one block of 32, with the bursts of MASK solved
+  auto block_rows = [&](auto mask_tag, int rb, int rend) {
+    constexpr int MASK = decltype(mask_tag)::value;
+    row_terms(rb);
+    int16_t hn = colin && rb < rlim ? __ldg(demc + (int64_t)rb * io.dem_pitch) : 0;
+    for (int r = rb; r < rend; ++r) {
+      const double sinlat = __shfl_sync(0xffffffffu, r_sin, r & 31);
+      const double coslat = __shfl_sync(0xffffffffu, r_cos, r & 31);
+      const double re = __shfl_sync(0xffffffffu, r_re, r & 31);
+      const double hgt = i32_to_f64(hn);
+      if (colin && r + 1 < rend && r + 1 < rlim) hn = __ldg(demc + (int64_t)(r + 1) * io.dem_pitch);
+      double p[3];
+      llh_point(sinlat, coslat, re, sinlon, coslon, hgt, p);
+      const int w0 = row0w[0] + r, w1 = row0w[1] + r;
+      const bool act[2] = {colw[0] >= 0 && w0 >= 0 && w0 < nrw[0], colw[1] >= 0 && w1 >= 0 && w1 < nrw[1]};
+      float2 v[2];
+      geo_pair_pixel<TSrc, kFused, MASK>(sp, s_gc, &s_zd[0][wid], &s_zd[1][wid], &s_seed[0][wid], &s_seed[1][wid], p,
+                                         hgt, r, colw, act,
+                                         src0, src1, tops0, tops1, v);
+      if ((MASK & 1) && (v[0].x != 0.f || v[0].y != 0.f)) {
+        rlo0 = min(rlo0, w0);
+        rhi0 = w0 + 1;
+      }
+      if ((MASK & 2) && (v[1].x != 0.f || v[1].y != 0.f)) {
+        rlo1 = min(rlo1, w1);
+        rhi1 = w1 + 1;
+      }
+      xm_accumulate(v[0], v[1], ir, ii, p1, p2);
+      if (++lr == d.rowlook) {
+        if (colin) __stcs(part, make_float4(ir, ii, p1, p2));
+        part += pr.part_cols;
+        ir = ii = p1 = p2 = 0.f;
+        lr = 0;
+      }
+    }
+  };
   for (int rb = 0; rb < nr; rb += 32) {
     const int rend = min(rb + 32, nr), j = rb >> 5;
     const bool on0 = !((off[0] >> j) & 1u), on1 = !((off[1] >> j) & 1u);  // warp-uniform
-    if (on0 || on1) {
-      row_terms(rb);
-      bool first0 = true, first1 = true;
-      int16_t hn = colin && rb < rlim ? __ldg(demc + (int64_t)rb * io.dem_pitch) : 0;
-      for (int r = rb; r < rend; ++r) {
-        const double sinlat = __shfl_sync(0xffffffffu, r_sin, r & 31);
-        const double coslat = __shfl_sync(0xffffffffu, r_cos, r & 31);
-        const double re = __shfl_sync(0xffffffffu, r_re, r & 31);
-        const double hgt = i32_to_f64(hn);
-        if (colin && r + 1 < rend && r + 1 < rlim) hn = __ldg(demc + (int64_t)(r + 1) * io.dem_pitch);
-        double p[3];
-        llh_point(sinlat, coslat, re, sinlon, coslon, hgt, p);
-        float2 v0 = make_float2(0.f, 0.f), v1 = make_float2(0.f, 0.f);
-        const int w0 = row0w[0] + r, w1 = row0w[1] + r;
-        if (on0 && colw[0] >= 0 && w0 >= 0 && w0 < nrw[0]) {
-          v0 = geo_pixel<TSrc, kFused>(sp[0], s_gc[0], s_zd[0][wid], s_seed[0][wid], p, hgt, r, colw[0], first0,
-                                       inv_c1a, src0, tops0);
-          first0 = false;
-          if (v0.x != 0.f || v0.y != 0.f) {
-            rlo0 = min(rlo0, w0);
-            rhi0 = w0 + 1;
-          }
-        }
-        if (on1 && colw[1] >= 0 && w1 >= 0 && w1 < nrw[1]) {
-          v1 = geo_pixel<TSrc, kFused>(sp[1], s_gc[1], s_zd[1][wid], s_seed[1][wid], p, hgt, r, colw[1], first1,
-                                       inv_c1b, src1, tops1);
-          first1 = false;
-          if (v1.x != 0.f || v1.y != 0.f) {
-            rlo1 = min(rlo1, w1);
-            rhi1 = w1 + 1;
-          }
-        }
-        xm_accumulate(v0, v1, ir, ii, p1, p2);
-        if (++lr == d.rowlook) {
-          if (colin) __stcs(part, make_float4(ir, ii, p1, p2));
-          part += pr.part_cols;
-          ir = ii = p1 = p2 = 0.f;
-          lr = 0;
-        }
-      }
+    if (on0 && on1) {
+      block_rows(std::integral_constant<int, 3>{}, rb, rend);
+    } else if (on0) {
+      block_rows(std::integral_constant<int, 1>{}, rb, rend);
+    } else if (on1) {
+      block_rows(std::integral_constant<int, 2>{}, rb, rend);
     } else {
       // neither burst has a pixel to solve here: their samples are zero
       for (int r = rb; r < rend; ++r) {

@@ -205,6 +205,7 @@ __device__ __forceinline__ void zero_doppler_cubic(const OrbitCubic &o, const do
 struct ZeroDopplerPatch {
   double t0, x[3], v[3], a[3], jh[3];  // jh = j / 2
   double vv, k2, c3;                   // |v|^2, (3/2) v.a, c3
+  double inv_c1;                       // 1 / f'(0) at the patch's own centre point (chord slope)
 };
 
 __device__ __forceinline__ void zero_doppler_patch(const OrbitCubic &o, ZeroDopplerPatch &z) {
@@ -253,6 +254,52 @@ __device__ __forceinline__ double zero_doppler_solve(const ZeroDopplerPoint &q, 
     if (fabs(step) < 5.0e-9) break;
   }
   return fma(-h, fma(fma(fma(0.5 * c3, h, (2.0 / 3.0) * q.c2), h, q.c1), h, 2.0 * q.c0), q.dd);
+}
+
+// zero_doppler_solve as straight-line code: two chord-Newton steps from the
+// seed, then the same stopping test (|step| < 5e-9 s), with further steps
+// only when the second step is not yet below it and `more` is set.  From a
+// seed within ~1e-6 s of the root and a slope within 1e-3 of f' the second
+// step is below 1e-9 s, so the common path has no data-dependent branch and
+// independent solves (the two bursts of a pair) interleave.  Returns the
+// squared range.
+__device__ __forceinline__ double zero_doppler_solve2(const ZeroDopplerPoint &q, double c3, double inv_c1,
+                                                      double &h, bool more) {
+  double f = fma(fma(fma(c3, h, q.c2), h, q.c1), h, q.c0);
+  double step = f * inv_c1;
+  h -= step;
+  f = fma(fma(fma(c3, h, q.c2), h, q.c1), h, q.c0);
+  step = f * inv_c1;
+  h -= step;
+  if (more && fabs(step) >= 5.0e-9) {
+    for (int it = 2; it < 51; ++it) {
+      f = fma(fma(fma(c3, h, q.c2), h, q.c1), h, q.c0);
+      step = f * inv_c1;
+      h -= step;
+      if (fabs(step) < 5.0e-9) break;
+    }
+  }
+  return fma(-h, fma(fma(fma(0.5 * c3, h, (2.0 / 3.0) * q.c2), h, q.c1), h, 2.0 * q.c0), q.dd);
+}
+
+// exp(i pi x) of an FP32 phase in half-cycles (|x| < 2^22): the reduction
+// x - 2 rint(x / 2) is exact, then the hardware sine and cosine of the
+// reduced angle (absolute error ~4e-7 on [-pi, pi]).
+__device__ __forceinline__ float2 phasor_pi_f(float x) {
+  const float r = fmaf(-2.f, rintf(0.5f * x), x);
+  float s, c;
+  __sincosf(r * 3.14159265f, &s, &c);
+  return make_float2(c, s);
+}
+
+// exp(i pi x) for the small rotations between neighbouring burst columns
+// (|pi x| <= 0.1: Taylor series of cos and sin to the fourth and fifth
+// order, truncation error < 1e-7), larger angles through phasor_pi_f.
+__device__ __forceinline__ float2 rotation_pi_f(float x) {
+  const float a = x * 3.14159265f;
+  if (fabsf(a) > 0.1f) return phasor_pi_f(x);
+  const float a2 = a * a;
+  return make_float2(fmaf(a2, fmaf(a2, 1.f / 24.f, -0.5f), 1.f), a * fmaf(a2, -1.f / 6.f, 1.f));
 }
 
 // sqrt(s) for normal s in float range, to FP64 accuracy: Heron's method

@@ -4,6 +4,8 @@ amplitude multilook and coherence of s1proc/coherence.py, fused.
 """
 from __future__ import annotations
 
+import os
+
 import numpy as np
 import torch
 
@@ -93,3 +95,118 @@ def cc_raster(amp1: np.ndarray, amp2: np.ndarray, coh: np.ndarray) -> np.ndarray
     out[:, :ncol] = amp1.astype(np.float32) * amp2.astype(np.float32)
     out[:, ncol:] = coh
     return out
+
+
+# ----------------------------------------------------------------------------
+# s1proc's interfere() call surface (s1proc/interfere.py:536-704)
+# ----------------------------------------------------------------------------
+
+def _subswaths(burst_files):
+    """Burst files of one date grouped by subswath (``iw1``..``iw3`` in the
+    name) and sorted by top + bottom of their crop, as sario.BurstGroup /
+    Subswath do (s1proc/sario.py:218-266).  Returns [[(path, header)], x3]."""
+    out = []
+    for sw in range(1, 4):
+        bs = []
+        for f in burst_files:
+            if f"iw{sw}" in f:
+                bs.append((f, formats.read_header(f)))
+        bs.sort(key=lambda b: int(b[1][3]) + int(b[1][5]))
+        out.append(bs)
+    return out
+
+
+def match_bursts(ref_bursts, sec_bursts):
+    """For every reference burst the secondary burst of the nearest crop
+    rows (|top difference| + |bottom difference|, first minimum), as
+    s1proc/interfere.py:17-45.  Bursts: [(path, header)]."""
+    if not ref_bursts or not sec_bursts:
+        return []
+    tops = np.array([int(h[3]) for _, h in sec_bursts])
+    bottoms = np.array([int(h[5]) for _, h in sec_bursts])
+    pairs = []
+    for f, h in ref_bursts:
+        k = int(np.argmin(np.abs(tops - int(h[3])) + np.abs(bottoms - int(h[5]))))
+        pairs.append((f, sec_bursts[k][0]))
+    return pairs
+
+
+def burst_pair_tasks(ref_files, sec_files, ifg_path):
+    """(ref, sec, out) burst-pair tasks of one date pair, subswath by
+    subswath, the output named <ref burst>_<sec burst>.int in ``ifg_path``
+    (s1proc/interfere.py:48-78, 183-210)."""
+    tasks = []
+    for rb, sb in zip(_subswaths(ref_files), _subswaths(sec_files)):
+        for f1, f2 in match_bursts(rb, sb):
+            n1 = os.path.splitext(os.path.basename(f1))[0]
+            n2 = os.path.splitext(os.path.basename(f2))[0]
+            tasks.append((f1, f2, os.path.join(ifg_path, n1 + "_" + n2 + ".int")))
+    return tasks
+
+
+def check_tuning(io_workers=-1, cpu_workers=-1, gpu_workers=-1, streams_per_gpu=-1, max_slots=-1):
+    """The daemon's all-or-nothing tuning contract (s1proc/interfere.py:642-663):
+    every value -1 (automatic) or every value a positive int; anything else
+    prints the reference's fatal message and exits with status 1."""
+    vals = (io_workers, cpu_workers, gpu_workers, streams_per_gpu, max_slots)
+    if all(v == -1 for v in vals) or all(isinstance(v, int) and v > 0 for v in vals):
+        return
+    import sys
+    print("[FATAL] Invalid parameter configuration. Please either omit all tuning arguments for hardware-managed "
+          "auto-tuning, or provide the complete set of parameters (--io-workers, --cpu-workers, --streams-per-gpu, "
+          "--gpu-workers, --max-slots). Partial overrides are not allowed.", file=sys.stderr)
+    raise SystemExit(1)
+
+
+def interfere(img_pair_file: str, slc_path: str, rscfile: str, small_rsc_file: str, ifg_path: str = "igrams",
+              rowlook: int = 1, collook: int = 1, out_float: bool = False, io_workers: int = -1,
+              cpu_workers: int = -1, gpu_workers: int = -1, streams_per_gpu: int = -1, max_slots: int = -1,
+              verbose: bool = False):
+    """Interferograms of the date pairs listed in ``ifg_path/img_pair_file``
+    (lines ``<ref date> <sec date>``) from the geocoded bursts
+    ``slc_path/<date>*.gslc``: the multilooked RSC written to
+    ``small_rsc_file``, burst pairs matched per subswath, crossmul + looks on
+    the GPU for every burst pair whose output is missing, then the burst
+    interferograms stitched into ``ifg_path/<ref>_<sec>.int`` (raw, frame
+    grid) with the burst files removed.  Same arguments, files and
+    behaviour as s1proc/interfere.py:536-704; the daemon's host-pipeline
+    tuning arguments are checked the same way and otherwise unused (the
+    burst pairs run in-process on the GPU).  Returns (ok, failed)."""
+    import glob
+
+    from . import stitch as _stitch
+    os.makedirs(ifg_path, exist_ok=True)
+    rsc = formats.read_rsc(rscfile)
+    if os.path.dirname(small_rsc_file):
+        os.makedirs(os.path.dirname(small_rsc_file), exist_ok=True)
+    formats.write_rsc(small_rsc_file, rsc.take_look(rowlook, collook))
+    pairs, groups = [], {}
+    with open(os.path.join(ifg_path, img_pair_file)) as f:
+        for line in f:
+            w = line.split()
+            if len(w) < 2:
+                continue
+            pairs.append((w[0], w[1]))
+            for d in w[:2]:
+                if d not in groups:
+                    groups[d] = glob.glob(os.path.join(slc_path, f"{d}*.gslc"))
+    tasks, frame_map = [], {}
+    for ref, sec in pairs:
+        outfile = os.path.join(ifg_path, f"{ref}_{sec}.int")
+        if os.path.exists(outfile):
+            continue
+        t = burst_pair_tasks(groups[ref], groups[sec], ifg_path)
+        frame_map[outfile] = [x[2] for x in t]
+        if not all(os.path.exists(x[2]) for x in t):
+            tasks.extend(t)
+    if not tasks:
+        for outfile, parts in frame_map.items():
+            _stitch.stitch(parts, outfile, out_float)
+        return 0, 0
+    check_tuning(io_workers, cpu_workers, gpu_workers, streams_per_gpu, max_slots)
+    todo = [t for t in tasks if not os.path.exists(t[2])]
+    emit = print if verbose else (lambda *a, **k: None)
+    ok, failed = crossmul_files(todo, rowlook, collook, out_float=out_float, emit=emit)
+    for outfile, parts in frame_map.items():
+        _stitch.stitch(parts, outfile, out_float)
+    return ok, failed
