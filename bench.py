@@ -67,7 +67,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="s1b", choices=["s1b", "reference"])
     ap.add_argument("--config", default="frame",
-                    choices=["frame", "frame_small", "frame_pairs", "c1", "c1geo", "c0", "small", "adjoint"])
+                    choices=["frame", "frame_small", "frame_pairs", "c1", "c1geo", "c0", "small", "adjoint", "stack"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the checker leg (pair 0 against the reference executables and the float64 oracle)")
@@ -975,6 +975,13 @@ def run_s1b(args):
         if not args.no_extras:
             extras["radar_grid_c1"] = _radar_extras(dev, peak)
             extras["adjoint_c3"] = adjoint_measure(dev, max(3, min(args.steps, 10)), world, compact=True)
+            stack = stack_measure(dev, 3, world)
+            by_date = {}
+            for p in stack.pop("per_pair"):
+                if p["mean_coherence"] is not None:
+                    by_date.setdefault(p["date"], []).append(p["mean_coherence"])
+            stack["mean_coherence_per_date"] = [round(sum(v) / len(v), 4) for _, v in sorted(by_date.items())]
+            extras["stack_c4"] = stack
             line["extras"] = extras
         if pair0 is not None:
             line["parity"] = parity_leg(pair0, sc.dem.cpu().numpy(), sc.rsc, (sc.rowlook, sc.collook), sc.alpha,
@@ -1333,6 +1340,123 @@ def adjoint_measure(dev, steps, world, compact=False):
     return out
 
 
+STACK_SEED = 20261203 + 5000
+STACK_BATCH = 10  # secondary dates per batch of the stack
+
+
+def stack_measure(dev, steps, world, n_sec=29, offsets_rows=0, xmul=None):
+    """The time series of one subswath: a reference date and ``n_sec``
+    secondary dates of 9 bursts of 1500 x 21000 complex64 (baselines +-200 m,
+    temporal coherence 0.9 exp(-dt / 60 d) at 12-day revisits, a 1 cm/yr
+    deformation ramp).  Every reference-secondary burst pair runs through the
+    batched frame path in batches of STACK_BATCH dates (one descriptor table
+    and one CUDA graph per batch; the reference bursts stored once per batch);
+    a batch's device time per replay is timed with CUDA events on resident
+    inputs.  ``xmul``: crossmul fused into the geocoding (True), on geocoded
+    windows (False: each burst geocoded once, the reference shared by the
+    batch's pairs), or None to time both on the first batch and keep the
+    faster.  ``offsets_rows`` > 0: per date, the geocoding's sample
+    coordinates of burst 0 against the float64 oracle on that many rows."""
+    import torch
+
+    from sentinel_gpu_processor_b200 import synth
+    from sentinel_gpu_processor_b200.chain import BatchedFrameChain
+    st = synth.make_stack(seed=STACK_SEED, device=dev, n_sec=n_sec)
+    nb = st.n_bursts
+    ref_slcs = [synth.stack_slc(st, -1, b, dev) for b in range(nb)]
+    batches = [list(range(i, min(i + STACK_BATCH, n_sec))) for i in range(0, n_sec, STACK_BATCH)]
+    total_ms, px, per_pair, tried = 0.0, 0, [], {}
+    for bi, dates in enumerate(batches):
+        acqs = list(st.ref) + [st.sec[d][b] for d in dates for b in range(nb)]
+        pairs = [(b, nb + j * nb + b) for j in range(len(dates)) for b in range(nb)]
+        modes = [xmul] if xmul is not None else ([True, False] if bi == 0 else [tried["chosen"]])
+        best = None
+        for mode in modes:
+            chain = BatchedFrameChain(acqs, None, st.rsc, st.rowlook, st.collook, st.alpha, device=dev, pairs=pairs,
+                                      crossmul_fused=mode)
+            for b in range(nb):
+                chain.views[b].copy_(ref_slcs[b])
+            for j, d in enumerate(dates):
+                for b in range(nb):
+                    chain.views[nb + j * nb + b].copy_(synth.stack_slc(st, d, b, dev))
+            chain.capture(st.dem)
+            ms = _timed_replays(chain.replay, steps)
+            if bi == 0:
+                tried["fused" if mode else "windows"] = ms
+            if best is None or ms < best[0]:
+                stats = []
+                for k, r in enumerate(chain.results()):
+                    d = dates[k // nb]
+                    stats.append({"date": d, "burst": k % nb, "days": st.days[d],
+                                  "baseline_m": round(st.baselines[d], 2), "coherence_sim": round(st.coherence[d], 4),
+                                  "mean_coherence": None if r is None else float(r.coh.float().mean())})
+                best = (ms, mode, chain.burst_pixels, stats)
+            chain.graph = None
+            del chain
+            torch.cuda.empty_cache()
+        ms, mode, bpx, stats = best
+        tried["chosen"] = mode
+        total_ms += ms
+        px += bpx
+        per_pair += stats
+    out = {"workload": (f"time series of one subswath: 1 reference + {n_sec} secondary dates x {nb} bursts of "
+                        f"{st.lines} x {st.samples} complex64, 12-day revisits, baselines +-200 m, coherence "
+                        f"0.9 exp(-dt/60 d), 1 cm/yr deformation ramp; batches of {STACK_BATCH} dates, one CUDA "
+                        "graph per batch"),
+           "value": px / (total_ms / 1e3), "unit": UNIT, "burst_pairs": len(per_pair), "burst_px": px,
+           "ms_per_stack": total_ms, "batches": len(batches),
+           "crossmul": "fused into the geocoding" if tried["chosen"] else "kernel on geocoded windows (reference "
+                                                                       "bursts geocoded once per batch)",
+           "first_batch_ms": {k: v for k, v in tried.items() if k != "chosen"}, "per_pair": per_pair}
+    if offsets_rows > 0:
+        import numpy as np
+
+        from oracle import geo2rdr as og2
+        from sentinel_gpu_processor_b200 import kernels, plan as _plan
+        dem_h = st.dem.cpu().numpy()
+        r = st.rsc
+        stats = []
+        for d in range(-1, n_sec):
+            acq = st.ref[0] if d < 0 else st.sec[d][0]
+            pl = _plan.burst_plan(acq.radar, acq.orbit, acq.fm, acq.dc, acq.bursts[0], st.rsc)
+            az, rg = kernels.geo2rdr_grid_offsets(pl, st.dem)
+            rows = np.linspace(0, pl.nrow - 1, offsets_rows).round().astype(np.int64)
+            rad = og2.Radar(**{k: getattr(acq.radar, k) for k in og2.Radar.__dataclass_fields__})
+            b = og2.BurstMeta(**{k: getattr(acq.bursts[0], k) for k in og2.BurstMeta.__dataclass_fields__})
+            oaz, org = og2.window_offsets(dem_h[pl.win_top:pl.win_bottom, pl.win_left:pl.win_right], rows, rad,
+                                          acq.orbit, b, r.latmax + r.dlat * pl.win_top, r.lonmin + r.dlon * pl.win_left,
+                                          r.dlat, r.dlon)
+            gaz, grg = az.cpu().numpy()[rows], rg.cpu().numpy()[rows]
+            used = ((org > b.first_valid_sample) & (org < b.last_valid_sample - 1) & (oaz >= b.first_valid_line + 5)
+                    & (oaz < b.last_valid_line - 5))
+            stats.append({"date": d, "max_az_px": float(np.abs(gaz - oaz)[used].max()),
+                          "max_rg_px": float(np.abs(grg - org)[used].max()), "pixels": int(used.sum())})
+        out["offsets_vs_float64_oracle"] = stats
+        out["offset_px"] = max(max(x["max_az_px"], x["max_rg_px"]) for x in stats)
+    return out
+
+
+def run_stack(args):
+    """configs C4 as its own bench line."""
+    import torch
+    rank, world, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", local)
+    clocks = Clocks(local)
+    clocks.start()
+    m = stack_measure(dev, args.steps, world, offsets_rows=0 if args.no_parity else 4)
+    clk = clocks.stop()
+    value = max_over_ranks(m["ms_per_stack"], world)
+    line = {"metric": METRIC, "value": world * m["burst_px"] / (value / 1e3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": 3, "ms_per_step": value, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 geometry + c64", "data": "synthetic",
+            "config": {"workload": m.pop("workload"), "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2"}, "stack": m}
+    if clk is not None:
+        line["clocks"] = clk
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_adjoint(args):
     """The adjoint measurement as its own bench line (metric: adjoint evals/s)."""
     import torch
@@ -1367,6 +1491,8 @@ def main():
         run_reference(args)
     elif args.config == "adjoint":
         run_adjoint(args)
+    elif args.config == "stack":
+        run_stack(args)
     else:
         run_s1b(args)
 

@@ -163,6 +163,41 @@ int s1b_bounds(const s1b_orbit_poly_t *orbit, double start_time, double end_time
 int s1b_orbit_eval_host(const s1b_orbit_poly_t *orbit, const double *t, int64_t n,
                         double *satx, double *satv);
 
+/* One burst for s1b_burst_geometry (device record): what the reference's
+ * geo2rdr reads from its DB for the burst (csrc/src/geo2rdr.cu:333-376). */
+typedef struct s1b_burst_geometry_in_t {
+  int32_t orbit;              /* index into the orbit-polynomial array */
+  int32_t fm_table, dc_table; /* indices into the packed FM-rate / Doppler tables */
+  int32_t lines, samples;
+  double tstart;              /* azimuthTimeSeconds<i> */
+  double prf, azimuth_time_interval, slant_range_time, range_sampling_rate;
+  double radar_frequency, azimuth_steering_rate; /* Hz, degrees / s */
+  double hmin, hmax;
+} s1b_burst_geometry_in_t;
+
+/* Result of s1b_burst_geometry for one burst (device record). */
+typedef struct s1b_burst_geometry_t {
+  double latlon_box[4]; /* footprint latmin, latmax, lonmin, lonmax at hmin..hmax */
+  double ks, etac0;     /* TOPS steering rate term and etac at the first range sample */
+  double fm[4], dc[4];  /* FM-rate / Doppler t0, c0, c1, c2 at the burst centre */
+  int32_t win[4];       /* DEM window left, top, right, bottom on `rsc` (0 without rsc) */
+  int32_t status;       /* 0 ok; 1 a bad index or radar parameter (record zeroed) */
+} s1b_burst_geometry_t;
+
+/* Burst geometry prep of n bursts on the GPU in one launch, FP64: the
+ * footprint at hmin..hmax (bounds/rah2ll, csrc/src/bounds.cu:237-317, as
+ * geo2rdr.cu:387-400 calls it), the DEM window on `rsc` (569-586) and the
+ * FM-rate / Doppler interpolation and TOPS steering term at the burst
+ * centre (469-542) -- the host planner's functions (s1b_burst_plan) on the
+ * device.  orbits: device [n_orbits] (s1b_orbit_poly); tables: device
+ * [n_tables * max_records * 5] records (time, t0, c0, c1, c2), table_records:
+ * device [n_tables] record counts; bursts, out: device [n]; rsc: host
+ * pointer or NULL. */
+int s1b_burst_geometry(const s1b_orbit_poly_t *orbits, int32_t n_orbits, const double *tables,
+                       const int32_t *table_records, int32_t n_tables, int32_t max_records,
+                       const s1b_burst_geometry_in_t *bursts, int32_t n, const s1b_rsc_t *rsc,
+                       s1b_burst_geometry_t *out, void *stream);
+
 /* ------------------------------------------------------------- geo2rdr */
 
 /* TOPS deramp of one burst: out = in * exp(-i pi kt (eta - etaref)^2).

@@ -98,6 +98,20 @@ class BurstPlan(ctypes.Structure):
 
 
 # name -> (restype, argtypes); the table is the C ABI of include/s1b.h
+class BurstGeometryIn(ctypes.Structure):
+    """s1b_burst_geometry_in_t: one burst of s1b_burst_geometry."""
+    _fields_ = [("orbit", c_int32), ("fm_table", c_int32), ("dc_table", c_int32), ("lines", c_int32),
+                ("samples", c_int32), ("tstart", c_double), ("prf", c_double), ("azimuth_time_interval", c_double),
+                ("slant_range_time", c_double), ("range_sampling_rate", c_double), ("radar_frequency", c_double),
+                ("azimuth_steering_rate", c_double), ("hmin", c_double), ("hmax", c_double)]
+
+
+class BurstGeometry(ctypes.Structure):
+    """s1b_burst_geometry_t: footprint, DEM window and TOPS centre terms of one burst."""
+    _fields_ = [("latlon_box", c_double * 4), ("ks", c_double), ("etac0", c_double), ("fm", c_double * 4),
+                ("dc", c_double * 4), ("win", c_int32 * 4), ("status", c_int32)]
+
+
 class StitchBurst(ctypes.Structure):
     _fields_ = [("offset", c_int64), ("left", c_int32), ("top", c_int32), ("right", c_int32), ("bottom", c_int32),
                 ("subswath", c_int32), ("group", c_int32)]
@@ -150,6 +164,8 @@ _SIGNATURES = {
                               c_void_p]),
     "s1b_geo2rdr_grid_offsets": (c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_void_p]),
     "s1b_set_staging_poll_limit": (ctypes.c_uint32, [ctypes.c_uint32]),
+    "s1b_burst_geometry": (c_int, [c_void_p, c_int32, c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_int32,
+                                   c_void_p, c_void_p, c_void_p]),
     "s1b_goldstein_noalloc": (c_int, [c_void_p, c_void_p, c_int32, c_int32, c_int32, c_float, c_void_p]),
     "s1b_amp_looks": (c_int, [c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32, c_int32, c_int32, c_int32,
                               c_int32, c_void_p, c_void_p]),

@@ -21,6 +21,9 @@ INCLUDE = os.path.join(ROOT, "include")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libs1b.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# per-source flags: the device burst geometry rounds FP64 operation by
+# operation like the host planner (no FMA contraction)
+EXTRA_FLAGS = {"k_plan.cu": ["-fmad=false"]}
 
 
 def _nvcc():
@@ -52,7 +55,7 @@ def build(force=False, verbose_ptxas=False, quiet=False):
         if (not force and os.path.exists(obj) and os.path.getmtime(obj) >= os.path.getmtime(src)
                 and os.path.getmtime(obj) >= hdr_mtime):
             continue
-        cmd = [nvcc, *flags, "-c", src, "-o", obj]
+        cmd = [nvcc, *flags, *EXTRA_FLAGS.get(os.path.basename(src), []), "-c", src, "-o", obj]
         if verbose_ptxas and src.endswith(".cu"):
             cmd[1:1] = ["-Xptxas", "-v"]
         r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)

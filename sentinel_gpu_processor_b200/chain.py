@@ -340,7 +340,7 @@ class BatchedFrameChain:
     """
 
     def __init__(self, refs, secs, rsc, rowlook, collook, alpha, n_win=32, device="cuda", fill_seed=0,
-                 sample_format="c64", deramp_fused=True, crossmul_fused=True):
+                 sample_format="c64", deramp_fused=True, crossmul_fused=True, pairs=None):
         import ctypes
         if sample_format not in ("c64", "ci16"):
             raise ValueError("sample_format must be 'c64' (complex64) or 'ci16' (complex int16)")
@@ -348,19 +348,31 @@ class BatchedFrameChain:
         self.dev = torch.device(device)
         self.rowlook, self.collook, self.alpha, self.n_win = int(rowlook), int(collook), float(alpha), int(n_win)
         self.fill_seed = int(fill_seed)
+        if pairs is None:
+            # refs[k] with secs[k]: bursts 2k and 2k + 1
+            acqs = [a for ra, sa in zip(refs, secs) for a in (ra, sa)]
+            pairs = [(2 * k, 2 * k + 1) for k in range(len(refs))]
+        else:
+            # ``refs`` lists every burst once; ``pairs`` indexes into it (a
+            # burst shared by several pairs, e.g. a stack's reference date, is
+            # stored and geocoded once when the crossmul is not fused)
+            acqs = list(refs)
+            pairs = [(int(a), int(b)) for a, b in pairs]
+            if any(not (0 <= i < len(acqs)) for pr in pairs for i in pr):
+                raise ValueError("pair index outside the burst list")
         plans = []
-        for ra, sa in zip(refs, secs):
-            for a in (ra, sa):
-                p = _plan.burst_plan(a.radar, a.orbit, a.fm, a.dc, a.bursts[0], rsc)
-                if p.nrow <= 0 or p.ncol <= 0:
-                    raise _lib.S1BError(_lib.S1B_ERR_EMPTY, "BatchedFrameChain: burst outside the DEM grid")
-                plans.append(p)
+        for a in acqs:
+            p = _plan.burst_plan(a.radar, a.orbit, a.fm, a.dc, a.bursts[0], rsc)
+            if p.nrow <= 0 or p.ncol <= 0:
+                raise _lib.S1BError(_lib.S1B_ERR_EMPTY, "BatchedFrameChain: burst outside the DEM grid")
+            plans.append(p)
         self.plans = plans
-        self.n_pairs = len(refs)
+        self.pair_index = pairs
+        self.n_pairs = len(pairs)
         lib = _lib.load()
         arr = (_lib.BurstPlan * len(plans))(*plans)
-        pref = (ctypes.c_int32 * self.n_pairs)(*range(0, 2 * self.n_pairs, 2))
-        psec = (ctypes.c_int32 * self.n_pairs)(*range(1, 2 * self.n_pairs, 2))
+        pref = (ctypes.c_int32 * self.n_pairs)(*[a for a, _ in pairs])
+        psec = (ctypes.c_int32 * self.n_pairs)(*[b for _, b in pairs])
         handle = ctypes.c_void_p()
         with torch.cuda.device(self.dev):
             _lib.check(lib.s1b_frame_create(arr, len(plans), pref, psec, self.n_pairs, self.rowlook, self.collook,
@@ -399,14 +411,16 @@ class BatchedFrameChain:
             self.burst_offsets.append(off.value)
             v = self.slc[off.value:off.value + p.lines * p.samples]
             views.append(v.view(p.lines, p.samples, 2) if sample_format == "ci16" else v.view(p.lines, p.samples))
-        self.ref_views, self.sec_views = views[0::2], views[1::2]
+        self.views = views
+        self.ref_views = [views[a] for a, _ in pairs]
+        self.sec_views = [views[b] for _, b in pairs]
         self.slots = []
         for k in range(self.n_pairs):
             off, r, c = ctypes.c_int64(), ctypes.c_int32(), ctypes.c_int32()
             _lib.check(lib.s1b_frame_pair_slot(handle, k, ctypes.byref(off), ctypes.byref(r), ctypes.byref(c)),
                        "s1b_frame_pair_slot")
             self.slots.append((off.value, r.value, c.value))
-        self.burst_pixels = sum(p.lines * p.samples for p in plans[0::2])
+        self.burst_pixels = sum(plans[a].lines * plans[a].samples for a, _ in pairs)
         self.graph = None
         self.geo_events = None
 
@@ -512,7 +526,7 @@ class BatchedFrameChain:
             off = self.slots[k][0]
             n = r["nrow_ml"] * r["ncol_ml"]
             shape = (r["nrow_ml"], r["ncol_ml"])
-            p1, p2 = self.plans[2 * k], self.plans[2 * k + 1]
+            p1, p2 = self.plans[self.pair_index[k][0]], self.plans[self.pair_index[k][1]]
             g = r["gslc_rows"]
             hs = (formats.make_header(p1.rsc_nlat, p1.rsc_nlon, p1.win_left, p1.win_top + g[0], p1.win_right,
                                       p1.win_top + g[1]),

@@ -110,3 +110,50 @@ def footprint_boxes(acq):
     acquisition (the burst bounds of geo2rdr.cu:387-400), from the planner."""
     return [tuple(float(v) for v in burst_plan(acq.radar, acq.orbit, acq.fm, acq.dc, b, None).latlon_box)
             for b in acq.bursts]
+
+
+def burst_geometry_device(acqs, rsc=None, device="cuda"):
+    """Footprint, DEM window (on ``rsc`` when given) and TOPS centre terms of
+    every burst of the acquisitions ``acqs`` in one GPU launch
+    (``s1b_burst_geometry``).  Returns one ``_lib.BurstGeometry`` per burst, in
+    the order of the acquisitions and their bursts."""
+    import torch
+    orbits, orbit_of, tables, bursts = [], {}, [], []
+    for a in acqs:
+        key = id(a.orbit)
+        if key not in orbit_of:
+            orbit_of[key] = len(orbits)
+            orbits.append(orbit_poly(*a.orbit))
+        for tab in (a.fm, a.dc):
+            tables.append(np.asarray(tab, dtype=np.float64).reshape(-1, 5))
+        r = a.radar
+        for b in a.bursts:
+            bursts.append(_lib.BurstGeometryIn(orbit_of[key], len(tables) - 2, len(tables) - 1,
+                                               int(r.lines_per_burst), int(r.samples_per_burst), float(b.azimuth_time),
+                                               float(r.prf), float(r.azimuth_time_interval),
+                                               float(r.slant_range_time), float(r.range_sampling_rate),
+                                               float(r.radar_frequency), float(r.azimuth_steering_rate),
+                                               float(r.hmin), float(r.hmax)))
+    max_rec = max(len(t) for t in tables)
+    packed = np.zeros((len(tables), max_rec, 5), dtype=np.float64)
+    for i, t in enumerate(tables):
+        packed[i, :len(t)] = t
+    counts = np.array([len(t) for t in tables], dtype=np.int32)
+
+    def dev_bytes(obj):
+        raw = bytes(obj) if not isinstance(obj, np.ndarray) else obj.tobytes()
+        return torch.frombuffer(bytearray(raw), dtype=torch.uint8).to(device)
+
+    d_orb = dev_bytes((_lib.OrbitPoly * len(orbits))(*orbits))
+    d_tab = dev_bytes(packed)
+    d_cnt = dev_bytes(counts)
+    d_in = dev_bytes((_lib.BurstGeometryIn * len(bursts))(*bursts))
+    out = torch.empty(len(bursts) * ctypes.sizeof(_lib.BurstGeometry), dtype=torch.uint8, device=device)
+    crsc = c_rsc(rsc) if rsc is not None else None
+    _lib.check(_lib.load().s1b_burst_geometry(_lib.dptr(d_orb), len(orbits), _lib.dptr(d_tab), _lib.dptr(d_cnt),
+                                              len(tables), max_rec, _lib.dptr(d_in), len(bursts),
+                                              ctypes.byref(crsc) if crsc is not None else None, _lib.dptr(out),
+                                              _lib.stream_ptr()), "s1b_burst_geometry")
+    raw = bytes(out.cpu().numpy())
+    n = ctypes.sizeof(_lib.BurstGeometry)
+    return [_lib.BurstGeometry.from_buffer_copy(raw[i * n:(i + 1) * n]) for i in range(len(bursts))]

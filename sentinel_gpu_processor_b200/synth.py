@@ -589,6 +589,96 @@ def on_reference_safe_grid(sc: PairScene, boxes_of, pairs=(0,)) -> PairScene:
     return regrid(sc, reference_safe_rsc(sc.rsc, runs))
 
 
+@dataclass
+class StackScene:
+    """A time series of one subswath: a reference date and ``n_sec``
+    secondary dates over one DEM grid.  ``ref``: the reference's bursts
+    (one Acquisition each); ``sec[d]``: those of secondary date d.  SLCs are
+    made on demand (``stack_slc``), so a stack larger than the device's
+    memory can be processed in batches of dates."""
+    seed: int
+    ref: list
+    sec: list            # [n_sec][n_bursts] Acquisition
+    rsc: formats.Rsc
+    dem: object
+    days: list           # days after the reference, per secondary date
+    baselines: list      # perpendicular baselines (m), per secondary date
+    coherence: list      # 0.9 exp(-dt / 60 d), per secondary date
+    rowlook: int
+    collook: int
+    alpha: float
+    lines: int
+    samples: int
+    defo_rate: float = 0.01  # m / yr at the far range edge of the ramp
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def n_bursts(self):
+        return len(self.ref)
+
+
+def make_stack(seed=20261203 + 5000, device="cpu", n_sec=29, n_bursts=9, lines=1500, samples=21000, overlap=100,
+               kt=-1500.0, revisit_days=12, baseline_range=200.0, rowlook=4, collook=20, alpha=0.5, hmax=3000.0,
+               with_dem=True):
+    """Time-series stack of one subswath: ``n_sec`` secondary dates every
+    ``revisit_days`` days after the reference, each with a seeded
+    perpendicular baseline uniform in +-``baseline_range`` m and temporal
+    coherence 0.9 exp(-dt / 60 d); deformation: a phase ramp across range
+    growing at 1 cm/yr (``stack_slc``).  Bursts of ``lines`` x ``samples``,
+    consecutive bursts overlapping by ``overlap`` lines."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    orbit_ref = make_orbit(t_c=ORBIT_T0 + 50.0)
+    near = NEAR_RANGE
+    t0 = ORBIT_T0 + 50.0 - 0.5 * n_bursts * 2.75
+    radar = make_radar(lines, samples, near_range=near, hmin=-100.0, hmax=hmax + 100.0)
+    bursts, t = [], t0
+    for _ in range(n_bursts):
+        bursts.append((t, burst_meta(t, lines, samples)))
+        t += (lines - overlap) * AZIMUTH_INTERVAL
+    fm, dc = tops_tables(radar, ORBIT_T0 + 50.0, kt)
+
+    def acqs(orbit):
+        return [Acquisition(radar=radar, orbit=orbit, fm=fm.copy(), dc=dc.copy(), bursts=[b]) for _, b in bursts]
+
+    ref = acqs(orbit_ref)
+    sec, days, bls, cohs = [], [], [], []
+    for d in range(n_sec):
+        bl = float(rng.uniform(-baseline_range, baseline_range))
+        off = secondary_offset(orbit_ref, ORBIT_T0 + 50.0, near + samples * RANGE_SPACING / 2, bl)
+        sec.append(acqs(make_orbit(t_c=ORBIT_T0 + 50.0, offset=off)))
+        days.append(revisit_days * (d + 1))
+        bls.append(bl)
+        cohs.append(0.9 * math.exp(-revisit_days * (d + 1) / 60.0))
+    rsc = footprint_rsc(ref + [a for s in sec for a in s], 0.0, hmax, margin=0.02)
+    dem = make_dem(rsc, seed, hmax, device=device) if with_dem else None
+    return StackScene(seed=seed, ref=ref, sec=sec, rsc=rsc, dem=dem, days=days, baselines=bls, coherence=cohs,
+                      rowlook=rowlook, collook=collook, alpha=alpha, lines=lines, samples=samples,
+                      extra={"hmax": hmax})
+
+
+def stack_slc(st: StackScene, date: int, burst: int, device="cpu"):
+    """SLC of burst ``burst`` of date ``date`` (-1: the reference), TOPS-
+    modulated: the reference is unit circular-Gaussian speckle seeded per
+    burst; date d mixes it with its own speckle at the date's coherence and
+    adds the deformation phase 4 pi / wvl * rate * dt, the rate a ramp from 0
+    at near range to 1 cm/yr at far range."""
+    import torch
+    L, S = st.lines, st.samples
+    gen = torch.Generator(device=device)
+    gen.manual_seed(st.seed * 1000 + burst)
+    s = speckle(L, S, gen, device)
+    if date < 0:
+        return tops_modulate(s, st.ref[burst], st.ref[burst].bursts[0]).contiguous()
+    gen.manual_seed(st.seed * 1000 + 100000 * (date + 1) + burst)
+    g = st.coherence[date]
+    s = g * s + math.sqrt(1 - g * g) * speckle(L, S, gen, device)
+    ramp = torch.linspace(0.0, 1.0, S, dtype=torch.float64, device=device)
+    phase = (4 * math.pi / WAVELENGTH * st.defo_rate * st.days[date] / 365.25) * ramp
+    s = s * torch.polar(torch.ones_like(phase), phase).to(torch.complex64)[None, :]
+    acq = st.sec[date][burst]
+    return tops_modulate(s, acq, acq.bursts[0]).contiguous()
+
+
 def cint16(slc, scale: float = 2000.0):
     """Complex int16 samples (int16 [..., 2], re and im) of a synthetic SLC
     tensor, as a Sentinel-1 measurement TIFF holds them: ``round(scale *
