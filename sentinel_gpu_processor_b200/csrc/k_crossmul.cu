@@ -360,7 +360,7 @@ __global__ __launch_bounds__(XM_THREADS, 4) void frame_crossmul_kernel(const Fra
 // shared memory with coalesced loads, then each lane adds the collook
 // columns of its pixel in order and forms the outputs.
 // blockIdx.z = pair, y = multilooked row, x = groups of 128 multilooked columns.
-constexpr int XC_SPAN = 640;  // float4 per warp buffer (10 KB)
+constexpr int XC_SPAN = 704;  // float4 per warp buffer (11 KB)
 
 __global__ __launch_bounds__(128) void frame_xm_cells_kernel(const FrameDev d, const FrameIO io) {
   __shared__ float4 buf[4][XC_SPAN];
@@ -375,7 +375,7 @@ __global__ __launch_bounds__(128) void frame_xm_cells_kernel(const FrameDev d, c
   float2 *ifg = io.ifg + pr.ml_off;
   float *amp1 = io.amp1 ? io.amp1 + pr.ml_off : nullptr, *amp2 = io.amp2 ? io.amp2 + pr.ml_off : nullptr;
   float *coh = io.coh ? io.coh + pr.ml_off : nullptr;
-  if (cl > XC_SPAN) {  // very wide looks: each lane reads its own columns
+  if ((cl | 1) > XC_SPAN) {  // very wide looks: each lane reads its own columns
     const int j = jw + lane;
     if (j >= r.ncol_ml) return;
     float ir = 0.f, ii = 0.f, p1 = 0.f, p2 = 0.f;
@@ -389,17 +389,23 @@ __global__ __launch_bounds__(128) void frame_xm_cells_kernel(const FrameDev d, c
     xm_finish(ir, ii, p1, p2, d.rowlook, cl, (int64_t)i * r.ncol_ml + j, ifg, amp1, amp2, coh, nullptr, d.fill_seed);
     return;
   }
-  const int per = min(32, XC_SPAN / cl);  // pixels per pass
+  // each pixel's columns at an odd stride in float4 (cl | 1): the lanes'
+  // 16-byte reads of column u then fall in distinct banks
+  const int cs = cl | 1;
+  const int per = min(32, XC_SPAN / cs);  // pixels per pass
   for (int m0 = 0; m0 < 32; m0 += per) {
     const int j0 = jw + m0, n = min(min(per, 32 - m0), r.ncol_ml - j0);
     if (n <= 0) break;
     const float4 *src = row + (int64_t)j0 * cl;
     __syncwarp();  // the previous pass is done with the buffer
-    for (int e = lane; e < n * cl; e += 32) buf[w][e] = __ldcs(src + e);
+    for (int e = lane; e < n * cl; e += 32) {
+      const int m = e / cl;
+      buf[w][e + m * (cs - cl)] = __ldcs(src + e);
+    }
     __syncwarp();
     if (lane < n) {
       float ir = 0.f, ii = 0.f, p1 = 0.f, p2 = 0.f;
-      const float4 *b = buf[w] + lane * cl;
+      const float4 *b = buf[w] + lane * cs;
       for (int u = 0; u < cl; ++u) {
         const float4 v = b[u];
         ir += v.x;
