@@ -52,12 +52,15 @@ GEO_DRAM_BYTES_PER_GEO_PX = 23.63
 # bytes of one launch on the small frame (586.5 MB / 496.1 MB); both terms (raw
 # samples read, geocoded pixels written) scale with the frame
 GEO_FUSED_TRAFFIC_RATIO = 1.182
-# the same with the crossmul look sums formed in the geocoding (391.7 MB / 290.7 MB)
-GEO_XMUL_TRAFFIC_RATIO = 1.347
+# the same with the crossmul look sums formed in the geocoding, per sample format:
+# complex64 samples 450.7 MB / 491.7 MB (the gathers touch only the samples the
+# DEM window maps into, less than every sample of both bursts), complex int16
+# samples 391.7 MB / 290.7 MB
+GEO_XMUL_TRAFFIC_RATIO = {"c64": 0.917, "ci16": 1.347}
 RESAMPLE_DRAM_BYTES_PER_PX = 24.75
 # what bounds the frame geocoding, from its ncu counters (issue and warp stalls)
 GEO_LIMITER = ("latency: per-pixel chain of FP64 solve, gathers and phasors at 20 resident warps per SM "
-               "(issue active 47 %, FP64 pipe 24 %); not HBM")
+               "(issue active 43 %, XU pipe 31 %, FP64 pipe 21 %); not HBM")
 
 
 def parse():
@@ -916,8 +919,8 @@ def run_s1b(args):
     if top == "geo2rdr":
         if frame:  # one launch geocodes every burst
             if chain.crossmul_fused:
-                traffic = (GEO_XMUL_TRAFFIC_RATIO * table["geo2rdr"]["bytes_per_launch"]
-                           if GEO_XMUL_TRAFFIC_RATIO and chain.deramp_fused else None)
+                ratio = GEO_XMUL_TRAFFIC_RATIO.get(args.samples)
+                traffic = ratio * table["geo2rdr"]["bytes_per_launch"] if ratio and chain.deramp_fused else None
             else:
                 traffic = (GEO_FUSED_TRAFFIC_RATIO * table["geo2rdr"]["bytes_per_launch"] if chain.deramp_fused
                            else GEO_DRAM_BYTES_PER_GEO_PX * sum(p.nrow * p.ncol for p in chain.plans))

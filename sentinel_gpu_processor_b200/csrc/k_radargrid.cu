@@ -933,6 +933,7 @@ __global__ __launch_bounds__(C_THREADS, 1) void box_coherence_kernel(const __gri
   for (int k = 0;; ++k) {
     const int t = blockIdx.x + k * gridDim.x;
     if (t >= ntiles) break;
+    bool ok = true;  // this thread saw the tile's staging complete
     float2 *sr = stage0 + (k & 1) * C_STAGE;
     float2 *ss = sr + C_IH * C_IW;
     const int col0 = (t % ntx) * C_TW, row0 = (t / ntx) * C_TH;
@@ -944,19 +945,7 @@ __global__ __launch_bounds__(C_THREADS, 1) void box_coherence_kernel(const __gri
         tma_tile(nr, nr + C_IH * C_IW, tref, tsec, (tn % ntx) * C_TW - C_HX, (tn / ntx) * C_TH - C_MAXH,
                  smem_addr(&bars[(k + 1) & 1]));
       }
-      const uint32_t b = smem_addr(&bars[k & 1]);
-      const bool ok = mbar_wait(b, (k >> 1) & 1);
-      if (__syncthreads_or(!ok)) {
-        // never expected: record it, give this tile's and the next tile's
-        // copies a second bounded wait so none lands after the block exits,
-        // and stop (decided for the whole block)
-        if (threadIdx.x == 0) {
-          atomicExch(err, 1);
-          mbar_wait(b, (k >> 1) & 1);
-          if (tn < ntiles) mbar_wait(smem_addr(&bars[(k + 1) & 1]), ((k + 1) >> 1) & 1);
-        }
-        return;
-      }
+      ok = mbar_wait(smem_addr(&bars[k & 1]), (k >> 1) & 1);
     } else {
       for (int idx = threadIdx.x; idx < C_IH * C_IW; idx += C_THREADS) {
         const int r = idx / C_IW, c = idx - r * C_IW;
@@ -967,13 +956,42 @@ __global__ __launch_bounds__(C_THREADS, 1) void box_coherence_kernel(const __gri
       }
       __syncthreads();
     }
+    // products once per staged pixel, in place: sr <- conj(r) s, ss <- (|r|^2, |s|^2);
+    // two pixels per 16-byte access (rows are 16-byte aligned).  A thread
+    // whose staging wait gave up works on whatever the stage holds: the
+    // barrier below then ends the whole block before any result is stored.
+    {
+      float4 *sr4 = reinterpret_cast<float4 *>(sr);
+      float4 *ss4 = reinterpret_cast<float4 *>(ss);
+      for (int idx = threadIdx.x; idx < C_IH * C_IW / 2; idx += C_THREADS) {
+        const float4 a4 = sr4[idx], b4 = ss4[idx];
+        float2 cp[2], pw[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const float2 a = h ? make_float2(a4.z, a4.w) : make_float2(a4.x, a4.y);
+          const float2 b = h ? make_float2(b4.z, b4.w) : make_float2(b4.x, b4.y);
+          cp[h] = __ffma2_rn(make_float2(a.y, -a.y), make_float2(b.y, b.x), __fmul2_rn(make_float2(a.x, a.x), b));
+          const float2 xx = make_float2(a.x, b.x), yy = make_float2(a.y, b.y);
+          pw[h] = __ffma2_rn(yy, yy, __fmul2_rn(xx, xx));
+        }
+        sr4[idx] = make_float4(cp[0].x, cp[0].y, cp[1].x, cp[1].y);
+        ss4[idx] = make_float4(pw[0].x, pw[0].y, pw[1].x, pw[1].y);
+      }
+    }
+    if (__syncthreads_or(!ok)) {
+      // never expected: record it, give this tile's and the next tile's copies
+      // a second bounded wait so none lands after the block exits, and stop
+      // (decided for the whole block)
+      if (threadIdx.x == 0) {
+        atomicExch(err, 1);
+        mbar_wait(smem_addr(&bars[k & 1]), (k >> 1) & 1);
+        if (t + gridDim.x < ntiles) mbar_wait(smem_addr(&bars[(k + 1) & 1]), ((k + 1) >> 1) & 1);
+      }
+      return;
+    }
     // Two output columns per thread, c and c + 1 of the tile: their windows
     // cover staged columns s0 .. s0 + WIN, read as 16-byte pairs from the
     // even column below s0; the WIN - 1 taps they share are summed once.
-    // The conj product and both powers of each pixel are formed here from
-    // the staged samples (no product pass through shared memory: a pixel's
-    // products are recomputed by the threads whose windows hold it, which
-    // costs FP32 work but saves a write and a read of the stage and a barrier).
     constexpr int O = HALF & 1;                   // s0 is odd exactly when HALF is
     constexpr int NPX = (WIN + 1 + O + 1) & ~1;   // staged pixels read per row
     const int c = 2 * tp;
@@ -986,19 +1004,14 @@ __global__ __launch_bounds__(C_THREADS, 1) void box_coherence_kernel(const __gri
     for (int j = 0; j < C_ROWS + WIN - 1; ++j) {
       const float4 *pr = reinterpret_cast<const float4 *>(sr + (first + j) * C_IW + cs);
       const float4 *pp = reinterpret_cast<const float4 *>(ss + (first + j) * C_IW + cs);
-      float2 vr[NPX], vp[NPX];  // conj(r) s and (|r|^2, |s|^2) per staged pixel
+      float2 vr[NPX], vp[NPX];
 #pragma unroll
       for (int k = 0; k < NPX / 2; ++k) {
-        const float4 a4 = pr[k], b4 = pp[k];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const float2 a = h ? make_float2(a4.z, a4.w) : make_float2(a4.x, a4.y);
-          const float2 bb = h ? make_float2(b4.z, b4.w) : make_float2(b4.x, b4.y);
-          vr[2 * k + h] =
-              __ffma2_rn(make_float2(a.y, -a.y), make_float2(bb.y, bb.x), __fmul2_rn(make_float2(a.x, a.x), bb));
-          const float2 xx = make_float2(a.x, bb.x), yy = make_float2(a.y, bb.y);
-          vp[2 * k + h] = __ffma2_rn(yy, yy, __fmul2_rn(xx, xx));
-        }
+        const float4 a = pr[k], b = pp[k];
+        vr[2 * k] = make_float2(a.x, a.y);
+        vr[2 * k + 1] = make_float2(a.z, a.w);
+        vp[2 * k] = make_float2(b.x, b.y);
+        vp[2 * k + 1] = make_float2(b.z, b.w);
       }
       float2 ir = make_float2(0.f, 0.f), ip = ir;  // taps shared by both windows
 #pragma unroll
