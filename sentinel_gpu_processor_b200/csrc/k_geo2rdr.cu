@@ -1015,6 +1015,9 @@ __global__ __launch_bounds__(kXmTX, 5) void frame_geo_xmul_kernel(const FrameDev
     constexpr int MASK = decltype(mask_tag)::value;
     row_terms(rb);
     int16_t hn = colin && rb < rlim ? __ldg(demc + (int64_t)rb * io.dem_pitch) : 0;
+    // two rows per trip: the second row's solve overlaps the first row's
+    // gathers (8.32 against 8.48 ms per frame, although it spills 36 bytes)
+#pragma unroll 2
     for (int r = rb; r < rend; ++r) {
       const double sinlat = __shfl_sync(0xffffffffu, r_sin, r & 31);
       const double coslat = __shfl_sync(0xffffffffu, r_cos, r & 31);
