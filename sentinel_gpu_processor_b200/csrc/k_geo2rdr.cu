@@ -991,6 +991,13 @@ __global__ __launch_bounds__(kXmTX, 5) void frame_geo_xmul_kernel(const FrameDev
   }
   __syncwarp();  // lane 0's patch and seed models are visible to the warp
   const TSrc *src0, *src1;
+  // tile rows [alo, ahi) of each burst's window at the thread's column
+  int alo[2], ahi[2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    alo[q] = max(0, -row0w[q]);
+    ahi[q] = colw[q] >= 0 ? max(alo[q], nrw[q] - row0w[q]) : alo[q];
+  }
   const double2 *tops0 = nullptr, *tops1 = nullptr;
   {
     const FrameBurst &f0 = d.bursts[pr.ref], &f1 = d.bursts[pr.sec];
@@ -1026,19 +1033,18 @@ __global__ __launch_bounds__(kXmTX, 5) void frame_geo_xmul_kernel(const FrameDev
       if (colin && r + 1 < rend && r + 1 < rlim) hn = __ldg(demc + (int64_t)(r + 1) * io.dem_pitch);
       double p[3];
       llh_point(sinlat, coslat, re, sinlon, coslon, hgt, p);
-      const int w0 = row0w[0] + r, w1 = row0w[1] + r;
-      const bool act[2] = {colw[0] >= 0 && w0 >= 0 && w0 < nrw[0], colw[1] >= 0 && w1 >= 0 && w1 < nrw[1]};
+      const bool act[2] = {r >= alo[0] && r < ahi[0], r >= alo[1] && r < ahi[1]};
       float2 v[2];
       geo_pair_pixel<TSrc, kFused, MASK>(sp, s_gc, &s_zd[0][wid], &s_zd[1][wid], &s_seed[0][wid], &s_seed[1][wid], p,
                                          hgt, r, colw, act,
                                          src0, src1, tops0, tops1, v);
       if ((MASK & 1) && (v[0].x != 0.f || v[0].y != 0.f)) {
-        rlo0 = min(rlo0, w0);
-        rhi0 = w0 + 1;
+        rlo0 = min(rlo0, r);
+        rhi0 = r + 1;
       }
       if ((MASK & 2) && (v[1].x != 0.f || v[1].y != 0.f)) {
-        rlo1 = min(rlo1, w1);
-        rhi1 = w1 + 1;
+        rlo1 = min(rlo1, r);
+        rhi1 = r + 1;
       }
       xm_accumulate(v[0], v[1], ir, ii, p1, p2);
       if (++lr == d.rowlook) {
@@ -1077,12 +1083,12 @@ __global__ __launch_bounds__(kXmTX, 5) void frame_geo_xmul_kernel(const FrameDev
   rhi1 = __reduce_max_sync(0xffffffffu, rhi1);
   if (lane == 0) {
     if (rhi0 >= 0) {
-      atomicMin(d.rows + 2 * pr.ref, rlo0);
-      atomicMax(d.rows + 2 * pr.ref + 1, rhi0);
+      atomicMin(d.rows + 2 * pr.ref, rlo0 + R0 - sp[0].win_top);
+      atomicMax(d.rows + 2 * pr.ref + 1, rhi0 + R0 - sp[0].win_top);
     }
     if (rhi1 >= 0) {
-      atomicMin(d.rows + 2 * pr.sec, rlo1);
-      atomicMax(d.rows + 2 * pr.sec + 1, rhi1);
+      atomicMin(d.rows + 2 * pr.sec, rlo1 + R0 - sp[1].win_top);
+      atomicMax(d.rows + 2 * pr.sec + 1, rhi1 + R0 - sp[1].win_top);
     }
   }
 }
