@@ -1159,53 +1159,49 @@ int resample_tma_slots() {
 // ------------------------------------------------- box coherence, row walk
 // Windows up to 5 x 5 (the coherence window of the chain).  One warp per
 // strip of 64 columns x W_ROWS output rows; each lane owns two adjacent
-// columns and walks down the strip.  Rows are brought into a per-warp ring
-// of W_PD shared-memory slots by cp.async (16 bytes per lane and array, zero
+// columns and walks down the strip.  Strips overlap by 4 columns: lanes 0
+// and 31 only supply their columns to their neighbours, lanes 1..30 produce
+// the strip's 60 output columns.  Rows are brought into a per-warp ring of
+// W_PD shared-memory slots by cp.async (16 bytes per lane and array, zero
 // fill outside the raster), W_PD - 1 rows ahead of the one being reduced, so
 // the copies in flight hold no registers; a lane reads back only what it
 // copied itself, so no barrier is needed.  Per row: the conj product and both
-// powers of the lane's two columns, the neighbours' values by two lane
-// rotations (lane 31 sends the strip's left halo pair to lane 0, lane 0 the
-// right halo pair to lane 31), horizontal sums, then a ring of the last WIN
-// rows' horizontal sums in registers: the complex channel slides with Kahan
-// compensation, the powers are summed directly over the ring (exact zeros
-// stay zero).  Everything between the HBM reads and the coherence store stays
-// in registers: 16 B read and 4 B written per pixel.
+// powers of the lane's two columns, the neighbours' by lane shuffles,
+// horizontal sums, then a ring of the last WIN rows' horizontal sums in
+// registers: the complex channel slides with Kahan compensation, the powers
+// are summed directly over the ring (exact zeros stay zero).  Between the HBM
+// reads and the coherence store everything stays in registers: 16 B read and
+// 4 B written per pixel.
 constexpr int W_ROWS = 64;  // output rows per strip
-constexpr int W_PD = 6;     // shared-memory row slots per warp (rows W_PD - 1 ahead)
+constexpr int W_PD = 4;     // shared-memory row slots per warp (rows W_PD - 1 ahead)
 constexpr int W_WARPS = 4;  // strips per CTA, side by side
+constexpr int W_OUT = 60;   // output columns per strip
 
-struct WalkSlot {  // one staged row of a warp's strip, ref and sec
-  float4 r[34], s[34];  // [lane]: the lane's column pair; [32]: left halo pair; [33]: right halo pair
+struct WalkSlot {  // one staged row of a warp's strip: the lanes' column pairs of ref and sec
+  float4 r[32], s[32];
 };
 
 template <bool kVec16>
-__device__ __forceinline__ void walk_copy_pair(float4 *dst, const float2 *row, const float2 *base, int col, int S,
-                                               bool rin) {
+__device__ __forceinline__ void walk_copy_pair(float4 *dst, const float2 *src, const float2 *base, bool in0,
+                                               bool in1) {
   if (kVec16) {  // S even, 16-byte rows: a pair is inside or outside as a whole
-    const bool in = rin && col >= 0 && col < S;
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_addr(dst)),
-                 "l"(in ? row + col : base), "r"(in ? 16 : 0)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_addr(dst)), "l"(in0 ? src : base),
+                 "r"(in0 ? 16 : 0)
                  : "memory");
   } else {
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const bool in = rin && col + h >= 0 && col + h < S;
-      asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(smem_addr(reinterpret_cast<float2 *>(dst) + h)),
-                   "l"(in ? row + col + h : base), "r"(in ? 8 : 0)
-                   : "memory");
-    }
+    const uint32_t d = smem_addr(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(in0 ? src : base), "r"(in0 ? 8 : 0)
+                 : "memory");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d + 8), "l"(in1 ? src + 1 : base),
+                 "r"(in1 ? 8 : 0)
+                 : "memory");
   }
 }
 
-// conj(a) b and (|a|^2, |b|^2) of one pixel
-__device__ __forceinline__ void walk_products(float2 a, float2 b, float2 &cp, float2 &pw) {
-  cp = __ffma2_rn(make_float2(a.y, -a.y), make_float2(b.y, b.x), __fmul2_rn(make_float2(a.x, a.x), b));
-  const float2 xx = make_float2(a.x, b.x), yy = make_float2(a.y, b.y);
-  pw = __ffma2_rn(yy, yy, __fmul2_rn(xx, xx));
+// conj(a) b and (|a|^2, |b|^2) of one pixel as (re, im, |a|^2, |b|^2)
+__device__ __forceinline__ float4 walk_products(float ax, float ay, float bx, float by) {
+  return make_float4(fmaf(ax, bx, ay * by), fmaf(ax, by, -(ay * bx)), fmaf(ax, ax, ay * ay), fmaf(bx, bx, by * by));
 }
-
-__device__ __forceinline__ float4 walk_pack(float2 c, float2 p) { return make_float4(c.x, c.y, p.x, p.y); }
 __device__ __forceinline__ float4 walk_add(float4 a, float4 b) {
   const float2 c = __fadd2_rn(make_float2(a.x, a.y), make_float2(b.x, b.y));
   const float2 p = __fadd2_rn(make_float2(a.z, a.w), make_float2(b.z, b.w));
@@ -1224,42 +1220,43 @@ __global__ __launch_bounds__(32 * W_WARPS) void box_walk_kernel(const float2 *__
   constexpr int WIN = 2 * HALF + 1;
   __shared__ WalkSlot slots[W_WARPS][W_PD];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int W0 = (blockIdx.x * W_WARPS + warp) * 64;  // first column of the strip
-  if (W0 >= S) return;                                 // warp-uniform; no block barrier below
+  const int W0 = (blockIdx.x * W_WARPS + warp) * W_OUT;  // first output column of the strip
+  if (W0 >= S) return;                                    // warp-uniform; no block barrier below
   const int y0 = blockIdx.y * W_ROWS;
   const int nout = min(W_ROWS, L - y0);
-  const int NR = nout + 2 * HALF;  // rows staged: y0 - HALF .. y0 + nout - 1 + HALF
-  const int c0 = W0 + 2 * lane;
+  const int NR = nout + 2 * HALF;    // rows staged: y0 - HALF .. y0 + nout - 1 + HALF
+  const int c0 = W0 - 2 + 2 * lane;  // the lane's first column
+  const bool in0 = c0 >= 0 && c0 < S, in1 = c0 + 1 >= 0 && c0 + 1 < S;
+  const bool out_lane = lane >= 1 && lane <= 30;
   WalkSlot *ring = slots[warp];
-  auto stage = [&](int j) {  // row j of the walk into slot j % W_PD
-    const int y = y0 - HALF + j;
-    const bool rin = y >= 0 && y < L;
-    const size_t off = (size_t)(rin ? y : 0) * S;
-    WalkSlot &sl = ring[j % W_PD];
-    walk_copy_pair<kVec16>(&sl.r[lane], ref + off, ref, c0, S, rin);
-    walk_copy_pair<kVec16>(&sl.s[lane], sec + off, sec, c0, S, rin);
-    if (HALF > 0 && lane == 31) {
-      walk_copy_pair<kVec16>(&sl.r[32], ref + off, ref, W0 - 2, S, rin);
-      walk_copy_pair<kVec16>(&sl.s[32], sec + off, sec, W0 - 2, S, rin);
-    }
-    if (HALF > 0 && lane == 0) {
-      walk_copy_pair<kVec16>(&sl.r[33], ref + off, ref, W0 + 64, S, rin);
-      walk_copy_pair<kVec16>(&sl.s[33], sec + off, sec, W0 + 64, S, rin);
-    }
+  // the lane's pair of the next row to stage, and that row
+  int ys = y0 - HALF;
+  const float2 *pr = ref + (ptrdiff_t)ys * S + c0, *ps = sec + (ptrdiff_t)ys * S + c0;
+  auto stage = [&](int slot) {
+    const bool rin = (unsigned)ys < (unsigned)L;
+    WalkSlot &sl = ring[slot];
+    walk_copy_pair<kVec16>(&sl.r[lane], pr, ref, rin && in0, rin && in1);
+    walk_copy_pair<kVec16>(&sl.s[lane], ps, sec, rin && in0, rin && in1);
+    ++ys;
+    pr += S;
+    ps += S;
   };
 #pragma unroll
   for (int j = 0; j < W_PD - 1; ++j) {
     if (j < NR) stage(j);
     asm volatile("cp.async.commit_group;" ::: "memory");
   }
-  // rings of the last WIN rows' horizontal sums: complex (rc) and powers (rp),
-  // columns c0 (index 0) and c0 + 1 (index 1)
+  // rings of the last WIN rows' horizontal sums, complex (rc) and powers (rp),
+  // of the lane's columns c0 (index 0) and c0 + 1 (index 1)
   float2 rc[WIN][2], rp[WIN][2];
 #pragma unroll
   for (int u = 0; u < WIN; ++u)
 #pragma unroll
     for (int q = 0; q < 2; ++q) rc[u][q] = rp[u][q] = make_float2(0.f, 0.f);
   Kahan2 vs[2];
+  float *dst = coh + (ptrdiff_t)y0 * S + c0;  // output row y0 - 2 HALF + j at step j >= 2 HALF
+  dst -= (ptrdiff_t)2 * HALF * S;
+  static_assert((W_PD & (W_PD - 1)) == 0, "ring slots are taken modulo a power of two");
   for (int jb = 0; jb < NR; jb += WIN) {
 #pragma unroll
     for (int u = 0; u < WIN; ++u) {
@@ -1267,38 +1264,26 @@ __global__ __launch_bounds__(32 * W_WARPS) void box_walk_kernel(const float2 *__
       if (j >= NR) break;  // warp-uniform
       // this lane's copies of row j have landed (rows j + 1 .. j + W_PD - 2 may still fly)
       asm volatile("cp.async.wait_group %0;" ::"n"(W_PD - 2) : "memory");
-      const WalkSlot &sl = ring[j % W_PD];
+      const WalkSlot &sl = ring[j & (W_PD - 1)];
       const float4 ra = sl.r[lane], sa = sl.s[lane];
-      float2 ca, pa, cb, pb;  // the lane's two columns
-      walk_products(make_float2(ra.x, ra.y), make_float2(sa.x, sa.y), ca, pa);
-      walk_products(make_float2(ra.z, ra.w), make_float2(sa.z, sa.w), cb, pb);
-      const float4 Pa = walk_pack(ca, pa), Pb = walk_pack(cb, pb);
-      float4 Ha = Pa, Hb = Pb;  // horizontal sums of the two columns
+      const float4 Pa = walk_products(ra.x, ra.y, sa.x, sa.y), Pb = walk_products(ra.z, ra.w, sa.z, sa.w);
+      // the slot of row j - 1 is free (its values were consumed a step ago): stage row j + W_PD - 1
+      if (j + W_PD - 1 < NR) stage((j + W_PD - 1) & (W_PD - 1));
+      asm volatile("cp.async.commit_group;" ::: "memory");
+      float4 Ha = Pa, Hb = Pb;  // horizontal sums of the lane's two columns
       if (HALF > 0) {
-        // the halo pair this lane forwards (lane 31: left halo, lane 0: right halo)
-        const int hi = lane == 31 ? 32 : 33;
-        const float4 rh = sl.r[hi], sh = sl.s[hi];
-        float2 cx, px, cy, py;
-        walk_products(make_float2(rh.x, rh.y), make_float2(sh.x, sh.y), cx, px);
-        walk_products(make_float2(rh.z, rh.w), make_float2(sh.z, sh.w), cy, py);
-        const float4 Qa = walk_pack(cx, px), Qb = walk_pack(cy, py);
         const float4 A = walk_add(Pa, Pb);
-        // left neighbour's second column (and pair sum), right neighbour's first (and pair sum)
-        const float4 Lb = walk_shfl(lane == 31 ? Qb : Pb, (lane + 31) & 31);
-        const float4 Ra = walk_shfl(lane == 0 ? Qa : Pa, (lane + 1) & 31);
+        const float4 Lb = walk_shfl(Pb, lane - 1);  // lane 0 gets its own: not an output lane
+        const float4 Ra = walk_shfl(Pa, lane + 1);  // lane 31 likewise
         if (HALF == 1) {
           Ha = walk_add(Lb, A);
           Hb = walk_add(A, Ra);
         } else {
-          const float4 LA = walk_shfl(lane == 31 ? walk_add(Qa, Qb) : A, (lane + 31) & 31);
-          const float4 RA = walk_shfl(lane == 0 ? walk_add(Qa, Qb) : A, (lane + 1) & 31);
+          const float4 LA = walk_shfl(A, lane - 1), RA = walk_shfl(A, lane + 1);
           Ha = walk_add(walk_add(LA, A), Ra);
           Hb = walk_add(walk_add(Lb, A), RA);
         }
       }
-      // the slot of row j - 1 is free (its values were consumed above): stage row j + W_PD - 1
-      if (j + W_PD - 1 < NR) stage(j + W_PD - 1);
-      asm volatile("cp.async.commit_group;" ::: "memory");
       const float2 hc[2] = {make_float2(Ha.x, Ha.y), make_float2(Hb.x, Hb.y)};
       const float2 hp[2] = {make_float2(Ha.z, Ha.w), make_float2(Hb.z, Hb.w)};
 #pragma unroll
@@ -1308,8 +1293,7 @@ __global__ __launch_bounds__(32 * W_WARPS) void box_walk_kernel(const float2 *__
         rp[u][q] = hp[q];
         vs[q].add(hc[q]);
       }
-      if (j >= 2 * HALF) {
-        const int y = y0 + j - 2 * HALF;
+      if (j >= 2 * HALF && out_lane) {
         float out[2];
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
@@ -1321,14 +1305,14 @@ __global__ __launch_bounds__(32 * W_WARPS) void box_walk_kernel(const float2 *__
           const float num2 = fmaf(v.x, v.x, v.y * v.y);
           out[q] = den2 > 0.f ? sqrtf(num2) * rsqrtf(den2) : 0.f;
         }
-        float *dst = coh + (size_t)y * S + c0;
         if (kVec16) {
-          if (c0 < S) __stcs(reinterpret_cast<float2 *>(dst), make_float2(out[0], out[1]));
+          if (in0) __stcs(reinterpret_cast<float2 *>(dst), make_float2(out[0], out[1]));
         } else {
-          if (c0 < S) __stcs(dst, out[0]);
-          if (c0 + 1 < S) __stcs(dst + 1, out[1]);
+          if (in0) __stcs(dst, out[0]);
+          if (in1) __stcs(dst + 1, out[1]);
         }
       }
+      dst += S;
     }
   }
 }
@@ -1337,7 +1321,7 @@ template <int HALF>
 int launch_walk(const void *ref, const void *sec, int lines, int samples, float *coh, cudaStream_t st) {
   const bool vec16 = samples % 2 == 0 && reinterpret_cast<uintptr_t>(ref) % 16 == 0 &&
                      reinterpret_cast<uintptr_t>(sec) % 16 == 0 && reinterpret_cast<uintptr_t>(coh) % 8 == 0;
-  const dim3 grid((samples + 64 * W_WARPS - 1) / (64 * W_WARPS), (lines + W_ROWS - 1) / W_ROWS);
+  const dim3 grid((samples + W_OUT * W_WARPS - 1) / (W_OUT * W_WARPS), (lines + W_ROWS - 1) / W_ROWS);
   if (vec16)
     box_walk_kernel<HALF, true><<<grid, 32 * W_WARPS, 0, st>>>((const float2 *)ref, (const float2 *)sec, lines,
                                                                 samples, coh);
