@@ -313,6 +313,23 @@ def speckle(lines, samples, gen, device):
     return torch.view_as_complex(z)
 
 
+def band_limited_speckle(lines, samples, gen, device, band=0.8):
+    """Unit-power circular-Gaussian speckle whose spectrum is flat over the
+    central ``band`` of the sampling rate in both axes and zero outside (a
+    Sentinel-1 SLC is oversampled by about 1.2 in range and azimuth).  Values
+    between samples are then fixed by the samples, so two grids that sample
+    one scene at shifted positions see correlated values."""
+    import torch
+    z = torch.fft.fft2(speckle(lines, samples, gen, device))
+    ka = torch.fft.fftfreq(lines, device=device).abs() <= band / 2
+    kr = torch.fft.fftfreq(samples, device=device).abs() <= band / 2
+    z *= ka[:, None].to(z.dtype)
+    z *= kr[None, :].to(z.dtype)
+    z = torch.fft.ifft2(z)
+    z /= math.sqrt(float(ka.sum()) * float(kr.sum()) / (lines * samples))
+    return z.to(torch.complex64)
+
+
 def tops_modulate(slc, acq: Acquisition, burst: Burst, sign=+1.0):
     """Multiply by exp(sign * i pi kt (eta - etaref)^2) (inverse of the deramp)."""
     import torch
@@ -656,26 +673,92 @@ def make_stack(seed=20261203 + 5000, device="cpu", n_sec=29, n_bursts=9, lines=1
                       extra={"hmax": hmax})
 
 
+def _stack_cache(st: StackScene, name: str) -> dict:
+    return st.extra.setdefault(name, {})
+
+
+def stack_reference_field(st: StackScene, burst: int, device):
+    """The scene of reference burst ``burst`` on its own sample grid, before
+    the TOPS modulation: band-limited speckle seeded per burst (cached)."""
+    import torch
+    cache = _stack_cache(st, "_field")
+    if burst not in cache:
+        gen = torch.Generator(device=device)
+        gen.manual_seed(st.seed * 1000 + burst)
+        cache[burst] = band_limited_speckle(st.lines, st.samples, gen, device)
+    return cache[burst]
+
+
+def stack_reference_geometry(st: StackScene, burst: int, device):
+    """float64 lat/lon/height rasters of reference burst ``burst``'s samples
+    on the stack's terrain (``rdr2geo_grid``; cached)."""
+    cache = _stack_cache(st, "_geom")
+    if burst not in cache:
+        acq = st.ref[burst]
+        hmax = st.extra["hmax"]
+        cache[burst] = rdr2geo_grid(acq.orbit, acq.radar, acq.bursts[0],
+                                    lambda la, lo: fbm_height(la, lo, st.seed, hmax), device=device)
+    return cache[burst]
+
+
+def locked_to_reference(field, ref: Acquisition, sec: Acquisition, lat, lon, hgt):
+    """``field``, given on the reference burst's sample grid, as the secondary
+    acquisition ``sec`` sees it: the value at secondary sample q is the field
+    at the reference position p of the same ground point, p + off(p) = q,
+    where off is the secondary's geo2rdr of the reference grid (``lat``,
+    ``lon``, ``hgt``).  p is found by fixed-point iteration on the bilinearly
+    sampled offsets and the field read there by the 8-tap sinc (the s1b
+    resampler with the TOPS steering set to zero, i.e. no deramp).  Needs
+    CUDA tensors."""
+    import dataclasses
+
+    import torch
+    import torch.nn.functional as F
+
+    from . import kernels, plan as _plan
+    pl = _plan.burst_plan(sec.radar, sec.orbit, sec.fm, sec.dc, sec.bursts[0], None)
+    az, rg = kernels.geo2rdr_offsets(pl, lat, lon, hgt)
+    L, S = az.shape
+    dev = az.device
+    qa = torch.arange(L, device=dev, dtype=torch.float32)[:, None]
+    qr = torch.arange(S, device=dev, dtype=torch.float32)[None, :]
+    off = torch.stack([rg, az])[None]  # grid_sample's x is the range axis
+    da, dr = -az, -rg                   # p - q
+    for _ in range(3):
+        g = torch.stack([(qr + dr) * (2.0 / (S - 1)) - 1.0, (qa + da) * (2.0 / (L - 1)) - 1.0], -1)[None]
+        o = F.grid_sample(off, g, mode="bilinear", padding_mode="border", align_corners=True)[0]
+        dr, da = -o[0], -o[1]
+        del g, o
+    flat = dataclasses.replace(ref.radar, azimuth_steering_rate=0.0)
+    pl0 = _plan.burst_plan(flat, ref.orbit, ref.fm, ref.dc, ref.bursts[0], None)
+    return kernels.resample(pl0, field.contiguous(), da.contiguous(), dr.contiguous())
+
+
 def stack_slc(st: StackScene, date: int, burst: int, device="cpu"):
     """SLC of burst ``burst`` of date ``date`` (-1: the reference), TOPS-
-    modulated: the reference is unit circular-Gaussian speckle seeded per
-    burst; date d mixes it with its own speckle at the date's coherence and
-    adds the deformation phase 4 pi / wvl * rate * dt, the rate a ramp from 0
-    at near range to 1 cm/yr at far range."""
+    modulated.  The reference is band-limited speckle seeded per burst on its
+    own grid; date d sees that scene from its own orbit: the same ground
+    points at its own sample positions (``locked_to_reference``), mixed with
+    its own band-limited speckle at the date's coherence, plus the
+    deformation phase 4 pi / wvl * rate * dt, the rate a ramp from 0 at near
+    range to 1 cm/yr at far range.  Geocoded pairs are then coherent at the
+    date's coherence (less the interpolation's own loss).  Secondary dates
+    need CUDA (they use the s1b geo2rdr and resampler)."""
     import torch
     L, S = st.lines, st.samples
-    gen = torch.Generator(device=device)
-    gen.manual_seed(st.seed * 1000 + burst)
-    s = speckle(L, S, gen, device)
+    f = stack_reference_field(st, burst, device)
     if date < 0:
-        return tops_modulate(s, st.ref[burst], st.ref[burst].bursts[0]).contiguous()
+        return tops_modulate(f, st.ref[burst], st.ref[burst].bursts[0]).contiguous()
+    acq = st.sec[date][burst]
+    lat, lon, hgt = stack_reference_geometry(st, burst, device)
+    s = locked_to_reference(f, st.ref[burst], acq, lat, lon, hgt)
+    gen = torch.Generator(device=device)
     gen.manual_seed(st.seed * 1000 + 100000 * (date + 1) + burst)
     g = st.coherence[date]
-    s = g * s + math.sqrt(1 - g * g) * speckle(L, S, gen, device)
+    s = g * s + math.sqrt(1 - g * g) * band_limited_speckle(L, S, gen, device)
     ramp = torch.linspace(0.0, 1.0, S, dtype=torch.float64, device=device)
     phase = (4 * math.pi / WAVELENGTH * st.defo_rate * st.days[date] / 365.25) * ramp
     s = s * torch.polar(torch.ones_like(phase), phase).to(torch.complex64)[None, :]
-    acq = st.sec[date][burst]
     return tops_modulate(s, acq, acq.bursts[0]).contiguous()
 
 
