@@ -689,15 +689,33 @@ def stack_reference_field(st: StackScene, burst: int, device):
     return cache[burst]
 
 
+def dem_height_fn(rsc: formats.Rsc, dem):
+    """The terrain of a DEM raster as a function of (lat, lon) in degrees:
+    bilinear interpolation of its heights (float64), clamped at its edges."""
+    import torch
+    h = dem.to(torch.float64)
+    n0, n1 = h.shape
+
+    def fn(lat, lon):
+        y = ((lat - rsc.latmax) / rsc.dlat).clamp(0.0, n0 - 1.0)
+        x = ((lon - rsc.lonmin) / rsc.dlon).clamp(0.0, n1 - 1.0)
+        y0 = y.floor().clamp(max=n0 - 2).long()
+        x0 = x.floor().clamp(max=n1 - 2).long()
+        fy, fx = y - y0, x - x0
+        a, b = h[y0, x0], h[y0, x0 + 1]
+        c, d = h[y0 + 1, x0], h[y0 + 1, x0 + 1]
+        return (a + fx * (b - a)) + fy * ((c + fx * (d - c)) - (a + fx * (b - a)))
+    return fn
+
+
 def stack_reference_geometry(st: StackScene, burst: int, device):
     """float64 lat/lon/height rasters of reference burst ``burst``'s samples
-    on the stack's terrain (``rdr2geo_grid``; cached)."""
+    on the stack's DEM, interpolated bilinearly (``rdr2geo_grid``; cached)."""
     cache = _stack_cache(st, "_geom")
     if burst not in cache:
         acq = st.ref[burst]
-        hmax = st.extra["hmax"]
-        cache[burst] = rdr2geo_grid(acq.orbit, acq.radar, acq.bursts[0],
-                                    lambda la, lo: fbm_height(la, lo, st.seed, hmax), device=device)
+        cache[burst] = rdr2geo_grid(acq.orbit, acq.radar, acq.bursts[0], dem_height_fn(st.rsc, st.dem.to(device)),
+                                    device=device)
     return cache[burst]
 
 
@@ -708,8 +726,10 @@ def locked_to_reference(field, ref: Acquisition, sec: Acquisition, lat, lon, hgt
     where off is the secondary's geo2rdr of the reference grid (``lat``,
     ``lon``, ``hgt``).  p is found by fixed-point iteration on the bilinearly
     sampled offsets and the field read there by the 8-tap sinc (the s1b
-    resampler with the TOPS steering set to zero, i.e. no deramp).  Needs
-    CUDA tensors."""
+    resampler with the TOPS steering set to zero, i.e. no deramp); its phase
+    moves by the change of the point's two-way path between the orbits, so
+    that the geocoding, which adds 4 pi R / wvl at each burst's own range,
+    brings both back to one value.  Needs CUDA tensors."""
     import dataclasses
 
     import torch
@@ -731,7 +751,12 @@ def locked_to_reference(field, ref: Acquisition, sec: Acquisition, lat, lon, hgt
         del g, o
     flat = dataclasses.replace(ref.radar, azimuth_steering_rate=0.0)
     pl0 = _plan.burst_plan(flat, ref.orbit, ref.fm, ref.dc, ref.bursts[0], None)
-    return kernels.resample(pl0, field.contiguous(), da.contiguous(), dr.contiguous())
+    out = kernels.resample(pl0, field.contiguous(), da.contiguous(), dr.contiguous())
+    # each ground point's two-way path changes by R_sec - R_ref = dR (q_s - p_s):
+    # its phase by -4 pi dR (q_s - p_s) / wvl = 4 pi dR dr / wvl
+    k = 4.0 * math.pi * (SOL / 2.0 / sec.radar.range_sampling_rate) / sec.radar.wvl
+    ph = torch.remainder(k * dr.double(), 2 * math.pi)
+    return out * torch.polar(torch.ones_like(ph), ph).to(torch.complex64)
 
 
 def stack_slc(st: StackScene, date: int, burst: int, device="cpu"):
@@ -812,12 +837,14 @@ def _xyz2llh_t(x, y, z):
     return torch.rad2deg(lat), torch.rad2deg(lon), h
 
 
-def rdr2geo_grid(orbit, radar, burst, height_fn, device="cpu", outer=4, steps=44):
+def rdr2geo_grid(orbit, radar, burst, height_fn, device="cpu", steps=44):
     """Ground point of every pixel of a burst: zero-Doppler plane at the line
     time, slant range of the sample, on the terrain ``height_fn(lat, lon)``.
 
     Bisection on the look angle in the plane orthogonal to the velocity
-    (right-looking), iterated ``outer`` times against the terrain height.
+    (right-looking) for the point where the look ray meets the terrain (the
+    ray's height minus the terrain's there changes sign; under layover, one
+    of the crossings).
     Returns float64 (lat, lon, hgt) tensors [lines, samples]."""
     import torch
 
@@ -836,27 +863,24 @@ def rdr2geo_grid(orbit, radar, burst, height_fn, device="cpu", outer=4, steps=44
     c = c / torch.linalg.norm(c, dim=1, keepdim=True)
     r0 = radar.slant_range_time * SOL / 2.0
     R = (r0 + (SOL / 2.0 / radar.range_sampling_rate) * torch.arange(S, dtype=torch.float64, device=device))[None, :]
-    h = torch.zeros((L, S), dtype=torch.float64, device=device)
-    for _ in range(outer):
-        lo = torch.zeros((L, S), dtype=torch.float64, device=device)
-        hi = torch.full((L, S), math.radians(80.0), dtype=torch.float64, device=device)
-        for _ in range(steps):
-            th = 0.5 * (lo + hi)
-            ct, st = torch.cos(th), torch.sin(th)
-            gx = P[:, 0:1] + R * (ct * d[:, 0:1] + st * c[:, 0:1])
-            gy = P[:, 1:2] + R * (ct * d[:, 1:2] + st * c[:, 1:2])
-            gz = P[:, 2:3] + R * (ct * d[:, 2:3] + st * c[:, 2:3])
-            _, _, hg = _xyz2llh_t(gx, gy, gz)
-            up = hg > h  # the ray rises with the angle
-            hi = torch.where(up, th, hi)
-            lo = torch.where(up, lo, th)
-        th = 0.5 * (lo + hi)
+    lo = torch.zeros((L, S), dtype=torch.float64, device=device)
+    hi = torch.full((L, S), math.radians(80.0), dtype=torch.float64, device=device)
+
+    def ray_point(th):
         ct, st = torch.cos(th), torch.sin(th)
         gx = P[:, 0:1] + R * (ct * d[:, 0:1] + st * c[:, 0:1])
         gy = P[:, 1:2] + R * (ct * d[:, 1:2] + st * c[:, 1:2])
         gz = P[:, 2:3] + R * (ct * d[:, 2:3] + st * c[:, 2:3])
-        lat, lon, hg = _xyz2llh_t(gx, gy, gz)
-        h = height_fn(lat, lon).to(torch.float64)
+        return _xyz2llh_t(gx, gy, gz)
+
+    for _ in range(steps):
+        th = 0.5 * (lo + hi)
+        lat, lon, hg = ray_point(th)
+        up = hg > height_fn(lat, lon).to(torch.float64)  # the ray point is above the terrain
+        hi = torch.where(up, th, hi)
+        lo = torch.where(up, lo, th)
+        del lat, lon, hg, up
+    lat, lon, hg = ray_point(0.5 * (lo + hi))
     return lat.contiguous(), lon.contiguous(), hg.contiguous()
 
 
