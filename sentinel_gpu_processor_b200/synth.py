@@ -715,7 +715,7 @@ def stack_reference_geometry(st: StackScene, burst: int, device):
     if burst not in cache:
         acq = st.ref[burst]
         cache[burst] = rdr2geo_grid(acq.orbit, acq.radar, acq.bursts[0], dem_height_fn(st.rsc, st.dem.to(device)),
-                                    device=device)
+                                    device=device, terrain=True)
     return cache[burst]
 
 
@@ -837,14 +837,18 @@ def _xyz2llh_t(x, y, z):
     return torch.rad2deg(lat), torch.rad2deg(lon), h
 
 
-def rdr2geo_grid(orbit, radar, burst, height_fn, device="cpu", steps=44):
+def rdr2geo_grid(orbit, radar, burst, height_fn, device="cpu", outer=4, steps=44, terrain=False):
     """Ground point of every pixel of a burst: zero-Doppler plane at the line
     time, slant range of the sample, on the terrain ``height_fn(lat, lon)``.
 
     Bisection on the look angle in the plane orthogonal to the velocity
-    (right-looking) for the point where the look ray meets the terrain (the
-    ray's height minus the terrain's there changes sign; under layover, one
-    of the crossings).
+    (right-looking).  ``terrain=True``: for the point where the look ray
+    meets the terrain (the ray's height minus the terrain's there changes
+    sign; under layover, one of the crossings).  Otherwise ``outer`` rounds
+    of: the ray point at the height of the terrain found under the previous
+    round's point; on rough terrain these rounds need not reach the surface,
+    but the rasters are still points of the pixels' own look rays (the
+    radar-grid scenes use them as given).
     Returns float64 (lat, lon, hgt) tensors [lines, samples]."""
     import torch
 
@@ -863,8 +867,6 @@ def rdr2geo_grid(orbit, radar, burst, height_fn, device="cpu", steps=44):
     c = c / torch.linalg.norm(c, dim=1, keepdim=True)
     r0 = radar.slant_range_time * SOL / 2.0
     R = (r0 + (SOL / 2.0 / radar.range_sampling_rate) * torch.arange(S, dtype=torch.float64, device=device))[None, :]
-    lo = torch.zeros((L, S), dtype=torch.float64, device=device)
-    hi = torch.full((L, S), math.radians(80.0), dtype=torch.float64, device=device)
 
     def ray_point(th):
         ct, st = torch.cos(th), torch.sin(th)
@@ -873,14 +875,23 @@ def rdr2geo_grid(orbit, radar, burst, height_fn, device="cpu", steps=44):
         gz = P[:, 2:3] + R * (ct * d[:, 2:3] + st * c[:, 2:3])
         return _xyz2llh_t(gx, gy, gz)
 
-    for _ in range(steps):
-        th = 0.5 * (lo + hi)
-        lat, lon, hg = ray_point(th)
-        up = hg > height_fn(lat, lon).to(torch.float64)  # the ray point is above the terrain
-        hi = torch.where(up, th, hi)
-        lo = torch.where(up, lo, th)
-        del lat, lon, hg, up
-    lat, lon, hg = ray_point(0.5 * (lo + hi))
+    def bisect(below):  # the look angle where below(lat, lon, h) turns false
+        lo = torch.zeros((L, S), dtype=torch.float64, device=device)
+        hi = torch.full((L, S), math.radians(80.0), dtype=torch.float64, device=device)
+        for _ in range(steps):
+            th = 0.5 * (lo + hi)
+            up = ~below(*ray_point(th))
+            hi = torch.where(up, th, hi)
+            lo = torch.where(up, lo, th)
+        return 0.5 * (lo + hi)
+
+    if terrain:
+        return tuple(x.contiguous() for x in
+                     ray_point(bisect(lambda la, lo_, hg: hg <= height_fn(la, lo_).to(torch.float64))))
+    h = torch.zeros((L, S), dtype=torch.float64, device=device)
+    for _ in range(outer):
+        lat, lon, hg = ray_point(bisect(lambda la, lo_, hg_: hg_ <= h))
+        h = height_fn(lat, lon).to(torch.float64)
     return lat.contiguous(), lon.contiguous(), hg.contiguous()
 
 
