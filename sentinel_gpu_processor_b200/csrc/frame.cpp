@@ -172,7 +172,8 @@ extern "C" int s1b_frame_create(const s1b_burst_plan_t *plans, int32_t n_bursts,
     fb.slc_off = slc;
     slc += (int64_t)p.lines * p.samples;
     fb.der_off = work;
-    work = align_up(work + (int64_t)p.lines * p.samples);
+    // the deramped copy, or (fused deramp) the two TOPS column tables of 32 B per column
+    work = align_up(work + (int64_t)std::max(p.lines, 4) * p.samples);
   }
   for (int b = 0; b < n_bursts; ++b) {
     f->bursts[b].geo_off = work;

@@ -757,17 +757,25 @@ __device__ __forceinline__ void frame_geo_tile(const PlanTail &sp, const s1b_orb
                                     fb.nrow, fb.ncol, tx, ty, cull);
 }
 
-// Per-column TOPS coefficients (-kt, etaref) of every burst for the fused
-// geocoding: blockIdx.y = burst, a thread per column, written as double2
-// into the burst's deramped-copy slot of the workspace (unused when fused).
+// Per-column TOPS coefficients of every burst for the fused geocoding:
+// blockIdx.y = burst, a thread per column, written into the burst's
+// deramped-copy slot of the workspace (unused when fused): S double2
+// (-kt, etaref) for the per-burst gathers, then S float4 (kt, kt' - kt,
+// etaref' - etaref, etaref) with ' the next column, the differences formed in
+// FP64, for the pair kernel's FP32 phase differences.
 __global__ void frame_tops_table_kernel(const FrameDev d, const FrameIO io) {
   const int b = blockIdx.y;
   const s1b_burst_plan_t &sp = d.plans[b];
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= sp.samples) return;
-  double kt, eref;
+  double kt, eref, kt1 = 0.0, eref1 = 0.0;
   tops_kt(sp, c, kt, eref);
-  reinterpret_cast<double2 *>(io.work + d.bursts[b].der_off)[c] = make_double2(-kt, eref);
+  if (c + 1 < sp.samples) tops_kt(sp, c + 1, kt1, eref1);
+  double2 *slot = reinterpret_cast<double2 *>(io.work + d.bursts[b].der_off);
+  slot[c] = make_double2(-kt, eref);
+  reinterpret_cast<float4 *>(slot + sp.samples)[c] =
+      c + 1 < sp.samples ? make_float4((float)kt, (float)(kt1 - kt), (float)(eref1 - eref), (float)eref)
+                         : make_float4((float)kt, 0.f, 0.f, (float)eref);
 }
 
 // Minimum resident CTAs the frame's geocoding kernels are compiled for: 72
@@ -847,8 +855,8 @@ __device__ __forceinline__ void geo_pair_pixel(const PlanTail *sp, const GeoCons
                                                const ZeroDopplerPatch *zd1, const double4 *m0, const double4 *m1,
                                                const double p[3], double hgt, int r, const int *colw,
                                                const bool *act, const TSrc *__restrict__ src0,
-                                               const TSrc *__restrict__ src1, const double2 *__restrict__ tops0,
-                                               const double2 *__restrict__ tops1, float2 *v) {
+                                               const TSrc *__restrict__ src1, const float4 *__restrict__ tops0,
+                                               const float4 *__restrict__ tops1, float2 *v) {
   double h[2], r2[2];
 #pragma unroll
   for (int q = 0; q < 2; ++q) {
@@ -881,11 +889,10 @@ __device__ __forceinline__ void geo_pair_pixel(const PlanTail *sp, const GeoCons
     const size_t i1 = (size_t)inta * P.samples + intr;
     const double eta = -P.lines * P.dtaz / 2. + t - P.tstart;
     if constexpr (kFused) {
-      const double2 *tops = q ? tops1 : tops0;
-      const double2 c0 = __ldg(tops + intr), c1 = __ldg(tops + intr + 1);  // (-kt, etaref)
+      const float4 tc = __ldg((q ? tops1 : tops0) + intr);  // (kt, kt' - kt, etaref' - etaref, etaref)
       const double ea = deramp_eta(P, inta);
-      const float k0 = (float)(-c0.x), dk = (float)(c0.x - c1.x), de = (float)(c1.y - c0.y);
-      const float u = (float)(ea - c0.y), ati = (float)P.ati;
+      const float k0 = tc.x, dk = tc.y, de = tc.z;
+      const float u = (float)ea - tc.w, ati = (float)P.ati;
       const float w = fmaf(-fr, de, (float)(eta - ea));
       const float ub = u + ati, wb = w - ati, e = u + w;
       const float kfe = fr * dk * e * e;
@@ -998,14 +1005,14 @@ __global__ __launch_bounds__(kXmTX, 5) void frame_geo_xmul_kernel(const FrameDev
     alo[q] = max(0, -row0w[q]);
     ahi[q] = colw[q] >= 0 ? max(alo[q], nrw[q] - row0w[q]) : alo[q];
   }
-  const double2 *tops0 = nullptr, *tops1 = nullptr;
+  const float4 *tops0 = nullptr, *tops1 = nullptr;
   {
     const FrameBurst &f0 = d.bursts[pr.ref], &f1 = d.bursts[pr.sec];
     if constexpr (kFused) {
       src0 = static_cast<const TSrc *>(io.slc) + f0.slc_off;
       src1 = static_cast<const TSrc *>(io.slc) + f1.slc_off;
-      tops0 = reinterpret_cast<const double2 *>(io.work + f0.der_off);
-      tops1 = reinterpret_cast<const double2 *>(io.work + f1.der_off);
+      tops0 = reinterpret_cast<const float4 *>(io.work + f0.der_off) + sp[0].samples;
+      tops1 = reinterpret_cast<const float4 *>(io.work + f1.der_off) + sp[1].samples;
     } else {
       src0 = reinterpret_cast<const TSrc *>(io.work + f0.der_off);
       src1 = reinterpret_cast<const TSrc *>(io.work + f1.der_off);
