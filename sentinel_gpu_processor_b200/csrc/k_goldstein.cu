@@ -73,7 +73,9 @@ __host__ __device__ constexpr int brev5(int i) {
 
 // One radix-2 stage (butterfly span m = 2^S) of the 32-point FFT; a template
 // per stage so that every index is a compile-time constant and x stays in
-// registers.
+// registers.  The twiddles 1 and -+i are applied as copies and swaps: the
+// same values the multiplication gives for finite samples, without its
+// multiplies (46 of the 80 butterflies of a transform).
 template <int S, bool kInverse>
 __device__ __forceinline__ void fft32_stage(float2 (&x)[GN]) {
   constexpr int m = 1 << S, half = m >> 1, stride = GN / m;
@@ -81,10 +83,18 @@ __device__ __forceinline__ void fft32_stage(float2 (&x)[GN]) {
   for (int k = 0; k < GN; k += m) {
 #pragma unroll
     for (int j = 0; j < half; ++j) {
-      float2 w = c_tw[j * stride];
-      if (!kInverse) w.y = -w.y;
+      const int tw = j * stride;
       const float2 b = x[k + j + half];
-      const float2 t = make_float2(w.x * b.x - w.y * b.y, w.x * b.y + w.y * b.x);
+      float2 t;
+      if (tw == 0) {
+        t = b;
+      } else if (tw == GN / 4) {  // exp(-+i pi / 2)
+        t = kInverse ? make_float2(-b.y, b.x) : make_float2(b.y, -b.x);
+      } else {
+        float2 w = c_tw[tw];
+        if (!kInverse) w.y = -w.y;
+        t = make_float2(w.x * b.x - w.y * b.y, w.x * b.y + w.y * b.x);
+      }
       const float2 u = x[k + j];
       x[k + j] = make_float2(u.x + t.x, u.y + t.y);
       x[k + j + half] = make_float2(u.x - t.x, u.y - t.y);
