@@ -84,6 +84,9 @@ def parse():
     ap.add_argument("--samples", default="c64", choices=["ci16", "c64"],
                     help="frame SLC sample type: complex int16 as in the measurement TIFF (widened on the GPU), "
                          "or complex64 as the reference's geo2rdr pipe carries it")
+    ap.add_argument("--write-pair0", metavar="DIR", default=None,
+                    help="write burst pair 0 of the frame's SLCs (ref.npy, sec.npy) to DIR and exit: the "
+                         "reference arm's inputs, made in a process of their own")
     return ap.parse_args()
 
 
@@ -232,19 +235,37 @@ FRAME_CONFIGS = ("frame", "frame_small")
 FRAME_SEED = 20261203 + 2000
 
 
-def frame_scene(config, rank, device, boxes_of, slc_pairs=None):
+def frame_scene(config, rank, device, boxes_of, slc_pairs=None, ground_locked=False):
     """The frame workload of both arms: the seeded synthetic frame on a DEM
     grid where the reference geo2rdr runs of burst pair 0 stay inside their
     buffers (both arms time the same frame on the same grid).
     ``boxes_of(acq)``: the bursts' footprint boxes (the library's planner in
     the s1b arm, the oracle's restatement in the reference arm; the grid
     search gives the same grid for either).  ``slc_pairs``: make the SLCs of
-    the first pairs only."""
+    the first pairs only.  ``ground_locked``: each pair's dates see one scene
+    (``synth.ground_lock_pairs``, made on that grid's DEM; needs CUDA and the
+    s1b library), else radar-coordinate speckle."""
     from sentinel_gpu_processor_b200 import synth
     small = config == "frame_small"
-    sc = synth.make_frame(seed=FRAME_SEED + rank, device=device, slc_pairs=slc_pairs,
+    sc = synth.make_frame(seed=FRAME_SEED + rank, device=device, slc_pairs=0 if ground_locked else slc_pairs,
                           **(dict(n_swaths=1, n_bursts=3, scale=0.5) if small else {}))
-    return synth.on_reference_safe_grid(sc, boxes_of, pairs=(0,))
+    sc = synth.on_reference_safe_grid(sc, boxes_of, pairs=(0,))
+    if ground_locked:
+        synth.ground_lock_pairs(sc, range(len(sc.ref) if slc_pairs is None else slc_pairs))
+    return sc
+
+
+def write_pair0(args):
+    """``--write-pair0 DIR``: burst pair 0's ground-locked SLCs as the s1b arm
+    makes them, written for the reference arm, whose own process must not
+    map the s1b library."""
+    import numpy as np
+    import torch
+
+    from sentinel_gpu_processor_b200 import plan as _plan
+    sc = frame_scene(args.config, 0, torch.device("cuda", 0), _plan.footprint_boxes, slc_pairs=1, ground_locked=True)
+    np.save(os.path.join(args.write_pair0, "ref.npy"), sc.ref_slc[0].cpu().numpy())
+    np.save(os.path.join(args.write_pair0, "sec.npy"), sc.sec_slc[0].cpu().numpy())
 
 
 def frame_config(args, sc, world):
@@ -257,7 +278,8 @@ def frame_config(args, sc, world):
             f"burst in 0.3..0.9")
     samples = "complex int16" if args.samples == "ci16" else "complex64"
     r = sc.rsc
-    return {"workload": f"{head}; {samples} SLC samples; int16 fBm DEM (0-3000 m) on a 1/7200-degree grid",
+    return {"workload": f"{head}; {samples} SLC samples (band-limited speckle, each pair's dates seeing one scene "
+                        f"at their own sample positions); int16 fBm DEM (0-3000 m) on a 1/7200-degree grid",
             "seed": int(sc.seed), "burst_pairs": n,
             "burst_px_per_step": int(sum(a.radar.lines_per_burst * a.radar.samples_per_burst for a in sc.ref)),
             "slc_samples": samples, "looks": [sc.rowlook, sc.collook],
@@ -358,7 +380,7 @@ def _workload(args, rank, dev):
         from sentinel_gpu_processor_b200.chain import BatchedFrameChain
         from sentinel_gpu_processor_b200 import plan as _plan
         small = args.config == "frame_small"
-        sc = frame_scene(args.config, rank, dev, _plan.footprint_boxes)
+        sc = frame_scene(args.config, rank, dev, _plan.footprint_boxes, ground_locked=True)
         chain = BatchedFrameChain(sc.ref, sc.sec, sc.rsc, sc.rowlook, sc.collook, sc.alpha, device=dev,
                                   sample_format=args.samples, deramp_fused=args.deramp == "fused",
                                   crossmul_fused=args.crossmul == "fused")
@@ -897,6 +919,10 @@ def run_s1b(args):
     if frame:
         run_info.update({"geo_px_total": sum(chain.geo_pixels()),
                          "ifg_ml_shapes_first3": [list(r.ifg.shape) for r in res[:3]],
+                         # simulated and measured (valid cells) coherence of every pair
+                         "coherence_sim_per_pair": [round(g, 3) for g in sc.extra["coherence"]],
+                         "mean_coherence_per_pair": [None if r is None else round(_mean_valid(r.coh), 3)
+                                                     for r in res],
                          "batched": True, "cuda_graph": True, "tuning": chain.tuned,
                          "deramp": "fused into the geocoding gathers" if chain.deramp_fused else "separate kernel",
                          "crossmul": ("look sums formed in the geocoding (no geocoded windows)"
@@ -1134,10 +1160,15 @@ def run_reference(args):
     if frame:
         import torch
         dev = "cuda" if torch.cuda.is_available() else "cpu"
-        sc = frame_scene(args.config, 0, dev, refrun.footprint_boxes, slc_pairs=1)
+        sc = frame_scene(args.config, 0, dev, refrun.footprint_boxes, slc_pairs=0)
         cfg = frame_config(args, sc, world)
         dem = sc.dem.cpu().numpy()
-        slcs = {"ref": sc.ref_slc[0].cpu().numpy(), "sec": sc.sec_slc[0].cpu().numpy()}
+        # burst pair 0's SLCs come from a process of their own (they are made
+        # with s1b kernels, which this process must not map)
+        with tempfile.TemporaryDirectory() as td:
+            subprocess.run([sys.executable, os.path.abspath(__file__), "--config", args.config, "--write-pair0", td],
+                           check=True, stdout=subprocess.DEVNULL)
+            slcs = {k: np.load(os.path.join(td, k + ".npy")) for k in ("ref", "sec")}
         if args.samples == "ci16":  # the reference's pipe carries the widened samples
             from sentinel_gpu_processor_b200 import synth
             slcs = {k: torch.view_as_complex(synth.cint16(torch.from_numpy(v)).float()).numpy()
@@ -1521,7 +1552,9 @@ def run_adjoint(args):
 
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.write_pair0:
+        write_pair0(args)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.config == "adjoint":
         run_adjoint(args)

@@ -759,6 +759,37 @@ def locked_to_reference(field, ref: Acquisition, sec: Acquisition, lat, lon, hgt
     return out * torch.polar(torch.ones_like(ph), ph).to(torch.complex64)
 
 
+def ground_lock_pairs(sc: PairScene, pairs) -> PairScene:
+    """Make the SLCs of the listed burst pairs of ``sc`` one scene seen by
+    both dates, as ``stack_slc`` does for a stack: pair k's reference holds
+    band-limited speckle seeded per pair, its ground points come from
+    ``rdr2geo_grid(terrain=True)`` on the scene's own DEM, the secondary sees
+    the same ground points at its own sample positions
+    (``locked_to_reference``) mixed with its own speckle at the pair's
+    coherence ``sc.extra["coherence"][k]``; both are TOPS-modulated.  The
+    geocoded interferogram of the pair is then coherent at about that
+    coherence.  Replaces ``sc.ref_slc[k]`` and ``sc.sec_slc[k]`` in place;
+    needs the DEM on a CUDA device."""
+    import torch
+    dev = sc.dem.device
+    height = dem_height_fn(sc.rsc, sc.dem)
+    for k in pairs:
+        ref, sec = sc.ref[k], sc.sec[k]
+        L, S = ref.radar.lines_per_burst, ref.radar.samples_per_burst
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(sc.seed * 1000 + 7 + k)
+        f = band_limited_speckle(L, S, gen, dev)
+        lat, lon, hgt = rdr2geo_grid(ref.orbit, ref.radar, ref.bursts[0], height, device=dev, terrain=True)
+        s = locked_to_reference(f, ref, sec, lat, lon, hgt)
+        del lat, lon, hgt
+        g = sc.extra["coherence"][k]
+        s = g * s + math.sqrt(1 - g * g) * band_limited_speckle(L, S, gen, dev)
+        sc.ref_slc[k] = tops_modulate(f, ref, ref.bursts[0]).contiguous()
+        sc.sec_slc[k] = tops_modulate(s, sec, sec.bursts[0]).contiguous()
+        del f, s
+    return sc
+
+
 def stack_slc(st: StackScene, date: int, burst: int, device="cpu"):
     """SLC of burst ``burst`` of date ``date`` (-1: the reference), TOPS-
     modulated.  The reference is band-limited speckle seeded per burst on its

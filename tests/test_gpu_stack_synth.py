@@ -36,3 +36,21 @@ def test_stack_pairs_coherent_at_simulated_coherence(cuda):
             # interpolation by the geocoding's bilinear gathers costs ~10 %
             assert 0.75 * g < m < 1.05 * g, (d, g, med[d])
     assert min(med[0]) > max(med[2])
+
+
+def test_frame_pairs_ground_locked_coherent(cuda):
+    """The frame's pairs made by ``synth.ground_lock_pairs`` (the bench's
+    headline workload) are coherent at about their simulated coherence."""
+    sc = synth.make_frame(device=cuda, n_swaths=1, n_bursts=3, scale=0.25, slc_pairs=0)
+    synth.ground_lock_pairs(sc, range(len(sc.ref)))
+    ch = BatchedFrameChain(sc.ref, sc.sec, sc.rsc, sc.rowlook, sc.collook, sc.alpha, device=cuda)
+    for v, s in zip(ch.ref_views + ch.sec_views, sc.ref_slc + sc.sec_slc):
+        v.copy_(s)
+    ch.capture(sc.dem)
+    ch.replay()
+    torch.cuda.synchronize()
+    for k, r in enumerate(ch.results()):
+        c = r.coh.float()
+        m = float(c[c > 0].mean())
+        g = sc.extra["coherence"][k]
+        assert 0.8 * g < m < 1.1 * g, (k, g, m)
