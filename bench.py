@@ -60,7 +60,31 @@ GEO_XMUL_TRAFFIC_RATIO = {"c64": 0.917, "ci16": 1.347}
 RESAMPLE_DRAM_BYTES_PER_PX = 24.75
 # what bounds the frame geocoding, from its ncu counters (issue and warp stalls)
 GEO_LIMITER = ("latency: per-pixel chain of FP64 solve, gathers and phasors at 20 resident warps per SM "
-               "(issue active 43 %, XU pipe 31 %, FP64 pipe 21 %); not HBM")
+               "(issue active 45 %, XU pipe 30 %, FP64 pipe 22 %); not HBM, not FP64 throughput")
+# FP64 operations of the frame geocoding per geocoded DEM pixel (both bursts):
+# ncu per-opcode thread-instruction counts of one launch on the small frame
+# (29.40 M geocoded pixels): 2 x 581.7 M DFMA + 273.7 M DMUL + 270.6 M DADD
+GEO_FP64_FLOP_PER_GEO_PX = 58.09
+
+
+def fp64_peak_tflops(dev):
+    """Measured FP64 throughput of this GPU: torch float64 matmul (cuBLAS
+    DGEMM) of 4096^3, best of 5, CUDA events."""
+    import torch
+    n = 4096
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
 def parse():
@@ -979,6 +1003,16 @@ def run_s1b(args):
                      "limiter": GEO_LIMITER if top == "geo2rdr" else "HBM"},
         "kernels": table,
     }
+    if frame and top == "geo2rdr" and chain.crossmul_fused and chain.deramp_fused:
+        # the geocoding's FP64 work against the GPU's measured FP64 throughput
+        flop = GEO_FP64_FLOP_PER_GEO_PX * run_info["geo_px_total"]
+        ach = flop / (t["avg_ms"] * 1e-3) / 1e12
+        pk = fp64_peak_tflops(dev)
+        line["roofline"]["fp64"] = {
+            "flop_per_launch": flop, "achieved_tflops": ach, "peak_tflops": pk, "frac": ach / pk,
+            "peak_kind": "measured: torch float64 matmul 4096^3, best of 5",
+            "count": f"{GEO_FP64_FLOP_PER_GEO_PX} FP64 operations per geocoded DEM pixel (ncu per-opcode counts: "
+                     f"2 DFMA + DMUL + DADD) x geocoded pixels"}
     if clk is not None:
         line["clocks"] = clk
     checker = rank == 0 and world == 1
