@@ -948,6 +948,7 @@ def run_s1b(args):
                          "mean_coherence_per_pair": [None if r is None else round(_mean_valid(r.coh), 3)
                                                      for r in res],
                          "batched": True, "cuda_graph": True, "tuning": chain.tuned,
+                         "tuning_source": chain.tuning_source,
                          "deramp": "fused into the geocoding gathers" if chain.deramp_fused else "separate kernel",
                          "crossmul": ("look sums formed in the geocoding (no geocoded windows)"
                                       if chain.crossmul_fused else "kernel reading the geocoded windows")})

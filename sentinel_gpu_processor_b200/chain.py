@@ -315,6 +315,63 @@ class RadarChain:
 FRAME_LIST_MAX = 240  # bursts per deramp launch (kFrameListMax, csrc/s1b_frame.h)
 
 
+TUNING_FIELDS = ("deramp_rows", "deramp_ctas", "geo_cols", "geo_ctas")
+
+
+def tuning_cache_path():
+    """The frame autotuner's cache file: ``$S1B_TUNING_CACHE``, else
+    ``$XDG_CACHE_HOME/s1b/frame_tuning.json`` (``~/.cache`` by default)."""
+    import os
+    p = os.environ.get("S1B_TUNING_CACHE")
+    if p:
+        return p
+    base = os.environ.get("XDG_CACHE_HOME") or os.path.join(os.path.expanduser("~"), ".cache")
+    return os.path.join(base, "s1b", "frame_tuning.json")
+
+
+def tuning_key(gpu_name, capability, sm_count, sample_format, deramp_fused, crossmul_fused, bursts):
+    """Key of a frame's shape class on one kind of GPU: the GPU (name,
+    compute capability, SM count), the frame's stage forms and its bursts'
+    count and median size, lines to 256 and samples to 2048 (the tile choices
+    depend on the burst shapes and the SM count, not on exact sizes)."""
+    lines = sorted(int(b[0]) for b in bursts)
+    samples = sorted(int(b[1]) for b in bursts)
+    ml, ms = lines[len(lines) // 2], samples[len(samples) // 2]
+    shape = f"{len(bursts)}x{(ml + 128) // 256 * 256}x{(ms + 1024) // 2048 * 2048}"
+    return (f"{gpu_name}|cc{capability[0]}.{capability[1]}|sm{sm_count}|{sample_format}|"
+            f"deramp={'fused' if deramp_fused else 'kernel'}|crossmul={'fused' if crossmul_fused else 'kernel'}|{shape}")
+
+
+def load_tuning(path):
+    """The cache's entries ({key: tuning dict}); empty when the file is
+    missing or unreadable, and entries without the four fields are dropped."""
+    import json
+    try:
+        with open(path) as f:
+            d = json.load(f)
+    except (OSError, ValueError):
+        return {}
+    if not isinstance(d, dict):
+        return {}
+    return {k: {f: int(v[f]) for f in TUNING_FIELDS} for k, v in d.items()
+            if isinstance(v, dict) and all(isinstance(v.get(f), int) for f in TUNING_FIELDS)}
+
+
+def store_tuning(path, key, tuning):
+    """Add or replace one entry; the file is replaced atomically, so
+    concurrent writers (ranks on one node) leave a complete file."""
+    import json
+    import os
+    import tempfile
+    d = load_tuning(path)
+    d[key] = {f: int(tuning[f]) for f in TUNING_FIELDS}
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    fd, tmp = tempfile.mkstemp(dir=os.path.dirname(os.path.abspath(path)), suffix=".tmp")
+    with os.fdopen(fd, "w") as f:
+        json.dump(d, f, indent=1, sort_keys=True)
+    os.replace(tmp, path)
+
+
 class BatchedFrameChain:
     """All burst pairs of a frame through one batched launch sequence
     (``s1b_frame_run``): deramp and geocoding over every burst (one CTA per
@@ -421,6 +478,7 @@ class BatchedFrameChain:
                        "s1b_frame_pair_slot")
             self.slots.append((off.value, r.value, c.value))
         self.burst_pixels = sum(plans[a].lines * plans[a].samples for a, _ in pairs)
+        self.tuning_source = "default"  # "timed" or "cache" once autotuned
         self.graph = None
         self.geo_events = None
 
@@ -457,11 +515,31 @@ class BatchedFrameChain:
         _lib.check(_call_frame("frame_run", _lib.load().s1b_frame_run, *self._args(dem, slc), _lib.stream_ptr()),
                    "s1b_frame_run")
 
-    def autotune(self, dem, reps=3):
-        """Time the tile-shape / grid candidates on this frame and keep the fastest."""
+    def autotune(self, dem, reps=3, cache=True):
+        """Time the tile-shape / grid candidates on this frame and keep the
+        fastest.  With ``cache``, the choice is kept in the tuning cache
+        (``tuning_cache_path``) under this GPU and the frame's shape class
+        (``tuning_key``), and a later frame of that class on that GPU takes it
+        from there without timing anything."""
+        key = path = None
+        if cache:
+            props = torch.cuda.get_device_properties(self.dev)
+            key = tuning_key(props.name, (props.major, props.minor), props.multi_processor_count,
+                             self.sample_format, self.deramp_fused, self.crossmul_fused,
+                             [(p.lines, p.samples) for p in self.plans])
+            path = tuning_cache_path()
+            hit = load_tuning(path).get(key)
+            if hit is not None:
+                self.set_tuning(**hit)
+                self.tuning_source = "cache"
+                return self.tuning()
         _lib.check(_lib.load().s1b_frame_autotune(*self._args(dem), int(reps), _lib.stream_ptr()),
                    "s1b_frame_autotune")
-        return self.tuning()
+        self.tuning_source = "timed"
+        t = self.tuning()
+        if cache:
+            store_tuning(path, key, t)
+        return t
 
     def profile(self, dem):
         """One run with CUDA events between stages: ms of deramp, geocoding, box,
