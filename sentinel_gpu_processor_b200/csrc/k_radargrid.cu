@@ -1,7 +1,8 @@
 // Radar-grid coregistration on sm_100a: secondary sample offsets from
 // float64 lat/lon/height rasters of the reference grid, TOPS-aware resampling
 // of the secondary onto the reference grid (8-tap windowed sinc or
-// bilinear), and boxcar coherence at full resolution.
+// bilinear), and boxcar coherence at full resolution (a register row walk
+// for windows up to 5 x 5, TMA-staged halo tiles for 7 x 7 and 9 x 9).
 //
 // The reference geocodes every SLC onto a lat/lon grid instead
 // (csrc/src/geo2rdr.cu:170-248); this mode has no reference counterpart.  It
@@ -841,6 +842,7 @@ __global__ __launch_bounds__(RT_THREADS, 2) void resample_tma_kernel(
 }
 
 // ------------------------------------------------------- box coherence
+// Windows of 7 x 7 and 9 x 9 (5 x 5 and smaller use the row walk below).
 // Persistent kernel, one CTA of 512 threads per SM, output tiles of 128
 // columns x 32 rows taken round-robin.  Both SLC tiles plus a halo are
 // brought into shared memory by TMA (cp.async.bulk.tensor, zero fill outside
