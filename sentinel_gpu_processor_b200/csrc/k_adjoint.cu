@@ -39,6 +39,10 @@ namespace {
 
 constexpr int A_TX = 64, A_TY = 4, A_RPT = 4, A_TH = A_TY * A_RPT;  // 16 rows x <= 64 columns
 constexpr int A_WROWS = 32, A_WCOLS = 96;
+// rows per deramp segment: at least two column groups share the window
+// (A_TX * A_TY / A_WCOLS >= 2), so a segment has at most A_WROWS / 2 rows
+constexpr int A_SEG = A_WROWS / 2;
+static_assert(A_TX * A_TY / A_WCOLS >= 2, "deramp segments hold at most A_SEG rows");
 constexpr int A_BINS = 1024;
 constexpr int A_PARTS = 8;  // per-tile partials: 6 parameter sums, sum of gamma, windows
 
@@ -263,12 +267,20 @@ __global__ __launch_bounds__(A_TX *A_TY, 2) void adjoint_kernel(const AdjArgs a)
         float2 ph = phasor_pi(mkt * u * u);
         float2 step = phasor_pi(mkt * P.ati * (2.0 * u + P.ati));
         const float2 dstep = phasor_pi(2.0 * mkt * P.ati * P.ati);
+        // the segment's samples are loaded first (at most A_SEG rows: wrows <=
+        // A_WROWS and at least two groups), so their reads overlap
         const float2 *src = sec + (size_t)(wa0 + r0) * P.samples + (wr0 + c);
-        for (int r = r0; r < r1; ++r) {
-          sm.win[r][c] = cmul(__ldg(src), ph);
-          src += P.samples;
-          ph = cmul(ph, step);
-          step = cmul(step, dstep);
+        float2 v[A_SEG];
+#pragma unroll
+        for (int k = 0; k < A_SEG; ++k)
+          if (r0 + k < r1) v[k] = __ldg(src + (size_t)k * P.samples);
+#pragma unroll
+        for (int k = 0; k < A_SEG; ++k) {
+          if (r0 + k < r1) {
+            sm.win[r0 + k][c] = cmul(v[k], ph);
+            ph = cmul(ph, step);
+            step = cmul(step, dstep);
+          }
         }
       }
     }
