@@ -108,6 +108,8 @@ def parse():
     ap.add_argument("--samples", default="c64", choices=["ci16", "c64"],
                     help="frame SLC sample type: complex int16 as in the measurement TIFF (widened on the GPU), "
                          "or complex64 as the reference's geo2rdr pipe carries it")
+    ap.add_argument("--adjoint-bursts", type=int, default=8,
+                    help="--config adjoint: bursts of 1500 x 21000 (8 as configured; fewer for a profile)")
     ap.add_argument("--write-pair0", metavar="DIR", default=None,
                     help="write burst pair 0 of the frame's SLCs (ref.npy, sec.npy) to DIR and exit: the "
                          "reference arm's inputs, made in a process of their own")
@@ -1292,8 +1294,8 @@ ADJ_STEP_PX = 1e-3   # central-difference step of the offset parameters (samples
 ADJ_STEP_M = 0.4     # central-difference step along the height-error direction (metres)
 
 
-def adjoint_measure(dev, steps, world, compact=False):
-    """Adjoint of the coherence objective on 8 bursts of 1500 x 21000: gradient
+def adjoint_measure(dev, steps, world, compact=False, n_bursts=8):
+    """Adjoint of the coherence objective on ``n_bursts`` (8) bursts of 1500 x 21000: gradient
     evaluations per second through the fused adjoint, against central finite
     differences of every parameter plus one height-error direction run with
     the fused forward on the same GPU; a 50-step Adam refinement.  Returns a
@@ -1302,7 +1304,7 @@ def adjoint_measure(dev, steps, world, compact=False):
 
     from sentinel_gpu_processor_b200 import synth
     from sentinel_gpu_processor_b200.refine import CoherenceObjective, CoregProblem, refine
-    n = 8
+    n = n_bursts
     # the reference grid is the burst's interior (16 samples off every edge):
     # no pixel's sinc support reaches the secondary burst's edge under the
     # perturbations, where J would jump as pixels enter or leave the support
@@ -1564,7 +1566,7 @@ def run_adjoint(args):
     dev = torch.device("cuda", local)
     clocks = Clocks(local)
     clocks.start()
-    m = adjoint_measure(dev, args.steps, world)
+    m = adjoint_measure(dev, args.steps, world, n_bursts=args.adjoint_bursts)
     clk = clocks.stop()
     line = {
         "metric": "adjoint evals/s (dJ/d offset polynomials and height field, J = -mean multilooked coherence)",
