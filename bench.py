@@ -1041,7 +1041,8 @@ def run_s1b(args):
         if not args.no_extras:
             extras["radar_grid_c1"] = _radar_extras(dev, peak)
             extras["adjoint_c3"] = adjoint_measure(dev, max(3, min(args.steps, 10)), world, compact=True)
-            stack = stack_measure(dev, 3, world, offsets_rows=0 if args.no_parity else 1)
+            # the float64 checker of every pair's sample coordinates runs at N = 1 only
+            stack = stack_measure(dev, 3, world, offsets_rows=0 if (args.no_parity or world > 1) else 1)
             by_date, errs = {}, []
             for p in stack.pop("per_pair"):
                 if p["mean_coherence"] is not None:
@@ -1545,7 +1546,7 @@ def run_stack(args):
     dev = torch.device("cuda", local)
     clocks = Clocks(local)
     clocks.start()
-    m = stack_measure(dev, args.steps, world, offsets_rows=0 if args.no_parity else 2)
+    m = stack_measure(dev, args.steps, world, offsets_rows=0 if (args.no_parity or world > 1) else 2)
     clk = clocks.stop()
     value = max_over_ranks(m["ms_per_stack"], world)
     line = {"metric": METRIC, "value": world * m["burst_px"] / (value / 1e3), "unit": UNIT, "n_gpus": world,
