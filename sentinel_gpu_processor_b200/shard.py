@@ -48,3 +48,41 @@ def frame_shard(ref_acqs, sec_acqs, rank, world):
 def shard_loads(weights, shards):
     """Total weight of each shard."""
     return [sum(float(weights[i]) for i in s) for s in shards]
+
+
+def gather_pairs(products, n_pairs, world, dst=0):
+    """Collect per-pair products of every rank on rank ``dst``, in pair order:
+    the one step that needs them together is stitching a subswath, whose
+    bursts the split may have put on different ranks.  ``products`` maps this
+    rank's pair indices to tensors (or tuples of tensors); they travel through
+    ``torch.distributed.gather_object`` (NCCL or gloo), leaving as host
+    copies.  Returns the list of ``n_pairs`` products on ``dst``, None
+    elsewhere; with ``world == 1`` no process group is needed."""
+    import torch
+
+    def host(x):
+        if isinstance(x, torch.Tensor):
+            return x.detach().cpu()
+        if isinstance(x, (tuple, list)):
+            return type(x)(host(y) for y in x)
+        return x
+
+    mine = {int(k): host(v) for k, v in products.items()}
+    if world == 1:
+        parts = [mine]
+    else:
+        import torch.distributed as dist
+        parts = [None] * world if dist.get_rank() == dst else None
+        dist.gather_object(mine, parts, dst=dst)
+        if dist.get_rank() != dst:
+            return None
+    out = [None] * n_pairs
+    for part in parts:
+        for k, v in part.items():
+            if out[k] is not None:
+                raise ValueError(f"pair {k} came from two ranks")
+            out[k] = v
+    missing = [k for k, v in enumerate(out) if v is None]
+    if missing:
+        raise ValueError(f"pairs {missing} came from no rank")
+    return out

@@ -33,6 +33,18 @@ def test_lpt_partition_and_bound_against_brute_force():
         assert max(shard.shard_loads(w, s)) <= (4 / 3 - 1 / (3 * m)) * best + 1e-9
 
 
+def test_gather_pairs_single_rank_and_errors():
+    import torch
+    out = shard.gather_pairs({1: torch.ones(2), 0: (torch.zeros(1), torch.ones(1))}, 2, 1)
+    assert torch.equal(out[1], torch.ones(2)) and torch.equal(out[0][1], torch.ones(1))
+    try:
+        shard.gather_pairs({0: torch.ones(1)}, 2, 1)
+    except ValueError as e:
+        assert "no rank" in str(e)
+    else:
+        raise AssertionError("a missing pair was accepted")
+
+
 def test_lpt_is_deterministic_and_handles_edges():
     assert shard.lpt_shards([], 3) == [[], [], []]
     assert shard.lpt_shards([5, 5, 5, 5], 2) == [[0, 2], [1, 3]]  # ties by index, then by rank
@@ -82,7 +94,11 @@ def _worker(rank, world, port, q):
         mine[idx] = rank + 1
         seen = [torch.zeros_like(mine) for _ in range(world)]
         dist.all_gather(seen, mine)  # test only: the data path itself has no collective
-        q.put((rank, [t.tolist() for t in seen]))
+        # per-pair products (a stand-in interferogram per pair) gathered on rank 0 for stitching
+        prods = {k: torch.full((2, 3), float(k)) for k in idx}
+        allp = sh.gather_pairs(prods, len(sc.ref), world, dst=0)
+        ok = None if allp is None else all(torch.equal(t, torch.full((2, 3), float(k))) for k, t in enumerate(allp))
+        q.put((rank, ([t.tolist() for t in seen], ok)))
     finally:
         dist.destroy_process_group()
 
@@ -98,6 +114,8 @@ def test_ranks_agree_on_disjoint_complete_shards():
         p.join(180)
         assert p.exitcode == 0
     got = dict(q.get(timeout=10) for _ in range(2))
+    assert got[0][1] is True and got[1][1] is None  # rank 0 holds every pair's product, in order
+    got = {r: v[0] for r, v in got.items()}
     assert got[0] == got[1]  # both ranks see the same assignment
     a, b = got[0]
     n = len(a)
