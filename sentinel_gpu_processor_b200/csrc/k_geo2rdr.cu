@@ -853,7 +853,7 @@ constexpr int kXmTX = kFrameXmCols;  // columns per tile
 template <typename TSrc, bool kFused, int MASK>
 __device__ __forceinline__ void geo_pair_pixel(const PlanTail *sp, const GeoConsts *gc, const ZeroDopplerPatch *zd0,
                                                const ZeroDopplerPatch *zd1, const double4 *m0, const double4 *m1,
-                                               const double p[3], double hgt, int r, const int *colw,
+                                               const double p[3], double hgt, double rd, const double *hb,
                                                const bool *act, const TSrc *__restrict__ src0,
                                                const TSrc *__restrict__ src1, const float4 *__restrict__ tops0,
                                                const float4 *__restrict__ tops1, float2 *v) {
@@ -864,7 +864,7 @@ __device__ __forceinline__ void geo_pair_pixel(const PlanTail *sp, const GeoCons
     const ZeroDopplerPatch &z = q ? *zd1 : *zd0;
     const double4 &m = q ? *m1 : *m0;
     const ZeroDopplerPoint pt = zero_doppler_point(z, p);
-    h[q] = fma(m.w, hgt, fma(m.z, i32_to_f64(r), fma(m.y, i32_to_f64(colw[q]), m.x)));
+    h[q] = fma(m.w, hgt, fma(m.z, rd, hb[q]));
     r2[q] = zero_doppler_solve2(pt, z.c3, z.inv_c1, h[q], act[q]);
   }
 #pragma unroll
@@ -997,6 +997,9 @@ __global__ __launch_bounds__(kXmTX, 5) void frame_geo_xmul_kernel(const FrameDev
     if (colw[q] < 0 || colw[q] >= fb.ncol) colw[q] = -1;  // the thread's column is outside this window
   }
   __syncwarp();  // lane 0's patch and seed models are visible to the warp
+  // the seed model's column term of the thread's column, per burst
+  const double hb[2] = {fma(s_seed[0][wid].y, i32_to_f64(colw[0]), s_seed[0][wid].x),
+                        fma(s_seed[1][wid].y, i32_to_f64(colw[1]), s_seed[1][wid].x)};
   const TSrc *src0, *src1;
   // tile rows [alo, ahi) of each burst's window at the thread's column
   int alo[2], ahi[2];
@@ -1043,7 +1046,7 @@ __global__ __launch_bounds__(kXmTX, 5) void frame_geo_xmul_kernel(const FrameDev
       const bool act[2] = {r >= alo[0] && r < ahi[0], r >= alo[1] && r < ahi[1]};
       float2 v[2];
       geo_pair_pixel<TSrc, kFused, MASK>(sp, s_gc, &s_zd[0][wid], &s_zd[1][wid], &s_seed[0][wid], &s_seed[1][wid], p,
-                                         hgt, r, colw, act,
+                                         hgt, i32_to_f64(r), hb, act,
                                          src0, src1, tops0, tops1, v);
       if ((MASK & 1) && (v[0].x != 0.f || v[0].y != 0.f)) {
         rlo0 = min(rlo0, r);
