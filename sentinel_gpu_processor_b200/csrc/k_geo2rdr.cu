@@ -257,14 +257,23 @@ __device__ __forceinline__ float2 load_ro(const short2 *p) {
 // height is written as zeros without solving its pixels.  Every pixel seeds
 // its Newton iteration from the line model, so its result does not depend on
 // whether the blocks before it were culled.
-// Per-burst constants of the pixel loop.
+// Per-burst constants of the pixel loop.  The validity bounds and the
+// line-0 times are kept as doubles here, formed by the same operations as
+// the per-pixel expressions they replace: converting the plan's integers per
+// pixel cost the pair kernel 6 % of its time.
 struct GeoConsts {
   double inv_dmrg, prf, two_over_c, k4_wvl;  // k4_wvl: two-way range phase, half-cycles per metre
+  double rg_lo, rg_hi, az_lo, az_hi;         // validity window fvs < rg < lvs - 1, fvl + 5 <= az < lvl - 5
+  double eta0, ea0;                          // -lines dtaz / 2, -lines ati / 2: line 0 from the burst centre
+  float ati_f;                               // ati in FP32
 };
 
 template <typename PL>
 __device__ __forceinline__ GeoConsts geo_consts(const PL &P) {
-  return GeoConsts{1.0 / P.dmrg, 1.0 / P.dtaz, 2.0 / kSolD, 4.0 / P.wvl};
+  return GeoConsts{1.0 / P.dmrg, 1.0 / P.dtaz, 2.0 / kSolD, 4.0 / P.wvl,
+                   (double)P.first_valid_sample, (double)(P.last_valid_sample - 1),
+                   (double)(P.first_valid_line + 5), (double)(P.last_valid_line - 5),
+                   -P.lines * P.dtaz / 2., -P.lines * P.ati / 2., (float)P.ati};
 }
 
 // Per-warp setup of one burst's geocoding.  The warp's pixels lie in window
@@ -879,20 +888,19 @@ __device__ __forceinline__ void geo_pair_pixel(const PlanTail *sp, const GeoCons
     const double rgoff = (rng - P.rngstart) * gc[q].inv_dmrg;
     const double azoff = (t - P.tstart) * gc[q].prf;
     // validity window, geo2rdr.cu:208-209, and the 2 x 2 neighbourhood inside the burst
-    bool valid = act[q] && rgoff > P.first_valid_sample && rgoff < P.last_valid_sample - 1 &&
-                 azoff >= P.first_valid_line + 5 && azoff < P.last_valid_line - 5;
+    bool valid = act[q] && rgoff > gc[q].rg_lo && rgoff < gc[q].rg_hi && azoff >= gc[q].az_lo && azoff < gc[q].az_hi;
     const int intr = valid ? (int)rgoff : 0, inta = valid ? (int)azoff : 0;
     valid = valid && intr >= 0 && intr + 1 < P.samples && inta >= 0 && inta + 1 < P.lines;
     if (!valid) continue;
     const double frd = rgoff - i32_to_f64(intr);
     const float fr = (float)frd, fa = (float)(azoff - i32_to_f64(inta));
     const size_t i1 = (size_t)inta * P.samples + intr;
-    const double eta = -P.lines * P.dtaz / 2. + t - P.tstart;
+    const double eta = gc[q].eta0 + t - P.tstart;
     if constexpr (kFused) {
       const float4 tc = __ldg((q ? tops1 : tops0) + intr);  // (kt, kt' - kt, etaref' - etaref, etaref)
-      const double ea = deramp_eta(P, inta);
+      const double ea = gc[q].ea0 + i32_to_f64(inta) * P.ati;  // deramp_eta(P, inta)
       const float k0 = tc.x, dk = tc.y, de = tc.z;
-      const float u = (float)ea - tc.w, ati = (float)P.ati;
+      const float u = (float)ea - tc.w, ati = gc[q].ati_f;
       const float w = fmaf(-fr, de, (float)(eta - ea));
       const float ub = u + ati, wb = w - ati, e = u + w;
       const float kfe = fr * dk * e * e;
