@@ -39,10 +39,7 @@ constexpr int DERAMP_ROWS = 16;
 // |x| < 2^22) and subtracting 1.5 * 2^23 leaves x exactly.  The same value as
 // (float)x, from an integer add and an FP32 add.
 __device__ __forceinline__ float i16_to_f32(int x) { return __int_as_float(0x4B400000 + x) - 12582912.0f; }
-// The same for int -> double with 1.5 * 2^52 (exact for |x| < 2^51).
-__device__ __forceinline__ double i32_to_f64(int x) {
-  return __longlong_as_double(0x4338000000000000LL + (long long)x) - 6755399441055744.0;
-}
+// int -> double: i32_to_f64 in s1b_device.cuh.
 
 // Two adjacent samples from an address aligned to their size (16 bytes for
 // complex64, 8 for complex int16), streamed.

@@ -294,8 +294,12 @@ __device__ __forceinline__ Coord coord_of(const s1b_burst_plan_t &P, const float
 }
 
 // Restore the secondary's TOPS phase at the fractional position (az lines).
-__device__ __forceinline__ float2 reramp(const s1b_burst_plan_t &P, float2 v, double mkt, double eref, double az) {
-  const double d = fma(az, P.ati, -P.lines * P.ati / 2.) - eref;
+// eta0 = -lines ati / 2 (line 0 from the burst centre), formed once per
+// thread: converting the plan's line count per pixel costs issue slots on the
+// conversion pipe.
+__device__ __forceinline__ float2 reramp(const s1b_burst_plan_t &P, float2 v, double mkt, double eref, double az,
+                                         double eta0) {
+  const double d = fma(az, P.ati, eta0) - eref;
   return cmul(v, phasor_pi_fast(-(mkt * d * d)));
 }
 
@@ -311,6 +315,7 @@ __global__ __launch_bounds__(R_TX *R_TY, 2) void resample_kernel(const __grid_co
   const int col = blockIdx.x * R_TX + tx;
   const int rowb = blockIdx.y * R_TH + ty * R_RPT;
   const int lo = sinc ? 3 : 0, hi = sinc ? 4 : 1;
+  const double eta0 = -P.lines * P.ati / 2.;  // line 0 from the burst centre
   if (tid == 0) {
     s_red[0] = INT_MAX;
     s_red[1] = INT_MIN;
@@ -416,7 +421,7 @@ __global__ __launch_bounds__(R_TX *R_TY, 2) void resample_kernel(const __grid_co
 #pragma unroll
     for (int q = 0; q < R_RPT; ++q) {
       const double t = k[q].fr;
-      const float2 v = reramp(P, acc[q], fma(t, dm, m0), fma(t, de, e0), (double)k[q].na + (double)k[q].fa);
+      const float2 v = reramp(P, acc[q], fma(t, dm, m0), fma(t, de, e0), i32_to_f64(k[q].na) + (double)k[q].fa, eta0);
       __stcs(out + (size_t)(rowb + q) * S + col, v);
     }
     return;
@@ -474,7 +479,7 @@ __global__ __launch_bounds__(R_TX *R_TY, 2) void resample_kernel(const __grid_co
       } else {
         tops_range(P, (double)kq.nr + (double)kq.fr, mkt, eref);
       }
-      v = reramp(P, acc, mkt, eref, (double)kq.na + (double)kq.fa);
+      v = reramp(P, acc, mkt, eref, i32_to_f64(kq.na) + (double)kq.fa, eta0);
     }
     __stcs(out + (size_t)row * S + col, v);
   }
@@ -569,6 +574,7 @@ __global__ __launch_bounds__(RT_THREADS, 2) void resample_tma_kernel(
   RtSmem &sm = *reinterpret_cast<RtSmem *>(rt_raw);
   const int tid = threadIdx.x, tx = tid % R_TX, ty = tid / R_TX, lane = tid % 32, warp = tid / 32;
   const int lo = sinc ? 3 : 0, hi = sinc ? 4 : 1;
+  const double eta0 = -P.lines * P.ati / 2.;  // line 0 from the burst centre
   const int n = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
   if (n == 0) return;
   {
@@ -775,7 +781,7 @@ __global__ __launch_bounds__(RT_THREADS, 2) void resample_tma_kernel(
 #pragma unroll
       for (int q = 0; q < R_RPT; ++q) {
         const double t = k[q].fr;
-        const float2 v = reramp(P, acc[q], fma(t, dm, m0), fma(t, de, e0), (double)k[q].na + (double)k[q].fa);
+        const float2 v = reramp(P, acc[q], fma(t, dm, m0), fma(t, de, e0), i32_to_f64(k[q].na) + (double)k[q].fa, eta0);
         __stcs(out + (size_t)(rowb + q) * S + col, v);
       }
     } else {
@@ -832,7 +838,7 @@ __global__ __launch_bounds__(RT_THREADS, 2) void resample_tma_kernel(
           } else {
             tops_range(P, (double)kq.nr + (double)kq.fr, mkt, eref);
           }
-          v = reramp(P, acc, mkt, eref, (double)kq.na + (double)kq.fa);
+          v = reramp(P, acc, mkt, eref, i32_to_f64(kq.na) + (double)kq.fa, eta0);
         }
         __stcs(out + (size_t)row * S + col, v);
       }

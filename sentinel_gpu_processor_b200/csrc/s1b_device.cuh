@@ -65,6 +65,13 @@ __device__ __forceinline__ float2 phasor_pi_fast(double h) {
   return make_float2(c, s);
 }
 
+// int -> double from an integer add and an FP64 add: adding x to the bit
+// pattern of 1.5 * 2^52 adds it to the value (exact for |x| < 2^51), and
+// subtracting 1.5 * 2^52 leaves x exactly.  The same value as (double)x.
+__device__ __forceinline__ double i32_to_f64(int x) {
+  return __longlong_as_double(0x4338000000000000LL + (long long)x) - 6755399441055744.0;
+}
+
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
